@@ -1,0 +1,155 @@
+/* rednoise-b200 additive path-tracing ABI (versioned, beside the drop-in
+ * rednoise.h). These entry points have no counterpart in the reference's C ABI;
+ * each one says which reference function's behaviour it exposes.
+ *
+ * Conventions
+ *  - Every function returns rn_status; RN_OK is 0. On failure
+ *    rn_pt_last_error() returns a message for the calling thread.
+ *  - Array arguments are host pointers and calls are synchronous, unless
+ *    `flags` contains RN_PT_DEVICE_POINTERS: then they are device pointers and
+ *    the work is enqueued on `stream` (a cudaStream_t, NULL = the scene's own
+ *    stream) without a host synchronisation.
+ *  - Triangle indices are the caller's original indices.
+ */
+#ifndef REDNOISE_PT_H
+#define REDNOISE_PT_H
+
+#include <stdint.h>
+
+#include "rednoise.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+	RN_OK = 0,
+	RN_ERR_INVALID_ARGUMENT = 1,
+	RN_ERR_CUDA = 2,
+	RN_ERR_OUT_OF_MEMORY = 3,
+	RN_ERR_UNSUPPORTED = 4,
+	RN_ERR_DEVICE_TIMEOUT = 5,
+	RN_ERR_CAPACITY = 6,
+	RN_ERR_INTERNAL = 7
+} rn_status;
+
+/* flags */
+#define RN_PT_DEVICE_POINTERS 1u /* arrays are device pointers; asynchronous on `stream` */
+#define RN_PT_ORDER_NEAREST 2u   /* closest hit: nearest-child-first traversal (default: reference order) */
+
+/* Physical-mode materials. */
+#define RN_PT_LAMBERT 0
+#define RN_PT_GGX 1
+#define RN_PT_DIELECTRIC 2
+
+/* A triangle scene given as arrays (all optional except vertices). The
+ * reference fields feed the drop-in reference-mode renderer (ModelTriangle,
+ * framework/ModelTriangle.h:26-39); the physical fields feed rn_pt_render. */
+typedef struct {
+	int num_triangles;
+	const float *vertices;       /* 9 floats per triangle: v0, v1, v2 */
+	const int *ref_rgb;          /* 3 ints per triangle, 0..255 (default 255) */
+	const int *ref_material;     /* reference Material enum value (default Diffuse) */
+	const float *ref_roughness;  /* reference Metal roughness (default 0.2) */
+	const float *ref_normal;     /* 3 floats per triangle (default: cross(e0,e1)/|cross|) */
+	const float *albedo;         /* 3 floats per triangle (default 0.8) */
+	const float *emission;       /* 3 floats per triangle, radiance Le (default 0) */
+	const int *material;         /* RN_PT_LAMBERT / RN_PT_GGX / RN_PT_DIELECTRIC (default Lambert) */
+	const float *material_param; /* GGX alpha, or dielectric IOR (default 0.2 / 1.5) */
+} rn_pt_scene_desc;
+
+/* Create a scene from arrays. The scene is freed with rn_scene_free. */
+rn_status rn_pt_scene_create(const rn_pt_scene_desc *desc, rn_scene **out);
+
+/* Build the reference BVH (src/BVH.cpp:6-63, identical tree and triangle
+ * order) and upload the scene now instead of at the first query. */
+rn_status rn_pt_scene_prepare(rn_scene *scene);
+
+/* Facts about the prepared scene. */
+typedef struct {
+	int num_triangles;
+	int internal_nodes;
+	int depth;
+	long long device_bytes;
+	double build_ms;
+} rn_pt_scene_info;
+rn_status rn_pt_scene_get_info(rn_scene *scene, rn_pt_scene_info *out);
+
+/* Dump the prepared BVH: order[n] (reference triangle order), and for each
+ * reference node (count = internal + leaves) its box and links
+ * (left, right, start, count) as BVH::Node holds them (src/BVH.h:22-26).
+ * Query the node count with nodes == NULL. */
+rn_status rn_pt_scene_dump_bvh(rn_scene *scene, int *order, int *node_count, float *bounds, int *links);
+
+/* Copy the scene's triangles out (any pointer may be NULL): vertices (9 per
+ * triangle), reference Colour (3 ints), reference Material and the face normal
+ * as the loader computed it (src/ObjLoader.cpp:170-176). */
+rn_status rn_pt_scene_get_triangles(const rn_scene *scene, float *vertices, int *ref_rgb, int *ref_material,
+                                    float *ref_normal);
+
+/* Closest hit for n rays (BVH::intersect, src/BVH.cpp:77-111): tri[i] is the
+ * original index of the hit triangle or -1; t/u/v as the reference reports them
+ * (t = +inf on a miss). ignore may be NULL (no triangle skipped). */
+rn_status rn_pt_trace_closest(rn_scene *scene, int n, const float *origins, const float *directions, const int *ignore,
+                              unsigned flags, void *stream, int *tri, float *t, float *u, float *v);
+
+/* Any hit strictly before tmax[i] (BVH::occluded, src/BVH.cpp:113-139). */
+rn_status rn_pt_trace_any(rn_scene *scene, int n, const float *origins, const float *directions, const float *tmax,
+                          const int *ignore, unsigned flags, void *stream, int *occluded);
+
+/* ---- reference-mode rendering (renderPathTraced, src/Renderer.cpp:1119-1170) ---- */
+
+/* A light with the reference Light's fields and defaults (src/Light.h:13-29).
+ * type: 0 point, 1 directional, 2 spot, 3 volume, 4 rectangle, 5 triangle. */
+typedef struct {
+	int type;
+	float position[3];
+	float direction[3];
+	float colour[3];
+	float intensity;
+	float radius;
+	float cone_cos;
+	float atten_constant, atten_linear, atten_quadratic;
+	float u_axis[3];
+	float v_axis[3];
+} rn_light;
+
+/* Camera(width, height, focal_length, position) + lookAt(target) with the
+ * reference's scale (src/Camera.h:13-25), plus renderPathTraced's arguments.
+ * num_lights == 0 uses the reference's default light (a 0.15-radius disk at
+ * (0, 0.95, 0), src/Renderer.cpp:1129-1134). max_depth is 4 in the reference. */
+typedef struct {
+	int width, height;
+	float position[3];
+	float target[3];
+	float focal_length;
+	float scale;
+	int orthographic;
+	float ortho_scale;
+	int samples;
+	int max_depth;
+	int num_lights;
+	const rn_light *lights;
+	float aperture, focus_distance;
+	float camera_motion[3];
+	int aperture_blades;
+} rn_pt_ref_params;
+
+/* Defaults of rn_render: camera at (0, 0, cam_z) looking at the origin,
+ * focal 2.0 x scale 150, depth 4, default light, no depth of field. */
+void rn_pt_ref_params_init(rn_pt_ref_params *p, int width, int height, float cam_z, int samples);
+
+/* Render with reference semantics. argb: width*height pixels in the reference
+ * Canvas format 0xAARRGGBB (may be NULL); mean_rgb: optional width*height*3
+ * floats of the per-pixel sample mean before the 8-bit clamp. */
+rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *params, unsigned flags, void *stream,
+                                 uint32_t *argb, float *mean_rgb);
+
+/* Message for the last failure on this thread ("" if none). */
+const char *rn_pt_last_error(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* REDNOISE_PT_H */

@@ -1,0 +1,267 @@
+"""TEST INFRASTRUCTURE ONLY -- the CPU oracle of rednoise_b200.
+
+Two checkers, loaded through ctypes:
+  * ``ref()``  -- oracle/_ref/librn_ref.so: the reference renderer's own sources
+    (BVH.cpp, Geometry.cpp, Renderer.cpp, ObjLoader.cpp, ...) compiled here by
+    oracle/Makefile, plus the flat test shim oracle/ref_shim.cpp;
+  * ``orc()``  -- oracle/_build/librn_oracle.so: the independent CPU restatement
+    oracle/rn_oracle.cpp, pinned against ``ref()`` by tests/test_oracle.py.
+
+Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py may use
+this package; the product library never links or calls it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_PATH = os.path.join(HERE, "_ref", "librn_ref.so")
+ORC_PATH = os.path.join(HERE, "_build", "librn_oracle.so")
+
+vp = ctypes.c_void_p
+ci = ctypes.c_int
+cf = ctypes.c_float
+
+_REF = None
+_ORC = None
+
+
+def P(a):
+    """ctypes pointer of a contiguous numpy array (None passes NULL)."""
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def ref_available() -> bool:
+    return os.path.isfile(REF_PATH)
+
+
+def ref() -> ctypes.CDLL:
+    global _REF
+    if _REF is None:
+        lib = ctypes.CDLL(REF_PATH)
+        sig = {
+            "refsh_model_new": (vp, [ci, vp, vp, vp, vp, vp]),
+            "refsh_model_from_obj": (vp, [ctypes.c_char_p, cf]),
+            "refsh_model_count": (ci, [vp]),
+            "refsh_model_get": (None, [vp, vp, vp, vp, vp, vp, vp]),
+            "refsh_model_free": (None, [vp]),
+            "refsh_bvh_new": (vp, [vp]),
+            "refsh_bvh_free": (None, [vp]),
+            "refsh_bvh_node_count": (ci, [vp]),
+            "refsh_bvh_root": (ci, [vp]),
+            "refsh_bvh_dump": (None, [vp, vp, vp, vp]),
+            "refsh_bvh_intersect": (None, [vp, ci, vp, vp, vp, vp, vp, vp, vp]),
+            "refsh_bvh_occluded": (None, [vp, ci, vp, vp, vp, vp, vp]),
+            "refsh_brute_intersect": (None, [vp, ci, vp, vp, vp, vp]),
+            "refsh_intersect_triangle": (ci, [vp, vp, vp, vp, vp, vp]),
+            "refsh_render_pathtraced": (None, [vp, ci, ci, cf, vp, vp, ci, ci, vp, cf, cf, vp, ci, vp]),
+            "rn_scene_load_obj": (vp, [ctypes.c_char_p, cf]),
+            "rn_scene_free": (None, [vp]),
+            "rn_render": (ci, [vp, ci, ci, ci, cf, ci, vp]),
+        }
+        for k, (r, a) in sig.items():
+            getattr(lib, k).restype = r
+            getattr(lib, k).argtypes = a
+        _REF = lib
+    return _REF
+
+
+def orc() -> ctypes.CDLL:
+    global _ORC
+    if _ORC is None:
+        lib = ctypes.CDLL(ORC_PATH)
+        sig = {
+            "orc_bvh_new": (vp, [ci, vp]),
+            "orc_bvh_free": (None, [vp]),
+            "orc_bvh_node_count": (ci, [vp]),
+            "orc_bvh_dump": (None, [vp, vp, vp, vp]),
+            "orc_intersect": (None, [vp, ci, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+            "orc_occluded": (None, [vp, ci, vp, vp, vp, vp, vp, vp, vp]),
+            "orc_render_reference": (None, [vp, vp, vp, vp, vp, ci, ci, ci, ci, cf, vp, vp, ci, ci, ci, vp, vp,
+                                            vp]),
+        }
+        for k, (r, a) in sig.items():
+            getattr(lib, k).restype = r
+            getattr(lib, k).argtypes = a
+        _ORC = lib
+    return _ORC
+
+
+# ---- convenience wrappers ---------------------------------------------------------
+
+class RefModel:
+    """A reference triangle list (vector<ModelTriangle>) and, lazily, its BVH."""
+
+    def __init__(self, handle):
+        self.h = handle
+        self._bvh = None
+
+    @classmethod
+    def from_obj(cls, path: str, scale: float) -> "RefModel":
+        return cls(ref().refsh_model_from_obj(os.fsencode(path), scale))
+
+    @classmethod
+    def from_arrays(cls, v9, rgb=None, material=None, roughness=None, normal=None) -> "RefModel":
+        v = np.ascontiguousarray(v9, np.float32).reshape(-1, 9)
+        keep = [v]
+        args = []
+        for a, dt in ((rgb, np.int32), (material, np.int32), (roughness, np.float32), (normal, np.float32)):
+            if a is None:
+                args.append(None)
+            else:
+                arr = np.ascontiguousarray(a, dt)
+                keep.append(arr)
+                args.append(P(arr))
+        return cls(ref().refsh_model_new(v.shape[0], P(v), *args))
+
+    @property
+    def count(self) -> int:
+        return ref().refsh_model_count(self.h)
+
+    def arrays(self) -> dict:
+        n = self.count
+        v = np.zeros((n, 9), np.float32)
+        rgb = np.zeros((n, 3), np.int32)
+        mat = np.zeros(n, np.int32)
+        nrm = np.zeros((n, 3), np.float32)
+        rough = np.zeros(n, np.float32)
+        ref().refsh_model_get(self.h, P(v), P(rgb), P(mat), P(nrm), P(rough), None)
+        return {"v": v, "rgb": rgb, "material": mat, "normal": nrm, "roughness": rough}
+
+    def bvh(self):
+        if self._bvh is None:
+            self._bvh = ref().refsh_bvh_new(self.h)
+        return self._bvh
+
+    def dump_bvh(self) -> dict:
+        b = self.bvh()
+        nn = ref().refsh_bvh_node_count(b)
+        order = np.zeros(self.count, np.int32)
+        bounds = np.zeros((nn, 6), np.float32)
+        links = np.zeros((nn, 4), np.int32)
+        ref().refsh_bvh_dump(b, P(order), P(bounds), P(links))
+        return {"order": order, "bounds": bounds, "links": links, "root": ref().refsh_bvh_root(b)}
+
+    def intersect(self, o, d, ignore=None):
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        ig = None if ignore is None else np.ascontiguousarray(ignore, np.int32)
+        idx = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        u = np.zeros(n, np.float32)
+        v = np.zeros(n, np.float32)
+        ref().refsh_bvh_intersect(self.bvh(), n, P(o), P(d), P(ig), P(idx), P(t), P(u), P(v))
+        return idx, t, u, v
+
+    def occluded(self, o, d, tmax, ignore=None):
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        tm = np.ascontiguousarray(tmax, np.float32)
+        n = o.shape[0]
+        ig = None if ignore is None else np.ascontiguousarray(ignore, np.int32)
+        occ = np.zeros(n, np.int32)
+        ref().refsh_bvh_occluded(self.bvh(), n, P(o), P(d), P(tm), P(ig), P(occ))
+        return occ
+
+    def brute(self, o, d):
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        idx = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        ref().refsh_brute_intersect(self.h, n, P(o), P(d), P(idx), P(t))
+        return idx, t
+
+    def render(self, w, h, samples, focal=2.0, pos=(0, 0, 4), target=(0, 0, 0), lights=None, aperture=0.0,
+               focus=4.0, motion=(0, 0, 0), blades=0) -> np.ndarray:
+        pos = np.asarray(pos, np.float32)
+        target = np.asarray(target, np.float32)
+        motion = np.asarray(motion, np.float32)
+        lt = None if not lights else np.ascontiguousarray(lights, np.float32).reshape(-1, 24)
+        out = np.zeros((h, w), np.uint32)
+        ref().refsh_render_pathtraced(self.h, w, h, focal, P(pos), P(target), samples,
+                                      0 if lt is None else lt.shape[0], P(lt), aperture, focus, P(motion), blades,
+                                      P(out))
+        return out
+
+    def close(self):
+        if self._bvh is not None:
+            ref().refsh_bvh_free(self._bvh)
+            self._bvh = None
+        if self.h:
+            ref().refsh_model_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OrcBvh:
+    """The oracle restatement's BVH over a (n, 9) vertex array."""
+
+    def __init__(self, v9):
+        self.v = np.ascontiguousarray(v9, np.float32).reshape(-1, 9)
+        self.h = orc().orc_bvh_new(self.v.shape[0], P(self.v))
+
+    def dump(self) -> dict:
+        nn = orc().orc_bvh_node_count(self.h)
+        order = np.zeros(self.v.shape[0], np.int32)
+        bounds = np.zeros((nn, 6), np.float32)
+        links = np.zeros((nn, 4), np.int32)
+        orc().orc_bvh_dump(self.h, P(order), P(bounds), P(links))
+        return {"order": order, "bounds": bounds, "links": links}
+
+    def intersect(self, o, d, ignore=None, counts=False):
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        ig = None if ignore is None else np.ascontiguousarray(ignore, np.int32)
+        idx = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        u = np.zeros(n, np.float32)
+        v = np.zeros(n, np.float32)
+        bx = np.zeros(n, np.int32) if counts else None
+        tr = np.zeros(n, np.int32) if counts else None
+        orc().orc_intersect(self.h, n, P(o), P(d), P(ig), P(idx), P(t), P(u), P(v), P(bx), P(tr))
+        return (idx, t, u, v, bx, tr) if counts else (idx, t, u, v)
+
+    def occluded(self, o, d, tmax, ignore=None, counts=False):
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        tm = np.ascontiguousarray(tmax, np.float32)
+        n = o.shape[0]
+        ig = None if ignore is None else np.ascontiguousarray(ignore, np.int32)
+        occ = np.zeros(n, np.int32)
+        bx = np.zeros(n, np.int32) if counts else None
+        tr = np.zeros(n, np.int32) if counts else None
+        orc().orc_occluded(self.h, n, P(o), P(d), P(tm), P(ig), P(occ), P(bx), P(tr))
+        return (occ, bx, tr) if counts else occ
+
+    def render_reference(self, normal, material, rgb, roughness, w, h, samples, y0=0, y1=None, focal=2.0,
+                         pos=(0, 0, 4), target=(0, 0, 0), max_depth=4, lights=None, want_mean=False):
+        y1 = h if y1 is None else y1
+        nrm = np.ascontiguousarray(normal, np.float32)
+        mat = np.ascontiguousarray(material, np.int32)
+        col = np.ascontiguousarray(rgb, np.int32)
+        rough = np.ascontiguousarray(roughness, np.float32)
+        pos = np.asarray(pos, np.float32)
+        target = np.asarray(target, np.float32)
+        lt = None if not lights else np.ascontiguousarray(lights, np.float32).reshape(-1, 24)
+        out = np.zeros((y1 - y0, w), np.uint32)
+        mean = np.zeros((y1 - y0, w, 3), np.float32) if want_mean else None
+        orc().orc_render_reference(self.h, P(nrm), P(mat), P(col), P(rough), w, h, y0, y1, focal, P(pos), P(target),
+                                   samples, max_depth, 0 if lt is None else lt.shape[0], P(lt), P(out), P(mean))
+        return (out, mean) if want_mean else out
+
+    def __del__(self):
+        try:
+            orc().orc_bvh_free(self.h)
+        except Exception:
+            pass

@@ -1,0 +1,679 @@
+// TEST INFRASTRUCTURE ONLY -- the CPU oracle. Never linked into the product.
+//
+// An independent CPU restatement of the reference path tracer's hot path, used
+// by tests/ (and the CPU-baseline leg of bench.py) to check the CUDA kernels.
+// It is pinned against the reference itself (oracle/_ref/librn_ref.so, built
+// from the reference sources) by the CPU tests in tests/test_oracle.py.
+//
+// Restated here, each from the cited reference lines:
+//   * BVH build, median split, leaf <= 4           src/BVH.cpp:6-63
+//   * slab test                                     src/BVH.cpp:66-75
+//   * closest hit / any hit traversal               src/BVH.cpp:77-139
+//   * ray/triangle test (glm inverse order)         src/Geometry.cpp:11-25
+//   * reference path-tracer estimator               src/Renderer.cpp:390-498, 555-563,
+//                                                   642-660, 775-907, 1103-1170
+//   * improved Perlin noise (procedural colour)     src/Noise.cpp:6-61, 246-255
+// The traversal is instrumented: it counts node box tests and triangle tests,
+// which give the algorithmic bytes of a ray query (24 B per box, 36 B per
+// triangle) used as the roofline numerator.
+//
+// Built with -ffp-contract=off (oracle/Makefile): no FMA contraction, so float
+// results follow the reference's non-FMA build operation by operation.
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "rn_oracle_rng.hpp"
+
+namespace {
+
+struct V3 {
+	float x, y, z;
+};
+inline V3 mk(float x, float y, float z) { return {x, y, z}; }
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator-(V3 a) { return {-a.x, -a.y, -a.z}; }
+inline V3 operator*(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+inline V3 operator*(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 operator*(float s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+inline V3 operator/(V3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+inline float dot(V3 a, V3 b) {
+	float x = a.x * b.x, y = a.y * b.y, z = a.z * b.z;
+	return (x + y) + z;
+}
+inline V3 cross(V3 x, V3 y) { return {x.y * y.z - y.y * x.z, x.z * y.x - y.z * x.x, x.x * y.y - y.x * x.y}; }
+inline float length(V3 v) { return std::sqrt(dot(v, v)); }
+inline V3 normalize(V3 v) { return v * (1.0f / std::sqrt(dot(v, v))); }
+inline V3 reflect(V3 I, V3 N) { return I - (N * dot(N, I)) * 2.0f; }
+inline V3 refract(V3 I, V3 N, float eta) {
+	float dv = dot(N, I);
+	float k = 1.0f - eta * eta * (1.0f - dv * dv);
+	return (k >= 0.0f) ? (eta * I - (eta * dv + std::sqrt(k)) * N) : mk(0, 0, 0);
+}
+inline V3 mix(V3 x, V3 y, float a) { return x * (1.0f - a) + y * a; }
+inline float gmin(float x, float y) { return (y < x) ? y : x; }
+inline float gmax(float x, float y) { return (x < y) ? y : x; }
+inline V3 vmin(V3 a, V3 b) { return {gmin(a.x, b.x), gmin(a.y, b.y), gmin(a.z, b.z)}; }
+inline V3 vmax(V3 a, V3 b) { return {gmax(a.x, b.x), gmax(a.y, b.y), gmax(a.z, b.z)}; }
+inline float comp(V3 v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+
+struct Tri {
+	V3 v0, v1, v2;
+};
+
+struct Node {
+	V3 bmin, bmax;
+	int left = -1, right = -1, start = 0, count = 0;
+};
+
+struct Bvh {
+	std::vector<Tri> tris;
+	std::vector<V3> cent;
+	std::vector<int> order;
+	std::vector<Node> nodes;
+	int root = -1;
+
+	int build(int start, int count) {
+		Node node;
+		V3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
+		for (int i = start; i < start + count; i++) {
+			const Tri &t = tris[order[i]];
+			for (V3 v : {t.v0, t.v1, t.v2}) {
+				lo = vmin(lo, v);
+				hi = vmax(hi, v);
+			}
+		}
+		node.bmin = lo;
+		node.bmax = hi;
+		if (count <= 4) {
+			node.start = start;
+			node.count = count;
+			nodes.push_back(node);
+			return static_cast<int>(nodes.size()) - 1;
+		}
+		V3 cmin = mk(1e30f, 1e30f, 1e30f), cmax = mk(-1e30f, -1e30f, -1e30f);
+		for (int i = start; i < start + count; i++) {
+			cmin = vmin(cmin, cent[order[i]]);
+			cmax = vmax(cmax, cent[order[i]]);
+		}
+		V3 e = cmax - cmin;
+		int axis = (e.x > e.y && e.x > e.z) ? 0 : (e.y > e.z ? 1 : 2);
+		int mid = start + count / 2;
+		std::nth_element(order.begin() + start, order.begin() + mid, order.begin() + start + count,
+		                 [&](int a, int b) { return comp(cent[a], axis) < comp(cent[b], axis); });
+		if (mid == start || mid == start + count) {
+			node.start = start;
+			node.count = count;
+			nodes.push_back(node);
+			return static_cast<int>(nodes.size()) - 1;
+		}
+		int self = static_cast<int>(nodes.size());
+		nodes.push_back(node);
+		int l = build(start, mid - start);
+		int r = build(mid, start + count - mid);
+		nodes[self].left = l;
+		nodes[self].right = r;
+		return self;
+	}
+};
+
+bool slab_hit(V3 o, V3 inv, V3 lo, V3 hi, float tmax) {
+	V3 t0 = (lo - o) * inv, t1 = (hi - o) * inv;
+	V3 ts = vmin(t0, t1), tb = vmax(t0, t1);
+	float te = ts.x;
+	if (te < ts.y)
+		te = ts.y;
+	if (te < ts.z)
+		te = ts.z;
+	float tx = tb.x;
+	if (tb.y < tx)
+		tx = tb.y;
+	if (tb.z < tx)
+		tx = tb.z;
+	float m0 = (te < 0.0f) ? 0.0f : te;
+	return tx >= m0 && te < tmax;
+}
+
+// inverse(mat3(-d, e0, e1)) * (o - v0) in glm's expression order.
+bool tri_hit(V3 o, V3 d, const Tri &tr, float &t, float &u, float &v) {
+	V3 e0 = tr.v1 - tr.v0, e1 = tr.v2 - tr.v0, sp = o - tr.v0;
+	V3 m0 = -d, m1 = e0, m2 = e1;
+	float det = +m0.x * (m1.y * m2.z - m2.y * m1.z) - m1.x * (m0.y * m2.z - m2.y * m0.z) +
+	            m2.x * (m0.y * m1.z - m1.y * m0.z);
+	if (std::fabs(det) < 1e-8f)
+		return false;
+	float k = 1.0f / (+m0.x * (m1.y * m2.z - m2.y * m1.z) - m1.x * (m0.y * m2.z - m2.y * m0.z) +
+	                  m2.x * (m0.y * m1.z - m1.y * m0.z));
+	float i00 = +(m1.y * m2.z - m2.y * m1.z) * k;
+	float i10 = -(m1.x * m2.z - m2.x * m1.z) * k;
+	float i20 = +(m1.x * m2.y - m2.x * m1.y) * k;
+	float i01 = -(m0.y * m2.z - m2.y * m0.z) * k;
+	float i11 = +(m0.x * m2.z - m2.x * m0.z) * k;
+	float i21 = -(m0.x * m2.y - m2.x * m0.y) * k;
+	float i02 = +(m0.y * m1.z - m1.y * m0.z) * k;
+	float i12 = -(m0.x * m1.z - m1.x * m0.z) * k;
+	float i22 = +(m0.x * m1.y - m1.x * m0.y) * k;
+	t = i00 * sp.x + i10 * sp.y + i20 * sp.z;
+	u = i01 * sp.x + i11 * sp.y + i21 * sp.z;
+	v = i02 * sp.x + i12 * sp.y + i22 * sp.z;
+	return (u >= 0.0f) && (v >= 0.0f) && (u + v <= 1.0f) && (t > 1e-5f);
+}
+
+struct Counts {
+	long boxes = 0, tris = 0;
+};
+
+struct Hit {
+	bool hit = false;
+	int idx = -1;
+	float t = INFINITY, u = 0, v = 0;
+	V3 point = mk(0, 0, 0);
+};
+
+Hit intersect(const Bvh &b, V3 o, V3 d, int ignore, Counts *cnt) {
+	Hit h;
+	if (b.root < 0)
+		return h;
+	V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+	int st[64], sp = 0;
+	st[sp++] = b.root;
+	while (sp > 0) {
+		const Node &n = b.nodes[st[--sp]];
+		if (cnt)
+			cnt->boxes++;
+		if (!slab_hit(o, inv, n.bmin, n.bmax, h.t))
+			continue;
+		if (n.count > 0) {
+			for (int i = n.start; i < n.start + n.count; i++) {
+				int ti = b.order[i];
+				if (ti == ignore)
+					continue;
+				float t, u, v;
+				if (cnt)
+					cnt->tris++;
+				if (tri_hit(o, d, b.tris[ti], t, u, v) && t < h.t) {
+					h.hit = true;
+					h.idx = ti;
+					h.t = t;
+					h.u = u;
+					h.v = v;
+					h.point = o + t * d;
+				}
+			}
+		} else {
+			st[sp++] = n.left;
+			st[sp++] = n.right;
+		}
+	}
+	return h;
+}
+
+bool occluded(const Bvh &b, V3 o, V3 d, float maxd, int ignore, Counts *cnt) {
+	if (b.root < 0)
+		return false;
+	V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+	int st[64], sp = 0;
+	st[sp++] = b.root;
+	while (sp > 0) {
+		const Node &n = b.nodes[st[--sp]];
+		if (cnt)
+			cnt->boxes++;
+		if (!slab_hit(o, inv, n.bmin, n.bmax, maxd))
+			continue;
+		if (n.count > 0) {
+			for (int i = n.start; i < n.start + n.count; i++) {
+				int ti = b.order[i];
+				if (ti == ignore)
+					continue;
+				float t, u, v;
+				if (cnt)
+					cnt->tris++;
+				if (tri_hit(o, d, b.tris[ti], t, u, v) && t < maxd)
+					return true;
+			}
+		} else {
+			st[sp++] = n.left;
+			st[sp++] = n.right;
+		}
+	}
+	return false;
+}
+
+// ---- reference-mode estimator ------------------------------------------------
+
+struct RefTri {
+	V3 normal;
+	int material;
+	V3 rgb;
+	float roughness;
+};
+
+struct Light {
+	int type;
+	V3 pos, dir, colour;
+	float intensity, radius, cone_cos, kc, kl, kq;
+	V3 u, v;
+};
+
+enum { kDiffuse = 0, kMirror, kGlass, kProcedural, kBump, kParallax, kMetal, kDispersive, kSubsurface, kNormalMap,
+       kEmissive };
+enum { kPoint = 0, kDirectional, kSpot, kVolume, kRectangle, kTriangle };
+
+const int kPerm[256] = {
+    151, 160, 137, 91,  90,  15,  131, 13,  201, 95,  96,  53,  194, 233, 7,   225, 140, 36,  103, 30,  69,  142,
+    8,   99,  37,  240, 21,  10,  23,  190, 6,   148, 247, 120, 234, 75,  0,   26,  197, 62,  94,  252, 219, 203,
+    117, 35,  11,  32,  57,  177, 33,  88,  237, 149, 56,  87,  174, 20,  125, 136, 171, 168, 68,  175, 74,  165,
+    71,  134, 139, 48,  27,  166, 77,  146, 158, 231, 83,  111, 229, 122, 60,  211, 133, 230, 220, 105, 92,  41,
+    55,  46,  245, 40,  244, 102, 143, 54,  65,  25,  63,  161, 1,   216, 80,  73,  209, 76,  132, 187, 208, 89,
+    18,  169, 200, 196, 135, 130, 116, 188, 159, 86,  164, 100, 109, 198, 173, 186, 3,   64,  52,  217, 226, 250,
+    124, 123, 5,   202, 38,  147, 118, 126, 255, 82,  85,  212, 207, 206, 59,  227, 47,  16,  58,  17,  182, 189,
+    28,  42,  223, 183, 170, 213, 119, 248, 152, 2,   44,  154, 163, 70,  221, 153, 101, 155, 167, 43,  172, 9,
+    129, 22,  39,  253, 19,  98,  108, 110, 79,  113, 224, 232, 178, 185, 112, 104, 218, 246, 97,  228, 251, 34,
+    242, 193, 238, 210, 144, 12,  191, 179, 162, 241, 81,  51,  145, 235, 249, 14,  239, 107, 49,  192, 214, 31,
+    181, 199, 106, 157, 184, 84,  204, 176, 115, 121, 50,  45,  127, 4,   150, 254, 138, 236, 205, 93,  222, 114,
+    67,  29,  24,  72,  243, 141, 128, 195, 78,  66,  215, 61,  156, 180};
+inline int P(int i) { return kPerm[i & 255]; }
+inline float fade(float t) { return t * t * t * (t * (t * 6.0f - 15.0f) + 10.0f); }
+inline float plerp(float t, float a, float b) { return a + t * (b - a); }
+inline float grad(int hash, float x, float y, float z) {
+	int h = hash & 15;
+	float u = h < 8 ? x : y;
+	float v = h < 4 ? y : (h == 12 || h == 14 ? x : z);
+	return ((h & 1) == 0 ? u : -u) + ((h & 2) == 0 ? v : -v);
+}
+float perlin(float x, float y, float z) {
+	int X = static_cast<int>(std::floor(x)) & 255, Y = static_cast<int>(std::floor(y)) & 255,
+	    Z = static_cast<int>(std::floor(z)) & 255;
+	x -= std::floor(x);
+	y -= std::floor(y);
+	z -= std::floor(z);
+	float u = fade(x), v = fade(y), w = fade(z);
+	int A = P(X) + Y, AA = P(A) + Z, AB = P(A + 1) + Z;
+	int B = P(X + 1) + Y, BA = P(B) + Z, BB = P(B + 1) + Z;
+	return plerp(w,
+	             plerp(v, plerp(u, grad(P(AA), x, y, z), grad(P(BA), x - 1, y, z)),
+	                   plerp(u, grad(P(AB), x, y - 1, z), grad(P(BB), x - 1, y - 1, z))),
+	             plerp(v, plerp(u, grad(P(AA + 1), x, y, z - 1), grad(P(BA + 1), x - 1, y, z - 1)),
+	                   plerp(u, grad(P(AB + 1), x, y - 1, z - 1), grad(P(BB + 1), x - 1, y - 1, z - 1))));
+}
+V3 procedural(V3 p) {
+	V3 q = p * 3.0f;
+	float sum = 0.0f, amp = 1.0f, freq = 1.0f, norm = 0.0f;
+	for (int i = 0; i < 4; i++) {
+		sum += amp * perlin(q.x * freq, q.y * freq, q.z * freq);
+		norm += amp;
+		amp *= 0.5f;
+		freq *= 2.0f;
+	}
+	float n = 0.5f + 0.5f * (sum / norm);
+	float rings = 0.5f + 0.5f * std::sin((q.x + q.y) * 3.0f + n * 8.0f);
+	return mix(mk(60, 30, 12), mk(205, 150, 90), rings);
+}
+
+struct RefScene {
+	const Bvh *bvh;
+	std::vector<RefTri> tri;
+	std::vector<Light> lights;
+	int max_depth;
+};
+
+float visibility(const RefScene &s, const Light &L, V3 p, int ig) {
+	const Bvh &b = *s.bvh;
+	if (L.type == kDirectional)
+		return occluded(b, p, -normalize(L.dir), 1e6f, ig, nullptr) ? 0.0f : 1.0f;
+	auto frac = [&](V3 sp) {
+		V3 to = sp - p;
+		float dist = length(to);
+		return occluded(b, p, to / dist, dist, ig, nullptr) ? 0 : 1;
+	};
+	if (L.type == kRectangle) {
+		const float g[9][2] = {{-1, -1}, {0, -1}, {1, -1}, {-1, 0}, {0, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}};
+		int u = 0;
+		for (auto &q : g)
+			u += frac(L.pos + L.u * q[0] + L.v * q[1]);
+		return u / 9.0f;
+	}
+	if (L.type == kTriangle) {
+		const float g[9][2] = {{0, 0}, {1, 0}, {0, 1}, {0.5f, 0}, {0, 0.5f}, {0.5f, 0.5f}, {0.25f, 0.25f},
+		                       {0.5f, 0.25f}, {1.0f / 3.0f, 1.0f / 3.0f}};
+		int u = 0;
+		for (auto &q : g)
+			u += frac(L.pos + L.u * q[0] + L.v * q[1]);
+		return u / 9.0f;
+	}
+	if (L.radius <= 0.0f)
+		return static_cast<float>(frac(L.pos));
+	if (L.type == kVolume) {
+		const float kPi = 3.14159265358979323846f;
+		V3 toc = L.pos - p;
+		float d = length(toc);
+		V3 dir = toc / d;
+		float smx = std::min(1.0f, L.radius / d);
+		if (smx >= 1.0f)
+			return 1.0f;
+		float cmx = std::sqrt(std::max(0.0f, 1.0f - smx * smx));
+		V3 up = std::fabs(dir.y) < 0.99f ? mk(0, 1, 0) : mk(1, 0, 0);
+		V3 tg = normalize(cross(up, dir)), bt = cross(dir, tg);
+		const float rc[2] = {0.85f, 0.4f}, ro[2] = {0.0f, 0.5f};
+		const int rn[2] = {5, 6};
+		int un = 0, tot = 1;
+		if (!occluded(b, p, dir, d, ig, nullptr))
+			un++;
+		for (int r = 0; r < 2; r++) {
+			float ct = 1.0f - rc[r] * (1.0f - cmx), st = std::sqrt(std::max(0.0f, 1.0f - ct * ct));
+			for (int i = 0; i < rn[r]; i++) {
+				float phi = 2.0f * kPi * ((static_cast<float>(i) + ro[r]) / static_cast<float>(rn[r]));
+				V3 sd = normalize(dir * ct + (tg * std::cos(phi) + bt * std::sin(phi)) * st);
+				if (!occluded(b, p, sd, d, ig, nullptr))
+					un++;
+				tot++;
+			}
+		}
+		return static_cast<float>(un) / static_cast<float>(tot);
+	}
+	const float ks[9][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}, {0.7f, 0.7f}, {-0.7f, 0.7f}, {0.7f, -0.7f},
+	                        {-0.7f, -0.7f}};
+	V3 axis = normalize(p - L.pos);
+	V3 up = std::fabs(axis.y) < 0.99f ? mk(0, 1, 0) : mk(1, 0, 0);
+	V3 tg = normalize(cross(up, axis)), bt = cross(axis, tg);
+	int u = 0;
+	for (auto &q : ks)
+		u += frac(L.pos + (tg * q[0] + bt * q[1]) * L.radius);
+	return u / 9.0f;
+}
+
+void light_dir(const Light &L, V3 p, V3 &dir, float &att) {
+	if (L.type == kDirectional) {
+		dir = -normalize(L.dir);
+		att = L.intensity / 40.0f;
+	} else {
+		V3 to = L.pos - p;
+		float dist = length(to);
+		dir = to / dist;
+		att = L.intensity / (L.kc + L.kl * dist + L.kq * dist * dist);
+	}
+}
+
+V3 direct_light(const RefScene &s, V3 p, V3 n, V3 albedo, int ig) {
+	V3 sum = mk(0, 0, 0);
+	for (const Light &L : s.lights) {
+		V3 ld;
+		float att;
+		light_dir(L, p, ld, att);
+		float cone = 1.0f;
+		if (L.type == kSpot)
+			cone = (dot(-ld, normalize(L.dir)) > L.cone_cos) ? 1.0f : 0.0f;
+		float vis = visibility(s, L, p, ig);
+		float inc = std::max(0.0f, dot(n, ld));
+		sum = sum + L.colour * (vis * cone * att * inc);
+	}
+	return albedo * vmin(sum, mk(1, 1, 1));
+}
+
+using Rng = std::mt19937;
+float U01(Rng &r) { return std::uniform_real_distribution<float>(0.0f, 1.0f)(r); }
+
+V3 cosine_hemisphere(V3 n, Rng &rng) {
+	float u1 = U01(rng), u2 = U01(rng);
+	float r = std::sqrt(u1), th = 2.0f * 3.14159265f * u2;
+	float x = r * std::cos(th), y = r * std::sin(th), z = std::sqrt(std::max(0.0f, 1.0f - u1));
+	V3 up = std::fabs(n.z) < 0.99f ? mk(0, 0, 1) : mk(1, 0, 0);
+	V3 t = normalize(cross(up, n)), b = cross(n, t);
+	return normalize(t * x + b * y + n * z);
+}
+
+V3 face_viewer(V3 n, V3 d) { return dot(n, d) > 0.0f ? -n : n; }
+
+V3 base_colour(const RefTri &t, V3 p) { return t.material == kProcedural ? procedural(p) : t.rgb; }
+
+V3 path_trace(const RefScene &s, V3 o, V3 d, int depth, Rng &rng) {
+	Hit h = intersect(*s.bvh, o, d, -1, nullptr);
+	if (!h.hit) {
+		float t = 0.5f * (d.y + 1.0f);
+		return mix(mk(200, 210, 235), mk(70, 120, 205), t) / 255.0f;
+	}
+	const RefTri &tr = s.tri[h.idx];
+	V3 p = h.point;
+	int ig = h.idx;
+	if (tr.material == kEmissive)
+		return tr.rgb / 255.0f * 4.0f;
+	if (tr.material == kMirror && depth > 0) {
+		V3 n = face_viewer(tr.normal, d), r = reflect(d, n);
+		return path_trace(s, p + 1e-4f * r, r, depth - 1, rng);
+	}
+	if ((tr.material == kGlass || tr.material == kDispersive) && depth > 0) {
+		V3 n = tr.normal;
+		float cosi = dot(d, n), etai = 1.0f, etat = 1.5f;
+		if (cosi < 0.0f) {
+			cosi = -cosi;
+		} else {
+			std::swap(etai, etat);
+			n = -n;
+		}
+		float r0 = (etai - etat) / (etai + etat);
+		r0 *= r0;
+		float fr = r0 + (1.0f - r0) * std::pow(1.0f - cosi, 5.0f);
+		V3 rf = refract(d, n, etai / etat);
+		V3 dir = (length(rf) < 1e-6f || U01(rng) < fr) ? reflect(d, n) : rf;
+		return path_trace(s, p + 1e-4f * dir, dir, depth - 1, rng);
+	}
+	if (tr.material == kMetal && depth > 0) {
+		V3 n = face_viewer(tr.normal, d), r = reflect(d, n);
+		V3 df = cosine_hemisphere(n, rng);
+		float r2 = tr.roughness * tr.roughness;
+		V3 dir = normalize(mix(r, df, r2));
+		if (dot(dir, n) <= 0.0f)
+			dir = r;
+		V3 albedo = base_colour(tr, p) / 255.0f;
+		return albedo * path_trace(s, p + 1e-4f * dir, dir, depth - 1, rng);
+	}
+	if (tr.material == kSubsurface) {
+		V3 n = face_viewer(tr.normal, d);
+		V3 albedo = base_colour(tr, p) / 255.0f;
+		V3 shade = mk(0, 0, 0);
+		for (const Light &L : s.lights) {
+			V3 to = L.pos - p;
+			float dist = length(to);
+			V3 ld = to / dist;
+			float att = L.intensity / (L.kc + L.kl * dist + L.kq * dist * dist);
+			float wd = std::max(0.0f, (dot(n, ld) + 0.5f) / (1.0f + 0.5f));
+			shade = shade + albedo * L.colour * (visibility(s, L, p, ig) * att * wd);
+			Hit ex = intersect(*s.bvh, p - n * 1e-3f, ld, ig, nullptr);
+			float th = ex.hit ? ex.t : 0.0f;
+			shade = shade + albedo * L.colour * (att * std::exp(-3.0f * th) * 0.6f);
+		}
+		V3 direct = vmin(shade, mk(1.5f, 1.5f, 1.5f));
+		if (depth <= 0)
+			return direct;
+		V3 sb = cosine_hemisphere(n, rng);
+		return direct + albedo * path_trace(s, p + 1e-4f * sb, sb, depth - 1, rng);
+	}
+	V3 n = face_viewer(tr.normal, d);
+	V3 albedo = base_colour(tr, p) / 255.0f;
+	V3 direct = direct_light(s, p, n, albedo, ig);
+	if (depth <= 0)
+		return direct;
+	V3 bnc = cosine_hemisphere(n, rng);
+	return direct + albedo * path_trace(s, p + 1e-4f * bnc, bnc, depth - 1, rng);
+}
+
+} // namespace
+
+extern "C" {
+
+// ---- BVH ---------------------------------------------------------------------------
+
+void *orc_bvh_new(int n, const float *v9) {
+	Bvh *b = new Bvh();
+	b->tris.resize(static_cast<size_t>(n));
+	b->cent.resize(static_cast<size_t>(n));
+	b->order.resize(static_cast<size_t>(n));
+	for (int i = 0; i < n; i++) {
+		const float *p = v9 + 9 * static_cast<size_t>(i);
+		b->tris[i] = {mk(p[0], p[1], p[2]), mk(p[3], p[4], p[5]), mk(p[6], p[7], p[8])};
+		b->cent[i] = (b->tris[i].v0 + b->tris[i].v1 + b->tris[i].v2) / 3.0f;
+		b->order[i] = i;
+	}
+	if (n > 0)
+		b->root = b->build(0, n);
+	return b;
+}
+
+void orc_bvh_free(void *h) { delete static_cast<Bvh *>(h); }
+
+int orc_bvh_node_count(const void *h) { return static_cast<int>(static_cast<const Bvh *>(h)->nodes.size()); }
+
+void orc_bvh_dump(const void *h, int *order, float *bounds, int *links) {
+	const Bvh *b = static_cast<const Bvh *>(h);
+	std::memcpy(order, b->order.data(), b->order.size() * sizeof(int));
+	for (size_t i = 0; i < b->nodes.size(); i++) {
+		const Node &n = b->nodes[i];
+		const float bb[6] = {n.bmin.x, n.bmin.y, n.bmin.z, n.bmax.x, n.bmax.y, n.bmax.z};
+		std::memcpy(bounds + 6 * i, bb, sizeof(bb));
+		links[4 * i] = n.left;
+		links[4 * i + 1] = n.right;
+		links[4 * i + 2] = n.start;
+		links[4 * i + 3] = n.count;
+	}
+}
+
+// Closest hit; boxes/tris (optional) receive the per-ray box and triangle test counts.
+void orc_intersect(const void *h, int n, const float *o3, const float *d3, const int *ignore, int *idx, float *t,
+                   float *u, float *v, int *boxes, int *tris) {
+	const Bvh *b = static_cast<const Bvh *>(h);
+#pragma omp parallel for schedule(dynamic, 256)
+	for (int i = 0; i < n; i++) {
+		Counts c;
+		Hit r = intersect(*b, mk(o3[3 * i], o3[3 * i + 1], o3[3 * i + 2]), mk(d3[3 * i], d3[3 * i + 1], d3[3 * i + 2]),
+		                  ignore ? ignore[i] : -1, &c);
+		idx[i] = r.hit ? r.idx : -1;
+		t[i] = r.t;
+		u[i] = r.u;
+		v[i] = r.v;
+		if (boxes)
+			boxes[i] = static_cast<int>(c.boxes);
+		if (tris)
+			tris[i] = static_cast<int>(c.tris);
+	}
+}
+
+void orc_occluded(const void *h, int n, const float *o3, const float *d3, const float *maxd, const int *ignore,
+                  int *occ, int *boxes, int *tris) {
+	const Bvh *b = static_cast<const Bvh *>(h);
+#pragma omp parallel for schedule(dynamic, 256)
+	for (int i = 0; i < n; i++) {
+		Counts c;
+		occ[i] = occluded(*b, mk(o3[3 * i], o3[3 * i + 1], o3[3 * i + 2]), mk(d3[3 * i], d3[3 * i + 1], d3[3 * i + 2]),
+		                  maxd[i], ignore ? ignore[i] : -1, &c)
+		             ? 1
+		             : 0;
+		if (boxes)
+			boxes[i] = static_cast<int>(c.boxes);
+		if (tris)
+			tris[i] = static_cast<int>(c.tris);
+	}
+}
+
+// ---- reference-mode render -----------------------------------------------------
+// Lights: 24-float records [type, pos3, dir3, colour3, I, radius, coneCos, kc, kl, kq, u3, v3, pad2];
+// n_lights == 0 -> the reference's default light (0.15 disk at (0, 0.95, 0)).
+// Renders rows [y0, y1) of a w x h image with the camera of Camera(w, h, focal, pos) + lookAt(target),
+// scale 150; writes argb (w x (y1-y0)) and optionally mean (3 floats per pixel).
+void orc_render_reference(const void *bvh, const float *normal3, const int *material, const int *rgb,
+                          const float *roughness, int w, int h, int y0, int y1, float focal, const float *pos3,
+                          const float *target3, int samples, int max_depth, int n_lights, const float *lights,
+                          uint32_t *argb, float *mean) {
+	const Bvh *b = static_cast<const Bvh *>(bvh);
+	RefScene s;
+	s.bvh = b;
+	s.max_depth = max_depth;
+	const size_t n = b->tris.size();
+	s.tri.resize(n);
+	for (size_t i = 0; i < n; i++) {
+		s.tri[i].normal = mk(normal3[3 * i], normal3[3 * i + 1], normal3[3 * i + 2]);
+		s.tri[i].material = material[i];
+		s.tri[i].rgb = mk(static_cast<float>(rgb[3 * i]), static_cast<float>(rgb[3 * i + 1]),
+		                  static_cast<float>(rgb[3 * i + 2]));
+		s.tri[i].roughness = roughness[i];
+	}
+	if (n_lights == 0) {
+		Light d{};
+		d.type = kPoint;
+		d.pos = mk(0.0f, 0.95f, 0.0f);
+		d.dir = mk(0.0f, -1.0f, 0.0f);
+		d.colour = mk(1, 1, 1);
+		d.intensity = 40.0f;
+		d.radius = 0.15f;
+		d.cone_cos = 0.9f;
+		d.kc = 0.0f;
+		d.kl = 0.0f;
+		d.kq = 12.566370f;
+		d.u = mk(0.3f, 0, 0);
+		d.v = mk(0, 0, 0.3f);
+		s.lights.push_back(d);
+	}
+	for (int i = 0; i < n_lights; i++) {
+		const float *r = lights + 24 * static_cast<size_t>(i);
+		Light L;
+		L.type = static_cast<int>(r[0]);
+		L.pos = mk(r[1], r[2], r[3]);
+		L.dir = mk(r[4], r[5], r[6]);
+		L.colour = mk(r[7], r[8], r[9]);
+		L.intensity = r[10];
+		L.radius = r[11];
+		L.cone_cos = r[12];
+		L.kc = r[13];
+		L.kl = r[14];
+		L.kq = r[15];
+		L.u = mk(r[16], r[17], r[18]);
+		L.v = mk(r[19], r[20], r[21]);
+		s.lights.push_back(L);
+	}
+	V3 pos = mk(pos3[0], pos3[1], pos3[2]), tgt = mk(target3[0], target3[1], target3[2]);
+	V3 fwd = normalize(pos - tgt);
+	V3 right = normalize(cross(mk(0, 1, 0), fwd));
+	V3 up = cross(fwd, right);
+	float f = focal * 150.0f;
+#pragma omp parallel for schedule(dynamic, 1)
+	for (int y = y0; y < y1; y++) {
+		for (int x = 0; x < w; x++) {
+			Rng rng(static_cast<unsigned>((static_cast<unsigned>(y) * static_cast<unsigned>(w) +
+			                               static_cast<unsigned>(x)) *
+			                                  9781u +
+			                              1u));
+			std::uniform_real_distribution<float> jit(-0.5f, 0.5f);
+			V3 sum = mk(0, 0, 0);
+			for (int sidx = 0; sidx < samples; sidx++) {
+				float jx = jit(rng), jy = jit(rng);
+				float sx = x + 0.5f + jx - w / 2.0f, sy = -(y + 0.5f + jy - h / 2.0f);
+				V3 vv = mk(sx / f, sy / f, -1.0f);
+				V3 dir = normalize(right * vv.x + up * vv.y + fwd * vv.z);
+				(void)U01(rng); // the motion-blur draw the reference always makes
+				sum = sum + path_trace(s, pos, dir, max_depth, rng);
+			}
+			V3 c = sum / static_cast<float>(samples) * 255.0f;
+			auto cv = [](float v) {
+				return (v >= -2147483648.0f && v < 2147483648.0f) ? static_cast<int>(v)
+				                                                   : static_cast<int>(0x80000000u);
+			};
+			int r = std::min(255, cv(c.x)), g = std::min(255, cv(c.y)), bl = std::min(255, cv(c.z));
+			size_t k = static_cast<size_t>(y - y0) * static_cast<size_t>(w) + static_cast<size_t>(x);
+			argb[k] = (255u << 24) | ((static_cast<uint32_t>(r) & 0xFF) << 16) |
+			          ((static_cast<uint32_t>(g) & 0xFF) << 8) | (static_cast<uint32_t>(bl) & 0xFF);
+			if (mean) {
+				V3 m = sum / static_cast<float>(samples);
+				mean[3 * k] = m.x;
+				mean[3 * k + 1] = m.y;
+				mean[3 * k + 2] = m.z;
+			}
+		}
+	}
+}
+
+} // extern "C"

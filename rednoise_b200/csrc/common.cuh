@@ -1,0 +1,59 @@
+// Shared CUDA helpers: error propagation to the C ABI status codes and
+// device buffers owned by a scene.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "rednoise/rednoise_pt.h"
+
+namespace rnb {
+
+// Thread-local last error message for rn_pt_last_error().
+void set_last_error(const std::string &msg);
+const char *get_last_error();
+
+// Record a CUDA failure and map it to a status.
+rn_status cuda_fail(cudaError_t e, const char *what);
+
+#define RNB_CUDA(call)                                                                                                 \
+	do {                                                                                                               \
+		cudaError_t e__ = (call);                                                                                      \
+		if (e__ != cudaSuccess)                                                                                        \
+			return ::rnb::cuda_fail(e__, #call);                                                                       \
+	} while (0)
+
+// A device allocation that frees itself.
+struct DevBuf {
+	void *p = nullptr;
+	size_t bytes = 0;
+	DevBuf() = default;
+	DevBuf(const DevBuf &) = delete;
+	DevBuf &operator=(const DevBuf &) = delete;
+	~DevBuf() { release(); }
+	void release() {
+		if (p)
+			cudaFree(p);
+		p = nullptr;
+		bytes = 0;
+	}
+	// Grow-only (re)allocation; contents are not preserved.
+	cudaError_t ensure(size_t n) {
+		if (n <= bytes)
+			return cudaSuccess;
+		release();
+		cudaError_t e = cudaMalloc(&p, n);
+		if (e == cudaSuccess)
+			bytes = n;
+		else
+			p = nullptr;
+		return e;
+	}
+	template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+inline int ceil_div(long a, long b) { return static_cast<int>((a + b - 1) / b); }
+
+} // namespace rnb

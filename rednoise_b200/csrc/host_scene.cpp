@@ -1,0 +1,368 @@
+#include "host_scene.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+
+namespace rnb {
+
+namespace {
+
+// glm::min / glm::max on scalars: (y < x) ? y : x and (x < y) ? y : x
+// (third_party/glm/detail/func_common.inl:17-30). The comparison order matters
+// for signed zeros, so it is kept.
+inline float gmin(float x, float y) { return (y < x) ? y : x; }
+inline float gmax(float x, float y) { return (x < y) ? y : x; }
+
+struct Builder {
+	const float *v;
+	std::vector<Vec3> centroids;
+	Bvh2 *out;
+
+	const float *tri(int i) const { return v + 9 * static_cast<size_t>(i); }
+
+	// src/BVH.cpp:18-63, restated: box over the triangles of order[start, start+count),
+	// leaf when count <= 4, else nth_element at the median centroid of the widest
+	// centroid axis; the node slot is reserved before the children (pre-order).
+	int build(int start, int count, int depth) {
+		if (depth > out->depth)
+			out->depth = depth;
+		BvhNode node;
+		float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+		for (int i = start; i < start + count; i++) {
+			const float *t = tri(out->order[i]);
+			for (int k = 0; k < 3; k++)
+				for (int a = 0; a < 3; a++) {
+					lo[a] = gmin(lo[a], t[3 * k + a]);
+					hi[a] = gmax(hi[a], t[3 * k + a]);
+				}
+		}
+		node.bmin = {lo[0], lo[1], lo[2]};
+		node.bmax = {hi[0], hi[1], hi[2]};
+		if (count <= 4) {
+			node.start = start;
+			node.count = count;
+			out->nodes.push_back(node);
+			return static_cast<int>(out->nodes.size()) - 1;
+		}
+		float cmin[3] = {1e30f, 1e30f, 1e30f}, cmax[3] = {-1e30f, -1e30f, -1e30f};
+		for (int i = start; i < start + count; i++) {
+			const Vec3 &c = centroids[out->order[i]];
+			const float cc[3] = {c.x, c.y, c.z};
+			for (int a = 0; a < 3; a++) {
+				cmin[a] = gmin(cmin[a], cc[a]);
+				cmax[a] = gmax(cmax[a], cc[a]);
+			}
+		}
+		const float ex = cmax[0] - cmin[0], ey = cmax[1] - cmin[1], ez = cmax[2] - cmin[2];
+		const int axis = (ex > ey && ex > ez) ? 0 : (ey > ez ? 1 : 2);
+		const int mid = start + count / 2;
+		const Vec3 *cen = centroids.data();
+		auto key = [cen, axis](int a) { return axis == 0 ? cen[a].x : (axis == 1 ? cen[a].y : cen[a].z); };
+		std::nth_element(out->order.begin() + start, out->order.begin() + mid, out->order.begin() + start + count,
+		                 [&key](int a, int b) { return key(a) < key(b); });
+		if (mid == start || mid == start + count) {
+			node.start = start;
+			node.count = count;
+			out->nodes.push_back(node);
+			return static_cast<int>(out->nodes.size()) - 1;
+		}
+		node.count = 0;
+		const int self = static_cast<int>(out->nodes.size());
+		out->nodes.push_back(node);
+		const int l = build(start, mid - start, depth + 1);
+		const int r = build(mid, start + count - mid, depth + 1);
+		out->nodes[self].left = l;
+		out->nodes[self].right = r;
+		return self;
+	}
+};
+
+} // namespace
+
+void build_reference_bvh(const float *v9, int n, Bvh2 &out) {
+	out.order.resize(static_cast<size_t>(n));
+	out.nodes.clear();
+	out.root = -1;
+	out.depth = 0;
+	Builder b;
+	b.v = v9;
+	b.out = &out;
+	b.centroids.resize(static_cast<size_t>(n));
+	// centroid = (v0 + v1 + v2) / 3.0f, component-wise in that order (src/BVH.cpp:10-13).
+	for (int i = 0; i < n; i++) {
+		out.order[i] = i;
+		const float *t = v9 + 9 * static_cast<size_t>(i);
+		b.centroids[i] = {((t[0] + t[3]) + t[6]) / 3.0f, ((t[1] + t[4]) + t[7]) / 3.0f, ((t[2] + t[5]) + t[8]) / 3.0f};
+	}
+	if (n > 0) {
+		// The tree is built in pre-order, so the node count of a subtree depends only
+		// on its triangle count; reserve once to avoid reallocations on big meshes.
+		out.nodes.reserve(static_cast<size_t>(n) / 2 + 8);
+		out.root = b.build(0, n, 1);
+	}
+}
+
+Vec3 loader_face_normal(const float *t) {
+	// cross(v1 - v0, v2 - v0), divided by its length when > 1e-8, else (0,1,0).
+	const float ax = t[3] - t[0], ay = t[4] - t[1], az = t[5] - t[2];
+	const float bx = t[6] - t[0], by = t[7] - t[1], bz = t[8] - t[2];
+	const float cx = ay * bz - by * az, cy = az * bx - bz * ax, cz = ax * by - bx * ay;
+	const float len = std::sqrt((cx * cx + cy * cy) + cz * cz);
+	if (len > 1e-8f)
+		return {cx / len, cy / len, cz / len};
+	return {0.0f, 1.0f, 0.0f};
+}
+
+namespace {
+
+int materialFor(const std::string &name) {
+	if (name == "Mirror")
+		return kRefMirror;
+	if (name == "Glass")
+		return kRefGlass;
+	if (name == "Marble")
+		return kRefProcedural;
+	if (name == "Bumpy")
+		return kRefBump;
+	if (name == "Parallax")
+		return kRefParallax;
+	if (name == "Metal")
+		return kRefMetal;
+	if (name == "Dispersive" || name == "Prism")
+		return kRefDispersive;
+	if (name == "Subsurface" || name == "SSS" || name == "Wax" || name == "Jade")
+		return kRefSubsurface;
+	if (name == "NormalMap" || name == "Normal")
+		return kRefNormalMap;
+	if (name == "Emissive" || name == "Emit" || name == "Glow")
+		return kRefEmissive;
+	return kRefDiffuse;
+}
+
+struct Mtl {
+	int r = 0, g = 0, b = 0;
+};
+
+bool parse_int_prefix(const std::string &s, int &out) {
+	// std::stoi semantics on the leading integer (leading spaces and sign allowed).
+	const char *p = s.c_str();
+	char *end = nullptr;
+	errno = 0;
+	long v = std::strtol(p, &end, 10);
+	if (end == p || errno != 0 || v < -2147483647L || v > 2147483647L)
+		return false;
+	out = static_cast<int>(v);
+	return true;
+}
+
+bool parse_face_vertex(const std::string &tok, int &v) {
+	size_t slash = tok.find('/');
+	return parse_int_prefix(slash == std::string::npos ? tok : tok.substr(0, slash), v) && (v -= 1, true);
+}
+
+std::map<std::string, Mtl> load_mtl(const std::string &path) {
+	std::map<std::string, Mtl> out;
+	std::ifstream f(path);
+	if (!f.is_open())
+		return out;
+	std::string line, cur;
+	while (std::getline(f, line)) {
+		std::stringstream ss(line);
+		std::string type;
+		ss >> type;
+		if (type == "newmtl") {
+			ss >> cur;
+		} else if (type == "Kd" && !cur.empty()) {
+			float r = 0, g = 0, b = 0;
+			ss >> r >> g >> b;
+			Mtl m;
+			m.r = static_cast<int>(r * 255);
+			m.g = static_cast<int>(g * 255);
+			m.b = static_cast<int>(b * 255);
+			out[cur] = m;
+		}
+	}
+	return out;
+}
+
+} // namespace
+
+bool load_obj(const std::string &path, float scale, TriangleSet &ts, std::string &err) {
+	std::ifstream f(path);
+	if (!f.is_open()) {
+		err = "cannot open " + path;
+		return false;
+	}
+	std::string dir;
+	size_t slash = path.find_last_of("/\\");
+	if (slash != std::string::npos)
+		dir = path.substr(0, slash + 1);
+	std::map<std::string, Mtl> mtls;
+	std::vector<float> verts;
+	struct Face {
+		int a, b, c, r, g, bl, mat;
+	};
+	std::vector<Face> faces;
+	int cr = 0, cg = 0, cb = 0, cmat = kRefDiffuse;
+	std::string line;
+	while (std::getline(f, line)) {
+		std::stringstream ss(line);
+		std::string type;
+		ss >> type;
+		if (type == "mtllib") {
+			std::string name;
+			ss >> name;
+			mtls = load_mtl(dir + name);
+		} else if (type == "usemtl") {
+			std::string name;
+			ss >> name;
+			cmat = materialFor(name);
+			auto it = mtls.find(name);
+			if (it != mtls.end()) {
+				cr = it->second.r;
+				cg = it->second.g;
+				cb = it->second.b;
+			}
+		} else if (type == "v") {
+			float x = 0, y = 0, z = 0;
+			ss >> x >> y >> z;
+			verts.push_back(x * scale);
+			verts.push_back(y * scale);
+			verts.push_back(z * scale);
+		} else if (type == "f") {
+			std::string t1, t2, t3;
+			ss >> t1 >> t2 >> t3;
+			Face fc{};
+			if (!parse_face_vertex(t1, fc.a) || !parse_face_vertex(t2, fc.b) || !parse_face_vertex(t3, fc.c)) {
+				err = "malformed face line: " + line;
+				return false;
+			}
+			fc.r = cr;
+			fc.g = cg;
+			fc.bl = cb;
+			fc.mat = cmat;
+			faces.push_back(fc);
+		}
+	}
+	const long nv = static_cast<long>(verts.size() / 3);
+	ts = TriangleSet();
+	ts.v.reserve(faces.size() * 9);
+	for (const Face &fc : faces) {
+		for (int idx : {fc.a, fc.b, fc.c}) {
+			if (idx < 0 || idx >= nv) {
+				err = "face references a vertex that does not exist";
+				return false;
+			}
+			ts.v.push_back(verts[3 * idx]);
+			ts.v.push_back(verts[3 * idx + 1]);
+			ts.v.push_back(verts[3 * idx + 2]);
+		}
+		ts.rgb.push_back(fc.r);
+		ts.rgb.push_back(fc.g);
+		ts.rgb.push_back(fc.bl);
+		ts.ref_material.push_back(fc.mat);
+		ts.roughness.push_back(0.2f);
+	}
+	const size_t n = faces.size();
+	ts.normal.resize(3 * n);
+	for (size_t i = 0; i < n; i++) {
+		Vec3 nn = loader_face_normal(&ts.v[9 * i]);
+		ts.normal[3 * i] = nn.x;
+		ts.normal[3 * i + 1] = nn.y;
+		ts.normal[3 * i + 2] = nn.z;
+	}
+	if (n == 0) {
+		err = "no faces in " + path;
+		return false;
+	}
+	return true;
+}
+
+void flatten_bvh(const TriangleSet &ts, const Bvh2 &bvh, DeviceLayout &out) {
+	const int n = static_cast<int>(ts.size());
+	out.nodes.clear();
+	out.tris.assign(static_cast<size_t>(n) * 3, F4{0, 0, 0, 0});
+	out.depth = bvh.depth;
+	// Dense indices for internal nodes, in reference node order.
+	std::vector<int> dense(bvh.nodes.size(), -1);
+	int ni = 0;
+	for (size_t i = 0; i < bvh.nodes.size(); i++)
+		if (bvh.nodes[i].count == 0)
+			dense[i] = ni++;
+	out.internal_count = ni;
+	auto ref_of = [&](int node) -> int {
+		const BvhNode &nd = bvh.nodes[static_cast<size_t>(node)];
+		if (nd.count > 0)
+			return ~((nd.start << 3) | nd.count);
+		return dense[static_cast<size_t>(node)];
+	};
+	auto as_float = [](int i) {
+		float f;
+		std::memcpy(&f, &i, 4);
+		return f;
+	};
+	out.nodes.resize(static_cast<size_t>(ni) * 4);
+	for (size_t i = 0; i < bvh.nodes.size(); i++) {
+		const BvhNode &nd = bvh.nodes[i];
+		if (nd.count > 0)
+			continue;
+		const BvhNode &L = bvh.nodes[static_cast<size_t>(nd.left)];
+		const BvhNode &R = bvh.nodes[static_cast<size_t>(nd.right)];
+		F4 *o = &out.nodes[static_cast<size_t>(dense[i]) * 4];
+		o[0] = {L.bmin.x, L.bmax.x, L.bmin.y, L.bmax.y};
+		o[1] = {R.bmin.x, R.bmax.x, R.bmin.y, R.bmax.y};
+		o[2] = {L.bmin.z, L.bmax.z, R.bmin.z, R.bmax.z};
+		o[3] = {as_float(ref_of(nd.left)), as_float(ref_of(nd.right)), 0.0f, 0.0f};
+	}
+	if (bvh.root >= 0) {
+		const BvhNode &r = bvh.nodes[static_cast<size_t>(bvh.root)];
+		out.root_lo[0] = r.bmin.x;
+		out.root_lo[1] = r.bmin.y;
+		out.root_lo[2] = r.bmin.z;
+		out.root_hi[0] = r.bmax.x;
+		out.root_hi[1] = r.bmax.y;
+		out.root_hi[2] = r.bmax.z;
+		out.root_ref = ref_of(bvh.root);
+	} else {
+		for (int a = 0; a < 3; a++) {
+			out.root_lo[a] = 1.0f;
+			out.root_hi[a] = -1.0f;
+		}
+		out.root_ref = 0;
+	}
+	// Static traversal rank: the reference pushes left then right and pops the
+	// right child first, so leaves are met in that order (src/BVH.cpp:77-111).
+	std::vector<int> rank_of_pos(static_cast<size_t>(n), 0);
+	if (bvh.root >= 0) {
+		std::vector<int> st;
+		st.push_back(bvh.root);
+		int next = 0;
+		while (!st.empty()) {
+			int k = st.back();
+			st.pop_back();
+			const BvhNode &nd = bvh.nodes[static_cast<size_t>(k)];
+			if (nd.count > 0) {
+				for (int p = nd.start; p < nd.start + nd.count; p++)
+					rank_of_pos[static_cast<size_t>(p)] = next++;
+			} else {
+				st.push_back(nd.left);
+				st.push_back(nd.right);
+			}
+		}
+	}
+	for (int p = 0; p < n; p++) {
+		const int ti = bvh.order[static_cast<size_t>(p)];
+		const float *t = &ts.v[9 * static_cast<size_t>(ti)];
+		F4 *o = &out.tris[3 * static_cast<size_t>(p)];
+		o[0] = {t[0], t[1], t[2], as_float(ti)};
+		o[1] = {t[3] - t[0], t[4] - t[1], t[5] - t[2], as_float(rank_of_pos[static_cast<size_t>(p)])};
+		o[2] = {t[6] - t[0], t[7] - t[1], t[8] - t[2], 0.0f};
+	}
+}
+
+} // namespace rnb

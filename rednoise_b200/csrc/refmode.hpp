@@ -1,0 +1,58 @@
+// Parameters of the reference-mode renderer (renderPathTraced semantics).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "traverse.cuh"
+
+namespace rnb {
+
+// Light types, same order as the reference's LightType (src/Light.h:8).
+enum RefLightType : int {
+	kLightPoint = 0,
+	kLightDirectional = 1,
+	kLightSpot = 2,
+	kLightVolume = 3,
+	kLightRectangle = 4,
+	kLightTriangle = 5,
+};
+
+// Mirrors the fields of the reference Light (src/Light.h:13-29).
+struct RefLight {
+	int type;
+	float position[3];
+	float direction[3];
+	float colour[3];
+	float intensity;
+	float radius;
+	float cone_cos;
+	float atten_constant, atten_linear, atten_quadratic;
+	float u_axis[3];
+	float v_axis[3];
+};
+
+constexpr int kMaxRefLights = 16;
+constexpr int kMaxRefDepth = 15;
+
+struct RefParams {
+	int width, height;
+	float position[3];
+	float orient[9]; // camera axes right, up, backward (glm mat3 columns)
+	float f;         // focalLength * scale, in pixels
+	int orthographic;
+	float ortho_scale;
+	int samples;
+	int max_depth;
+	int num_lights;
+	RefLight lights[kMaxRefLights];
+	float aperture, focus_distance;
+	float camera_motion[3];
+	int aperture_blades;
+	int aperture_args_right_to_left;
+};
+
+cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade, const RefParams *d_params, int width,
+                                    int height, uint32_t *argb, float *mean_rgb, int *status, cudaStream_t st);
+
+} // namespace rnb

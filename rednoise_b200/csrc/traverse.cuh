@@ -1,0 +1,337 @@
+// Ray traversal of the flattened reference BVH on sm_100a.
+//
+// Arithmetic contract: every operation on the closest-hit/any-hit path is an
+// explicitly rounded IEEE single-precision op (__fadd_rn/__fsub_rn/__fmul_rn/
+// __fdiv_rn never contract into FMA), evaluated in the order of the reference:
+//   * slab test             src/BVH.cpp:66-75
+//   * ray/triangle test     src/Geometry.cpp:11-25, which solves
+//                           inverse(mat3(-d, e0, e1)) * (o - v0) with glm's
+//                           determinant / inverse / mat3*vec3 expression order
+//                           (third_party/glm/detail/func_matrix.inl:253-344,
+//                            detail/type_mat3x3.inl:468-474)
+// so t, u, v and the accept/reject decision are bit-identical to the reference.
+//
+// Two closest-hit traversal orders share that arithmetic:
+//   * kOrderReference: the reference's depth-first order (push left, push right,
+//     pop right first) with its strict `tenter < closest` pruning, so the hit is
+//     the reference's hit by construction (src/BVH.cpp:77-111).
+//   * kOrderNearest: nearer child first, `tenter <= closest` pruning and ties on
+//     t broken by the triangle's rank in the reference's static order, which
+//     returns the same (t, rank)-minimal hit whenever the float slab test is
+//     conservative for the hit triangle.
+// Any-hit (src/BVH.cpp:113-139) is order independent on a fixed tree: the set of
+// reachable leaves depends only on the slab tests against the fixed maxDistance.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rnb {
+
+constexpr int kStack = 64; // same bound as the reference's int stack[64]
+
+struct SceneView {
+	const float4 *__restrict__ nodes; // 4 float4 per internal node
+	const float4 *__restrict__ tris;  // 3 float4 per triangle position
+	float root_lo[3];
+	float root_hi[3];
+	int root_ref;
+	int n_tris;
+};
+
+struct RayPre {
+	float ox, oy, oz;
+	float dx, dy, dz;
+	float ix, iy, iz;    // 1 / d, IEEE division (glm: 1.0f / direction)
+	float ndx, ndy, ndz; // -d
+};
+
+enum TraversalOrder : int { kOrderReference = 0, kOrderNearest = 1 };
+
+struct HitRec {
+	int idx;  // original triangle index, -1 on a miss
+	int rank; // rank in the reference's static traversal order
+	float t, u, v;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ RayPre make_ray(float ox, float oy, float oz, float dx, float dy, float dz) {
+	RayPre r;
+	r.ox = ox;
+	r.oy = oy;
+	r.oz = oz;
+	r.dx = dx;
+	r.dy = dy;
+	r.dz = dz;
+	r.ix = __fdiv_rn(1.0f, dx);
+	r.iy = __fdiv_rn(1.0f, dy);
+	r.iz = __fdiv_rn(1.0f, dz);
+	r.ndx = -dx;
+	r.ndy = -dy;
+	r.ndz = -dz;
+	return r;
+}
+
+// Slab test split into its tMax-independent part (returned) and tenter, so the
+// `tenter < tMax` half can be applied when the node is popped, exactly where
+// the reference applies it. Min/max keep glm's and std::min/max({...})'s
+// comparison order (NaN and signed-zero behaviour included).
+__device__ __forceinline__ bool slab(float lox, float hix, float loy, float hiy, float loz, float hiz,
+                                     const RayPre &r, float &tenter) {
+	const float t0x = __fmul_rn(__fsub_rn(lox, r.ox), r.ix);
+	const float t1x = __fmul_rn(__fsub_rn(hix, r.ox), r.ix);
+	const float t0y = __fmul_rn(__fsub_rn(loy, r.oy), r.iy);
+	const float t1y = __fmul_rn(__fsub_rn(hiy, r.oy), r.iy);
+	const float t0z = __fmul_rn(__fsub_rn(loz, r.oz), r.iz);
+	const float t1z = __fmul_rn(__fsub_rn(hiz, r.oz), r.iz);
+	const float sx = (t1x < t0x) ? t1x : t0x;
+	const float sy = (t1y < t0y) ? t1y : t0y;
+	const float sz = (t1z < t0z) ? t1z : t0z;
+	const float bx = (t0x < t1x) ? t1x : t0x;
+	const float by = (t0y < t1y) ? t1y : t0y;
+	const float bz = (t0z < t1z) ? t1z : t0z;
+	float te = sx;
+	if (te < sy)
+		te = sy;
+	if (te < sz)
+		te = sz;
+	float tx = bx;
+	if (by < tx)
+		tx = by;
+	if (bz < tx)
+		tx = bz;
+	const float m0 = (te < 0.0f) ? 0.0f : te;
+	tenter = te;
+	return tx >= m0;
+}
+
+// Reference ray/triangle test on a stored (v0, e0 = v1 - v0, e1 = v2 - v0)
+// record; e0/e1 were computed on the host with the same IEEE subtraction the
+// reference performs at test time, so they carry the same bits.
+__device__ __forceinline__ bool tri_test(const float4 a, const float4 b, const float4 c, const RayPre &r, float &t,
+                                         float &u, float &v) {
+	const float spx = __fsub_rn(r.ox, a.x);
+	const float spy = __fsub_rn(r.oy, a.y);
+	const float spz = __fsub_rn(r.oz, a.z);
+	// mat3(m0 = -d, m1 = e0, m2 = e1); cofactors named after glm's expressions.
+	const float c00 = __fsub_rn(__fmul_rn(b.y, c.z), __fmul_rn(c.y, b.z));     // m11*m22 - m21*m12
+	const float A = __fsub_rn(__fmul_rn(r.ndy, c.z), __fmul_rn(c.y, r.ndz));   // m01*m22 - m21*m02
+	const float B = __fsub_rn(__fmul_rn(r.ndy, b.z), __fmul_rn(b.y, r.ndz));   // m01*m12 - m11*m02
+	const float det = __fadd_rn(__fsub_rn(__fmul_rn(r.ndx, c00), __fmul_rn(b.x, A)), __fmul_rn(c.x, B));
+	if (fabsf(det) < 1e-8f)
+		return false;
+	const float k = __fdiv_rn(1.0f, det);
+	// Row 1 of the inverse gives u.
+	const float i01 = __fmul_rn(-A, k);
+	const float i11 = __fmul_rn(__fsub_rn(__fmul_rn(r.ndx, c.z), __fmul_rn(c.x, r.ndz)), k);
+	const float i21 = __fmul_rn(-__fsub_rn(__fmul_rn(r.ndx, c.y), __fmul_rn(c.x, r.ndy)), k);
+	u = __fadd_rn(__fadd_rn(__fmul_rn(i01, spx), __fmul_rn(i11, spy)), __fmul_rn(i21, spz));
+	if (!(u >= 0.0f))
+		return false;
+	const float i02 = __fmul_rn(B, k);
+	const float i12 = __fmul_rn(-__fsub_rn(__fmul_rn(r.ndx, b.z), __fmul_rn(b.x, r.ndz)), k);
+	const float i22 = __fmul_rn(__fsub_rn(__fmul_rn(r.ndx, b.y), __fmul_rn(b.x, r.ndy)), k);
+	v = __fadd_rn(__fadd_rn(__fmul_rn(i02, spx), __fmul_rn(i12, spy)), __fmul_rn(i22, spz));
+	if (!(v >= 0.0f) || !(__fadd_rn(u, v) <= 1.0f))
+		return false;
+	const float i00 = __fmul_rn(c00, k);
+	const float i10 = __fmul_rn(-__fsub_rn(__fmul_rn(b.x, c.z), __fmul_rn(c.x, b.z)), k);
+	const float i20 = __fmul_rn(__fsub_rn(__fmul_rn(b.x, c.y), __fmul_rn(c.x, b.y)), k);
+	t = __fadd_rn(__fadd_rn(__fmul_rn(i00, spx), __fmul_rn(i10, spy)), __fmul_rn(i20, spz));
+	return t > 1e-5f;
+}
+
+__device__ __forceinline__ int leaf_start(int ref) { return (~ref) >> 3; }
+__device__ __forceinline__ int leaf_count(int ref) { return (~ref) & 7; }
+
+// Closest hit. `ignore` is an original triangle index to skip (-1 = none).
+// `err` is set to 1 if the stack bound would be exceeded (the host rejects
+// trees deeper than the bound, so this only reports corrupted input).
+template <int kOrder>
+__device__ __forceinline__ HitRec trace_closest(const SceneView &s, const RayPre &r, int ignore, int &err) {
+	HitRec h;
+	h.idx = -1;
+	h.rank = 0x7fffffff;
+	h.t = __int_as_float(0x7f800000);
+	h.u = 0.0f;
+	h.v = 0.0f;
+	int st_ref[kStack];
+	float st_t[kStack];
+	int sp = 0;
+	float te;
+	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te)) {
+		st_ref[0] = s.root_ref;
+		st_t[0] = te;
+		sp = 1;
+	}
+	while (sp > 0) {
+		--sp;
+		int ref = st_ref[sp];
+		const float tent = st_t[sp];
+		if (kOrder == kOrderReference) {
+			if (!(tent < h.t))
+				continue;
+		} else {
+			if (tent > h.t)
+				continue;
+		}
+		// Descend through internal nodes until a leaf is reached.
+		while (ref >= 0) {
+			const float4 *nd = s.nodes + 4 * static_cast<size_t>(ref);
+			const float4 n0 = __ldg(nd + 0);
+			const float4 n1 = __ldg(nd + 1);
+			const float4 n2 = __ldg(nd + 2);
+			const float4 n3 = __ldg(nd + 3);
+			float tl, tr;
+			const bool hl = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, r, tl);
+			const bool hr = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, r, tr);
+			const int cl = __float_as_int(n3.x);
+			const int cr = __float_as_int(n3.y);
+			int next = -1;
+			bool have_next = false;
+			if (kOrder == kOrderReference) {
+				// Reference: push left, push right; the right child is popped next and
+				// tested against the (unchanged) closest distance.
+				if (hl) {
+					if (sp >= kStack) {
+						err = 1;
+						return h;
+					}
+					st_ref[sp] = cl;
+					st_t[sp] = tl;
+					++sp;
+				}
+				if (hr && tr < h.t) {
+					next = cr;
+					have_next = true;
+				}
+			} else {
+				const bool vl = hl && !(tl > h.t);
+				const bool vr = hr && !(tr > h.t);
+				if (vl && vr) {
+					// Nearer first; on equal entry distance keep the reference's right-first order.
+					const bool left_first = tl < tr;
+					if (sp >= kStack) {
+						err = 1;
+						return h;
+					}
+					st_ref[sp] = left_first ? cr : cl;
+					st_t[sp] = left_first ? tr : tl;
+					++sp;
+					next = left_first ? cl : cr;
+					have_next = true;
+				} else if (vl) {
+					next = cl;
+					have_next = true;
+				} else if (vr) {
+					next = cr;
+					have_next = true;
+				}
+			}
+			if (!have_next) {
+				ref = 0x7fffffff; // sentinel: nothing to descend into
+				break;
+			}
+			ref = next;
+		}
+		if (ref == 0x7fffffff)
+			continue;
+		// Leaf: test its triangles in ascending order.
+		const int start = leaf_start(ref);
+		const int count = leaf_count(ref);
+		for (int p = start; p < start + count; p++) {
+			const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
+			const float4 a = __ldg(tp + 0);
+			const int ti = __float_as_int(a.w);
+			if (ti == ignore)
+				continue;
+			const float4 b = __ldg(tp + 1);
+			const float4 c = __ldg(tp + 2);
+			float t, u, v;
+			if (!tri_test(a, b, c, r, t, u, v))
+				continue;
+			if (kOrder == kOrderReference) {
+				if (t < h.t) {
+					h.idx = ti;
+					h.t = t;
+					h.u = u;
+					h.v = v;
+					h.rank = __float_as_int(b.w);
+				}
+			} else {
+				const int rk = __float_as_int(b.w);
+				if (t < h.t || (t == h.t && rk < h.rank)) {
+					h.idx = ti;
+					h.t = t;
+					h.u = u;
+					h.v = v;
+					h.rank = rk;
+				}
+			}
+		}
+	}
+	return h;
+}
+
+// Any hit strictly before tmax (the reference's occluded()).
+__device__ __forceinline__ bool trace_any(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err) {
+	int st[kStack];
+	int sp = 0;
+	float te;
+	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te) &&
+	    te < tmax) {
+		st[0] = s.root_ref;
+		sp = 1;
+	}
+	while (sp > 0) {
+		int ref = st[--sp];
+		while (ref >= 0) {
+			const float4 *nd = s.nodes + 4 * static_cast<size_t>(ref);
+			const float4 n0 = __ldg(nd + 0);
+			const float4 n1 = __ldg(nd + 1);
+			const float4 n2 = __ldg(nd + 2);
+			const float4 n3 = __ldg(nd + 3);
+			float tl, tr;
+			const bool hl = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, r, tl) && tl < tmax;
+			const bool hr = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, r, tr) && tr < tmax;
+			const int cl = __float_as_int(n3.x);
+			const int cr = __float_as_int(n3.y);
+			if (hl && hr) {
+				if (sp >= kStack) {
+					err = 1;
+					return false;
+				}
+				const bool left_first = tl < tr;
+				st[sp++] = left_first ? cr : cl;
+				ref = left_first ? cl : cr;
+			} else if (hl) {
+				ref = cl;
+			} else if (hr) {
+				ref = cr;
+			} else {
+				ref = 0x7fffffff;
+				break;
+			}
+		}
+		if (ref == 0x7fffffff)
+			continue;
+		const int start = leaf_start(ref);
+		const int count = leaf_count(ref);
+		for (int p = start; p < start + count; p++) {
+			const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
+			const float4 a = __ldg(tp + 0);
+			if (__float_as_int(a.w) == ignore)
+				continue;
+			const float4 b = __ldg(tp + 1);
+			const float4 c = __ldg(tp + 2);
+			float t, u, v;
+			if (tri_test(a, b, c, r, t, u, v) && t < tmax)
+				return true;
+		}
+	}
+	return false;
+}
+
+#endif // __CUDACC__
+
+} // namespace rnb
