@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark of the path-tracing hot path on B200.
+
+Workload (one step = one full frame): the 1.31M-triangle displaced-icosphere
+Cornell box (seeded synthetic scene, rednoise_b200.scenes.icosphere_scene),
+1920x1080, 64 samples per pixel, max depth 8, Russian roulette from vertex 3,
+physical estimator. Metric: samples/s (whole job). Multi-GPU: weak scaling,
+each rank renders its own 64 samples per pixel (disjoint sample indices) with
+no data-path collective.
+
+  python bench.py [--gpus N --steps K --warmup W]
+  python bench.py --impl reference      # the reference's CPU renderPathTraced
+
+Printed: one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "samples/s (path-traced samples per second)"
+UNIT = "samples/s"
+WORKLOAD = "icosphere-cornell-1.31M-tris 1920x1080 64spp depth8"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--width", type=int, default=1920)
+    p.add_argument("--height", type=int, default=1080)
+    p.add_argument("--spp", type=int, default=64)
+    p.add_argument("--depth", type=int, default=8)
+    p.add_argument("--rr", type=int, default=3)
+    p.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = 1.31M triangles)")
+    p.add_argument("--integrator", default="auto", choices=["auto", "megakernel", "wavefront"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(
+        os.environ.get("WORLD_SIZE", "1"))
+
+
+# ---- clocks sampled during the timed region ------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.rows = []
+        self.proc = None
+        self.index = index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for k, name in enumerate(names):
+                    if r[3 + k].lower().startswith("active"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- CPU baseline: the reference's renderPathTraced (oracle/_ref) ---------------------
+
+def reference_model(sc):
+    import oracle
+
+    return oracle.RefModel.from_arrays(sc["vertices"], sc["ref_rgb"], sc["ref_material"], sc["ref_roughness"])
+
+
+def reference_focal(height: int) -> float:
+    # f = focalLength * 150 pixels gives the 40-degree vertical field of view.
+    return (height / 2.0) / math.tan(math.radians(20.0)) / 150.0
+
+
+def time_reference_step(model, w, h, spp) -> float:
+    from rednoise_b200 import scenes
+
+    t0 = time.perf_counter()
+    model.render(w, h, spp, focal=reference_focal(h), pos=(0.0, 0.0, scenes.CAMERA_Z), target=(0.0, 0.0, 0.0))
+    return time.perf_counter() - t0
+
+
+def reference_window(model, target_s: float):
+    """A frame size (same camera, 16:9) whose 1-spp reference render takes about target_s."""
+    w, h = 160, 90
+    dt = time_reference_step(model, w, h, 1)
+    while dt < target_s / 4 and w < 1920:
+        w, h = w * 2, h * 2
+        dt = time_reference_step(model, w, h, 1)
+    return w, h, dt
+
+
+def cpu_baseline(sc, target_s=12.0) -> dict:
+    model = reference_model(sc)
+    w, h, _ = reference_window(model, target_s)
+    total, samples, steps = 0.0, 0, 0
+    while total < target_s:
+        total += time_reference_step(model, w, h, 1)
+        samples += w * h
+        steps += 1
+    return {"value": samples / total, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"reference renderPathTraced (oracle/_ref, OpenMP, reference semantics: depth 4, default light)"
+                      f" on the same 1.31M-triangle geometry and camera, {steps} x {w}x{h} frames at 1 spp"
+                      f" ({samples} samples, {total:.1f} s, BVH rebuilt per call as the reference does)"}
+
+
+def run_reference_arm(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    from rednoise_b200 import scenes
+
+    sc = scenes.icosphere_scene(level=args.level)
+    model = reference_model(sc)
+    w, h, _ = reference_window(model, 4.0)
+    for _ in range(args.warmup):
+        time_reference_step(model, w, h, 1)
+    dts = [time_reference_step(model, w, h, 1) for _ in range(args.steps)]
+    total = sum(dts)
+    value = w * h * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "reference_step": f"{w}x{h} at 1 spp (bounded sample of the frame)",
+                   "semantics": "reference renderPathTraced: depth 4, default disk light, 8-bit output"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"{args.steps} steps of {w}x{h} at 1 spp"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm -----------------------------------------------------------------------
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.isfile(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per sample of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.isfile(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+def run_ours(args):
+    import torch
+
+    import rednoise_b200 as rn
+    from rednoise_b200 import _native, scenes
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    sc = scenes.icosphere_scene(level=args.level)
+    scene = rn.Scene.from_arrays(sc["vertices"], albedo=sc["albedo"], emission=sc["emission"],
+                                 material=sc["material"], material_param=sc["material_param"])
+    scene.prepare()
+    info = scene.info()
+    W, H, spp = args.width, args.height, args.spp
+    c = scenes.camera(W, H)
+    cam = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], W, H)
+    integ = {"auto": 0, "megakernel": 1, "wavefront": 2}[args.integrator]
+    lib = _native.load()
+    stream = torch.cuda.Stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    out = torch.empty(H * W * 3, dtype=torch.float32, device="cuda")
+    l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    flags = _native.RN_PT_DEVICE_POINTERS | _native.RN_PT_ORDER_NEAREST
+    step_counter = [0]
+
+    def settings():
+        k = step_counter[0]
+        step_counter[0] += 1
+        return rn.Settings.make(spp=spp, max_depth=args.depth, rr_depth=args.rr, integrator=integ, seed=1,
+                                sample_offset=(k * world + rank) * spp)
+
+    def render(st):
+        _native.check(lib.rn_pt_render(scene.handle, ctypes.byref(cam), ctypes.byref(st), flags, sptr,
+                                       ctypes.c_void_p(out.data_ptr())), "rn_pt_render")
+
+    # Algorithmic bytes per sample: reference-order traversal counters on the GPU.
+    counts = scene.count_traversal(cam, rn.Settings.make(spp=1, max_depth=args.depth, rr_depth=args.rr, seed=99))
+    bytes_per_sample = (24.0 * (counts["closest_boxes"] + counts["any_boxes"]) +
+                        36.0 * (counts["closest_tris"] + counts["any_tris"])) / counts["samples"]
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            l2.zero_()
+            render(settings())
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        clocks = ClockSampler(local_rank)
+        clocks.start()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for i in range(args.steps):
+            l2.zero_()
+            ev[i][0].record(stream)
+            render(settings())
+            ev[i][1].record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    render_ms = [a.elapsed_time(b) for a, b in ev]
+    if dist:
+        t = torch.tensor([total_ms, max(render_ms)], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, max_render = float(t[0]), float(t[1])
+    ms_per_step = total_ms / args.steps
+    samples_per_step = W * H * spp
+    value = world * samples_per_step / (ms_per_step / 1e3)
+
+    # End to end through the C ABI with host buffers: pinned host output, D2H inside the timed region.
+    host = torch.empty(H * W * 3, dtype=torch.float32, pin_memory=True)
+    hflags = _native.RN_PT_ORDER_NEAREST
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        st = settings()
+        _native.check(lib.rn_pt_render(scene.handle, ctypes.byref(cam), ctypes.byref(st), hflags, None,
+                                       ctypes.c_void_p(host.data_ptr())), "rn_pt_render (host)")
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t[0])
+    e2e_value = world * samples_per_step / e2e_s
+
+    # RMSE of one frame against the FP64 reference on its pixel subset (when available).
+    rmse = None
+    ref_path = os.path.join(ROOT, "tests", "golden", "fp64_ref.npz")
+    if os.path.isfile(ref_path) and (W, H, args.depth, args.rr) == (1920, 1080, 8, 3) and args.level == 8:
+        ref = np.load(ref_path)
+        px = ref["c2_pixels"]
+        img = host.numpy().reshape(-1, 3)[px].astype(np.float64)
+        mref = ref["c2_mean"]
+        rmse = float(np.sqrt(((img - mref) ** 2).mean()) / max(np.sqrt((mref ** 2).mean()), 1e-30))
+
+    peak, peak_kind = measured_peaks()
+    kernel_ms = float(np.mean(render_ms))
+    achieved = bytes_per_sample * samples_per_step / (kernel_ms / 1e3) / 1e9
+    tr = profiled_traffic()
+    traffic = None
+    if tr and tr.get("bytes_per_sample"):
+        traffic = tr["bytes_per_sample"] * samples_per_step
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": spp, "max_depth": args.depth,
+                   "rr_depth": args.rr, "triangles": info["num_triangles"], "integrator": args.integrator,
+                   "traversal": "nearest-first, reference arithmetic", "l2": "flushed (256 MB write) before each step",
+                   "parallelism": f"{world} independent ranks, disjoint sample indices"},
+        "gpu_launches": 2 * args.steps,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ctypes.sizeof(cam) + ctypes.sizeof(st),
+                "d2h_bytes_per_step": H * W * 3 * 4, "api": "rn_pt_render with host output buffer"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": traffic,
+                     "bytes_per_sample": bytes_per_sample,
+                     "algorithmic": "24 B per node-box test + 36 B per triangle test of the reference-order "
+                                    "traversal, counted on the GPU for 1 spp of the same frame",
+                     "kernel_ms": kernel_ms},
+        "clocks": clk,
+        "rmse_vs_fp64_64spp": rmse,
+        "scene_build_ms": info["build_ms"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sc)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

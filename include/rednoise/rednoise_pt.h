@@ -145,6 +145,58 @@ void rn_pt_ref_params_init(rn_pt_ref_params *p, int width, int height, float cam
 rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *params, unsigned flags, void *stream,
                                  uint32_t *argb, float *mean_rgb);
 
+/* ---- physical-mode rendering (the additive path-tracing estimator) ---- */
+
+/* Pinhole camera looking from `position` at `target`, vertical field of view. */
+typedef struct {
+	float position[3];
+	float target[3];
+	float up[3];
+	float vfov_deg;
+	int width, height;
+} rn_pt_camera;
+
+#define RN_PT_AUTO 0
+#define RN_PT_MEGAKERNEL 1
+#define RN_PT_WAVEFRONT 2
+
+/* spp samples per pixel, indices [sample_offset, sample_offset + spp); paths
+ * have at most max_depth scattering vertices; Russian roulette from vertex
+ * rr_depth (>= max_depth disables it); env is the radiance of escaping rays. */
+typedef struct {
+	int spp;
+	int max_depth;
+	int rr_depth;
+	int integrator; /* RN_PT_AUTO / RN_PT_MEGAKERNEL / RN_PT_WAVEFRONT */
+	unsigned long long seed;
+	unsigned sample_offset;
+	float env[3];
+} rn_pt_settings;
+
+/* Render and write the per-pixel mean radiance (width*height*3 floats, RGB,
+ * row-major, top row first) to rgb. Next-event estimation to emissive triangles,
+ * Lambert / GGX / dielectric sampling and Russian roulette (rednoise_b200's
+ * physical estimator; the reference's renderPathTraced loop structure,
+ * src/Renderer.cpp:1119-1170, with float accumulation instead of 8 bits). */
+rn_status rn_pt_render(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings, unsigned flags,
+                       void *stream, float *rgb);
+
+/* Add the per-pixel SUM of samples [sample_offset, sample_offset + spp) to
+ * accum (width*height*3 floats, read and written). Samples are added in index
+ * order, so splitting a render over calls reproduces one call bit for bit (a
+ * resumable progressive render). */
+rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
+                                  unsigned flags, void *stream, float *accum);
+
+/* Profiling counters of the reference traversal algorithm (src/BVH.cpp:77-139,
+ * box tests counted when a node is popped) over the rays of one render with
+ * these settings: counters[7] = samples, closest queries, any-hit queries,
+ * closest box tests, closest triangle tests, any-hit box tests, any-hit
+ * triangle tests. 24 B per box test and 36 B per triangle test are the
+ * algorithmic bytes of a query. */
+rn_status rn_pt_count_traversal(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
+                                long long *counters);
+
 /* Message for the last failure on this thread ("" if none). */
 const char *rn_pt_last_error(void);
 

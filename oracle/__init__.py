@@ -82,6 +82,11 @@ def orc() -> ctypes.CDLL:
             "orc_occluded": (None, [vp, ci, vp, vp, vp, vp, vp, vp, vp]),
             "orc_render_reference": (None, [vp, vp, vp, vp, vp, ci, ci, ci, ci, cf, vp, vp, ci, ci, ci, vp, vp,
                                             vp]),
+            "orc_pt_scene_new": (vp, [ci, vp, vp, vp, vp, vp]),
+            "orc_pt_scene_free": (None, [vp]),
+            "orc_pt_render": (None, [vp, vp, ci, ci, ci, ci, ci, ctypes.c_ulonglong, ctypes.c_uint, vp, ci, vp, ci,
+                                     vp]),
+            "orc_pt_count": (None, [vp, vp, ci, ci, ci, ci, ci, ctypes.c_ulonglong, ctypes.c_uint, vp, ci, vp, vp]),
         }
         for k, (r, a) in sig.items():
             getattr(lib, k).restype = r
@@ -181,7 +186,7 @@ class RefModel:
         pos = np.asarray(pos, np.float32)
         target = np.asarray(target, np.float32)
         motion = np.asarray(motion, np.float32)
-        lt = None if not lights else np.ascontiguousarray(lights, np.float32).reshape(-1, 24)
+        lt = None if lights is None or len(lights) == 0 else np.ascontiguousarray(lights, np.float32).reshape(-1, 24)
         out = np.zeros((h, w), np.uint32)
         ref().refsh_render_pathtraced(self.h, w, h, focal, P(pos), P(target), samples,
                                       0 if lt is None else lt.shape[0], P(lt), aperture, focus, P(motion), blades,
@@ -253,7 +258,7 @@ class OrcBvh:
         rough = np.ascontiguousarray(roughness, np.float32)
         pos = np.asarray(pos, np.float32)
         target = np.asarray(target, np.float32)
-        lt = None if not lights else np.ascontiguousarray(lights, np.float32).reshape(-1, 24)
+        lt = None if lights is None or len(lights) == 0 else np.ascontiguousarray(lights, np.float32).reshape(-1, 24)
         out = np.zeros((y1 - y0, w), np.uint32)
         mean = np.zeros((y1 - y0, w, 3), np.float32) if want_mean else None
         orc().orc_render_reference(self.h, P(nrm), P(mat), P(col), P(rough), w, h, y0, y1, focal, P(pos), P(target),
@@ -263,5 +268,49 @@ class OrcBvh:
     def __del__(self):
         try:
             orc().orc_bvh_free(self.h)
+        except Exception:
+            pass
+
+
+class OrcPhysScene:
+    """The oracle restatement of the physical estimator over a scene dict
+    (vertices, albedo, emission, material, material_param)."""
+
+    def __init__(self, sc: dict):
+        self._keep = [np.ascontiguousarray(sc["vertices"], np.float32), np.ascontiguousarray(sc["albedo"], np.float32),
+                      np.ascontiguousarray(sc["emission"], np.float32), np.ascontiguousarray(sc["material"], np.int32),
+                      np.ascontiguousarray(sc["material_param"], np.float32)]
+        v, a, e, m, p = self._keep
+        self.h = orc().orc_pt_scene_new(v.shape[0], P(v), P(a), P(e), P(m), P(p))
+
+    def render_sums(self, cam: dict, spp: int, max_depth: int, rr_depth: int, seed: int, offset: int = 0,
+                    env=(0.0, 0.0, 0.0), pixels=None, double: bool = False) -> np.ndarray:
+        """Per-pixel radiance SUMS over samples [offset, offset + spp), float64 (n, 3)."""
+        c10 = np.array(list(cam["position"]) + list(cam["target"]) + list(cam["up"]) + [cam["vfov_deg"]], np.float32)
+        envv = np.asarray(env, np.float32)
+        w, h = cam["width"], cam["height"]
+        px = None if pixels is None else np.ascontiguousarray(pixels, np.int32)
+        n = w * h if px is None else px.size
+        out = np.zeros((n, 3), np.float64)
+        orc().orc_pt_render(self.h, P(c10), w, h, spp, max_depth, rr_depth, seed, offset, P(envv),
+                            0 if px is None else px.size, P(px), 1 if double else 0, P(out))
+        return out
+
+    def count_queries(self, cam: dict, spp: int, max_depth: int, rr_depth: int, seed: int, offset: int = 0,
+                      env=(0.0, 0.0, 0.0), pixels=None) -> dict:
+        """Reference-order query counts of the FP32 estimator on the listed pixels:
+        closest / any-hit queries and their node-box and triangle tests."""
+        c10 = np.array(list(cam["position"]) + list(cam["target"]) + list(cam["up"]) + [cam["vfov_deg"]], np.float32)
+        envv = np.asarray(env, np.float32)
+        px = None if pixels is None else np.ascontiguousarray(pixels, np.int32)
+        out = np.zeros(6, np.int64)
+        orc().orc_pt_count(self.h, P(c10), cam["width"], cam["height"], spp, max_depth, rr_depth, seed, offset,
+                           P(envv), 0 if px is None else px.size, P(px), P(out))
+        keys = ("closest", "any", "closest_boxes", "closest_tris", "any_boxes", "any_tris")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def __del__(self):
+        try:
+            orc().orc_pt_scene_free(self.h)
         except Exception:
             pass

@@ -503,6 +503,351 @@ V3 path_trace(const RefScene &s, V3 o, V3 d, int depth, Rng &rng) {
 	return direct + albedo * path_trace(s, p + 1e-4f * bnc, bnc, depth - 1, rng);
 }
 
+
+// ---- physical-mode estimator (templated on the float type) ----------------------
+// Restates rednoise_b200's physical estimator (rednoise_b200/csrc/physical.cuh):
+// same camera, counter-based uniforms, BSDFs, MIS and roulette. With T = float the
+// closest hits come from the reference-exact traversal above; with T = double the
+// same BVH is traversed with a double-precision Moller-Trumbore test.
+
+template <typename T> struct X3 {
+	T x, y, z;
+};
+template <typename T> inline X3<T> x3(T a, T b, T c) { return {a, b, c}; }
+template <typename T> inline X3<T> operator+(X3<T> a, X3<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <typename T> inline X3<T> operator-(X3<T> a, X3<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <typename T> inline X3<T> operator-(X3<T> a) { return {-a.x, -a.y, -a.z}; }
+template <typename T> inline X3<T> operator*(X3<T> a, X3<T> b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+template <typename T> inline X3<T> operator*(X3<T> a, T s) { return {a.x * s, a.y * s, a.z * s}; }
+template <typename T> inline T dt(X3<T> a, X3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <typename T> inline X3<T> cr(X3<T> a, X3<T> b) {
+	return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <typename T> inline X3<T> nz(X3<T> a) { return a * (T(1) / std::sqrt(dt(a, a))); }
+template <typename T> inline T mx(X3<T> a) { return std::max(a.x, std::max(a.y, a.z)); }
+
+struct PhysScene {
+	Bvh bvh;
+	std::vector<float> albedo, emission, param, normal; // 3, 3, 1, 3 per triangle
+	std::vector<int> material;
+	struct Em {
+		float v0[3], e0[3], e1[3];
+		float area, cdf;
+		int tri;
+	};
+	std::vector<Em> em;
+	float area_total = 0.0f;
+};
+
+struct PhysCam {
+	float pos[3], fwd[3], right[3], up[3];
+	float tan_half, aspect;
+	int w, h;
+};
+
+struct PhysSet {
+	int spp, max_depth, rr_depth;
+	uint64_t seed;
+	uint32_t offset;
+	float env[3];
+};
+
+inline orc::U4 prand(uint64_t seed, uint32_t pix, uint32_t s, uint32_t block) {
+	return orc::philox4x32_10(orc::U4{pix, s, block, 0u}, static_cast<uint32_t>(seed),
+	                          static_cast<uint32_t>(seed >> 32));
+}
+
+template <typename T> struct PHit {
+	int idx = -1;
+	T t = T(0);
+};
+
+// Double-precision closest hit over the same tree (nearest-first not needed: full DFS).
+PHit<double> closest_d(const PhysScene &s, X3<double> o, X3<double> d, int ignore) {
+	PHit<double> h;
+	h.t = INFINITY;
+	const Bvh &b = s.bvh;
+	if (b.root < 0)
+		return h;
+	X3<double> inv = x3(1.0 / d.x, 1.0 / d.y, 1.0 / d.z);
+	int st[64], sp = 0;
+	st[sp++] = b.root;
+	while (sp > 0) {
+		const Node &n = b.nodes[st[--sp]];
+		double t0x = (n.bmin.x - o.x) * inv.x, t1x = (n.bmax.x - o.x) * inv.x;
+		double t0y = (n.bmin.y - o.y) * inv.y, t1y = (n.bmax.y - o.y) * inv.y;
+		double t0z = (n.bmin.z - o.z) * inv.z, t1z = (n.bmax.z - o.z) * inv.z;
+		double te = std::max(std::max(std::min(t0x, t1x), std::min(t0y, t1y)), std::min(t0z, t1z));
+		double tx = std::min(std::min(std::max(t0x, t1x), std::max(t0y, t1y)), std::max(t0z, t1z));
+		if (std::isnan(te) || std::isnan(tx))
+			te = 0, tx = INFINITY; // degenerate slab: visit conservatively
+		if (!(tx >= std::max(te, 0.0) * (1 - 1e-9) && te <= h.t))
+			continue;
+		if (n.count > 0) {
+			for (int i = n.start; i < n.start + n.count; i++) {
+				int ti = b.order[i];
+				if (ti == ignore)
+					continue;
+				const Tri &tr = b.tris[ti];
+				X3<double> v0 = x3<double>(tr.v0.x, tr.v0.y, tr.v0.z);
+				X3<double> e1 = x3<double>(tr.v1.x, tr.v1.y, tr.v1.z) - v0;
+				X3<double> e2 = x3<double>(tr.v2.x, tr.v2.y, tr.v2.z) - v0;
+				X3<double> p = cr(d, e2);
+				double det = dt(e1, p);
+				if (std::fabs(det) < 1e-18)
+					continue;
+				double id = 1.0 / det;
+				X3<double> tv = o - v0;
+				double u = dt(tv, p) * id;
+				if (u < 0 || u > 1)
+					continue;
+				X3<double> q = cr(tv, e1);
+				double v = dt(d, q) * id;
+				if (v < 0 || u + v > 1)
+					continue;
+				double t = dt(e2, q) * id;
+				if (t > 1e-5 && t < h.t) {
+					h.t = t;
+					h.idx = ti;
+				}
+			}
+		} else {
+			st[sp++] = n.left;
+			st[sp++] = n.right;
+		}
+	}
+	return h;
+}
+
+bool occluded_d(const PhysScene &s, X3<double> o, X3<double> d, double tmax, int ignore) {
+	PHit<double> h = closest_d(s, o, d, ignore);
+	return h.idx >= 0 && h.t < tmax;
+}
+
+// Optional per-thread counters of the reference-order queries (algorithmic bytes).
+struct QueryCounts {
+	long closest = 0, any = 0;
+	Counts cb, ab;
+};
+thread_local QueryCounts *g_qc = nullptr;
+
+template <typename T> PHit<T> closest_t(const PhysScene &s, X3<T> o, X3<T> d, int ignore);
+template <> PHit<float> closest_t<float>(const PhysScene &s, X3<float> o, X3<float> d, int ignore) {
+	if (g_qc)
+		g_qc->closest++;
+	Hit h = intersect(s.bvh, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), ignore, g_qc ? &g_qc->cb : nullptr);
+	PHit<float> r;
+	r.idx = h.hit ? h.idx : -1;
+	r.t = h.t;
+	return r;
+}
+template <> PHit<double> closest_t<double>(const PhysScene &s, X3<double> o, X3<double> d, int ignore) {
+	return closest_d(s, o, d, ignore);
+}
+template <typename T> bool occluded_t(const PhysScene &s, X3<T> o, X3<T> d, T tmax, int ignore);
+template <> bool occluded_t<float>(const PhysScene &s, X3<float> o, X3<float> d, float tmax, int ignore) {
+	if (g_qc)
+		g_qc->any++;
+	return occluded(s.bvh, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), tmax, ignore, g_qc ? &g_qc->ab : nullptr);
+}
+template <> bool occluded_t<double>(const PhysScene &s, X3<double> o, X3<double> d, double tmax, int ignore) {
+	return occluded_d(s, o, d, tmax, ignore);
+}
+
+template <typename T> void onb_t(X3<T> n, X3<T> &t, X3<T> &b) {
+	T sign = std::copysign(T(1), n.z);
+	T a = T(-1) / (sign + n.z);
+	T bb = n.x * n.y * a;
+	t = x3(T(1) + sign * n.x * n.x * a, sign * bb, -sign * n.x);
+	b = x3(bb, sign + n.y * n.y * a, -n.y);
+}
+template <typename T> T ggx_D_t(T cm, T a2) {
+	T k = cm * cm * (a2 - 1) + 1;
+	return a2 / (T(3.14159265358979323846) * k * k);
+}
+template <typename T> T ggx_L_t(T c, T a2) {
+	T c2 = c * c;
+	T t2 = std::max(T(0), 1 - c2) / std::max(c2, T(1e-12));
+	return T(0.5) * (-1 + std::sqrt(1 + a2 * t2));
+}
+template <typename T> X3<T> schlick_t(X3<T> f0, T c) {
+	T m = std::min(std::max(1 - c, T(0)), T(1));
+	T m5 = (m * m) * (m * m) * m;
+	return f0 + (x3<T>(1, 1, 1) - f0) * m5;
+}
+template <typename T> bool eval_t(int mat, X3<T> alb, T alpha, X3<T> n, X3<T> wo, X3<T> wi, X3<T> &fc, T &pdf) {
+	T ci = dt(n, wi), co = dt(n, wo);
+	if (ci <= 0 || co <= 0)
+		return false;
+	const T inv_pi = T(0.318309886183790671537767526745);
+	if (mat == 0) {
+		fc = alb * (ci * inv_pi);
+		pdf = ci * inv_pi;
+		return true;
+	}
+	T a2 = alpha * alpha;
+	X3<T> m = nz(wo + wi);
+	T cm = dt(n, m), om = dt(wo, m);
+	if (cm <= 0 || om <= 0)
+		return false;
+	T D = ggx_D_t(cm, a2), lo = ggx_L_t(co, a2), li = ggx_L_t(ci, a2);
+	T G2 = 1 / (1 + lo + li), G1 = 1 / (1 + lo);
+	fc = schlick_t(alb, om) * (D * G2 / (4 * co));
+	pdf = G1 * D / (4 * co);
+	return true;
+}
+template <typename T> T mis_t(T a, T b) { return a * a / (a * a + b * b); }
+
+template <typename T> X3<T> trace_phys(const PhysScene &s, const PhysCam &c, const PhysSet &st, uint32_t pix,
+                                       uint32_t sample) {
+	const T two_pi = T(6.28318530717958647692);
+	orc::U4 r0 = prand(st.seed, pix, sample, 0);
+	int px = static_cast<int>(pix % static_cast<uint32_t>(c.w)), py = static_cast<int>(pix / static_cast<uint32_t>(c.w));
+	T sx = ((T(px) + T(orc::u01(r0.x))) / T(c.w)) * 2 - 1;
+	T sy = 1 - ((T(py) + T(orc::u01(r0.y))) / T(c.h)) * 2;
+	X3<T> fwd = x3<T>(c.fwd[0], c.fwd[1], c.fwd[2]), right = x3<T>(c.right[0], c.right[1], c.right[2]),
+	      up = x3<T>(c.up[0], c.up[1], c.up[2]);
+	X3<T> o = x3<T>(c.pos[0], c.pos[1], c.pos[2]);
+	X3<T> d = nz(fwd + right * (sx * T(c.tan_half) * T(c.aspect)) + up * (sy * T(c.tan_half)));
+	X3<T> beta = x3<T>(1, 1, 1), L = x3<T>(0, 0, 0);
+	T prev_pdf = 0;
+	int ignore = -1;
+	const T eps = T(2e-4);
+	for (int bounce = 0;; bounce++) {
+		PHit<T> h = closest_t<T>(s, o, d, ignore);
+		if (h.idx < 0) {
+			L = L + beta * x3<T>(st.env[0], st.env[1], st.env[2]);
+			break;
+		}
+		size_t k = static_cast<size_t>(h.idx);
+		X3<T> ng = x3<T>(s.normal[3 * k], s.normal[3 * k + 1], s.normal[3 * k + 2]);
+		X3<T> p = o + d * h.t;
+		X3<T> wo = -d;
+		T cog = dt(ng, wo);
+		X3<T> Le = x3<T>(s.emission[3 * k], s.emission[3 * k + 1], s.emission[3 * k + 2]);
+		if (Le.x > 0 || Le.y > 0 || Le.z > 0) {
+			if (cog > 0) {
+				T w = 1;
+				if (prev_pdf > 0)
+					w = mis_t(prev_pdf, h.t * h.t / (cog * T(s.area_total)));
+				L = L + beta * Le * w;
+			}
+			break;
+		}
+		int mat = s.material[k];
+		X3<T> alb = x3<T>(s.albedo[3 * k], s.albedo[3 * k + 1], s.albedo[3 * k + 2]);
+		T param = s.param[k];
+		X3<T> n = cog >= 0 ? ng : -ng;
+		uint32_t b = static_cast<uint32_t>(bounce);
+		orc::U4 rA = prand(st.seed, pix, sample, 2u + 2u * b), rB = prand(st.seed, pix, sample, 3u + 2u * b);
+		if (mat != 2 && !s.em.empty()) {
+			float target = orc::u01(rA.x) * s.area_total;
+			int lo = 0, hi = static_cast<int>(s.em.size()) - 1;
+			while (lo < hi) {
+				int mid = (lo + hi) >> 1;
+				if (s.em[mid].cdf > target)
+					hi = mid;
+				else
+					lo = mid + 1;
+			}
+			const PhysScene::Em &E = s.em[lo];
+			T su = std::sqrt(T(orc::u01(rA.y)));
+			T b1 = T(orc::u01(rA.z)) * su, b2 = 1 - su;
+			X3<T> q = x3<T>(E.v0[0], E.v0[1], E.v0[2]) + x3<T>(E.e0[0], E.e0[1], E.e0[2]) * b1 +
+			          x3<T>(E.e1[0], E.e1[1], E.e1[2]) * b2;
+			X3<T> wi = q - p;
+			T dist2 = dt(wi, wi), dist = std::sqrt(dist2);
+			wi = wi * (T(1) / dist);
+			size_t ek = static_cast<size_t>(E.tri);
+			X3<T> ne = x3<T>(s.normal[3 * ek], s.normal[3 * ek + 1], s.normal[3 * ek + 2]);
+			T cos_l = -dt(ne, wi);
+			X3<T> fc;
+			T pb;
+			if (cos_l > 0 && dist > 0 && eval_t<T>(mat, alb, param, n, wo, wi, fc, pb)) {
+				T pl = dist2 / (cos_l * T(s.area_total));
+				X3<T> eLe = x3<T>(s.emission[3 * ek], s.emission[3 * ek + 1], s.emission[3 * ek + 2]);
+				T w = mis_t(pl, pb);
+				if (!occluded_t<T>(s, p + n * eps, wi, dist, E.tri))
+					L = L + beta * fc * eLe * (w / pl);
+			}
+		}
+		if (bounce + 1 >= st.max_depth)
+			break;
+		X3<T> wi, weight;
+		T pdf = 0;
+		if (mat == 0) {
+			T r = std::sqrt(T(orc::u01(rB.x)));
+			T ph = two_pi * T(orc::u01(rB.y));
+			X3<T> t, bt;
+			onb_t(n, t, bt);
+			T z = std::sqrt(std::max(T(0), 1 - T(orc::u01(rB.x))));
+			wi = t * (r * std::cos(ph)) + bt * (r * std::sin(ph)) + n * z;
+			T ci = dt(wi, n);
+			if (ci <= 0)
+				break;
+			weight = alb;
+			pdf = ci * T(0.318309886183790671537767526745);
+		} else if (mat == 1) {
+			T alpha = param, a2 = alpha * alpha;
+			X3<T> t, bt;
+			onb_t(n, t, bt);
+			X3<T> wl = x3(dt(wo, t), dt(wo, bt), dt(wo, n));
+			X3<T> vh = nz(x3(alpha * wl.x, alpha * wl.y, wl.z));
+			T lensq = vh.x * vh.x + vh.y * vh.y;
+			X3<T> T1 = lensq > 0 ? x3<T>(-vh.y, vh.x, 0) * (T(1) / std::sqrt(lensq)) : x3<T>(1, 0, 0);
+			X3<T> T2 = cr(vh, T1);
+			T r = std::sqrt(T(orc::u01(rB.x)));
+			T ph = two_pi * T(orc::u01(rB.y));
+			T t1 = r * std::cos(ph), t2 = r * std::sin(ph);
+			T sb = T(0.5) * (1 + vh.z);
+			t2 = (1 - sb) * std::sqrt(std::max(T(0), 1 - t1 * t1)) + sb * t2;
+			X3<T> nh = T1 * t1 + T2 * t2 + vh * std::sqrt(std::max(T(0), 1 - t1 * t1 - t2 * t2));
+			X3<T> ml = nz(x3(alpha * nh.x, alpha * nh.y, std::max(T(0), nh.z)));
+			X3<T> m = t * ml.x + bt * ml.y + n * ml.z;
+			T om = dt(wo, m);
+			wi = m * (2 * om) - wo;
+			T ci = dt(wi, n), co = wl.z;
+			if (ci <= 0 || om <= 0 || co <= 0)
+				break;
+			T lo_ = ggx_L_t(co, a2), li_ = ggx_L_t(ci, a2);
+			T G1 = 1 / (1 + lo_), G2 = 1 / (1 + lo_ + li_);
+			weight = schlick_t(alb, om) * (G2 / G1);
+			pdf = G1 * ggx_D_t(ml.z, a2) / (4 * co);
+		} else {
+			T eta = param;
+			bool entering = cog > 0;
+			T ei = entering ? T(1) : eta, et = entering ? eta : T(1);
+			T ci = std::fabs(cog), rel = ei / et;
+			T s2t = rel * rel * std::max(T(0), 1 - ci * ci);
+			T F = 1, ct = 0;
+			if (s2t < 1) {
+				ct = std::sqrt(1 - s2t);
+				T rs = (ei * ci - et * ct) / (ei * ci + et * ct), rp = (et * ci - ei * ct) / (et * ci + ei * ct);
+				F = T(0.5) * (rs * rs + rp * rp);
+			}
+			if (T(orc::u01(rA.w)) < F)
+				wi = n * (2 * ci) - wo;
+			else
+				wi = d * rel + n * (rel * ci - ct);
+			weight = x3<T>(1, 1, 1);
+			pdf = 0;
+		}
+		beta = beta * weight;
+		if (bounce + 1 >= st.rr_depth) {
+			T q = std::min(T(0.95), mx(beta));
+			if (!(T(orc::u01(rB.z)) < q))
+				break;
+			beta = beta * (T(1) / q);
+		}
+		T side = dt(wi, ng) >= 0 ? T(1) : T(-1);
+		o = p + ng * (side * eps);
+		d = wi;
+		prev_pdf = pdf;
+		ignore = h.idx;
+	}
+	return L;
+}
+
 } // namespace
 
 extern "C" {
@@ -673,6 +1018,163 @@ void orc_render_reference(const void *bvh, const float *normal3, const int *mate
 				mean[3 * k + 2] = m.z;
 			}
 		}
+	}
+}
+
+// ---- physical mode ---------------------------------------------------------------
+
+void *orc_pt_scene_new(int n, const float *v9, const float *albedo, const float *emission, const int *material,
+                       const float *param) {
+	PhysScene *s = new PhysScene();
+	Bvh &b = s->bvh;
+	b.tris.resize(static_cast<size_t>(n));
+	b.cent.resize(static_cast<size_t>(n));
+	b.order.resize(static_cast<size_t>(n));
+	s->normal.resize(3 * static_cast<size_t>(n));
+	double acc = 0.0;
+	for (int i = 0; i < n; i++) {
+		const float *p = v9 + 9 * static_cast<size_t>(i);
+		b.tris[i] = {mk(p[0], p[1], p[2]), mk(p[3], p[4], p[5]), mk(p[6], p[7], p[8])};
+		b.cent[i] = (b.tris[i].v0 + b.tris[i].v1 + b.tris[i].v2) / 3.0f;
+		b.order[i] = i;
+		double ax = double(p[3]) - p[0], ay = double(p[4]) - p[1], az = double(p[5]) - p[2];
+		double bx = double(p[6]) - p[0], by = double(p[7]) - p[1], bz = double(p[8]) - p[2];
+		double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+		double len = std::sqrt(cx * cx + cy * cy + cz * cz);
+		for (int a = 0; a < 3; a++)
+			s->normal[3 * i + a] = len > 0 ? static_cast<float>((a == 0 ? cx : a == 1 ? cy : cz) / len) : 0.0f;
+		const float *e = emission + 3 * static_cast<size_t>(i);
+		if ((e[0] > 0 || e[1] > 0 || e[2] > 0) && 0.5 * len > 0) {
+			acc += 0.5 * len;
+			PhysScene::Em E;
+			for (int a = 0; a < 3; a++) {
+				E.v0[a] = p[a];
+				E.e0[a] = p[3 + a] - p[a];
+				E.e1[a] = p[6 + a] - p[a];
+			}
+			E.area = static_cast<float>(0.5 * len);
+			E.cdf = static_cast<float>(acc);
+			E.tri = i;
+			s->em.push_back(E);
+		}
+	}
+	s->area_total = static_cast<float>(acc);
+	if (n > 0)
+		b.root = b.build(0, n);
+	s->albedo.assign(albedo, albedo + 3 * static_cast<size_t>(n));
+	s->emission.assign(emission, emission + 3 * static_cast<size_t>(n));
+	s->material.assign(material, material + n);
+	s->param.assign(param, param + n);
+	return s;
+}
+
+void orc_pt_scene_free(void *h) { delete static_cast<PhysScene *>(h); }
+
+// Count the reference-order ray queries of the FP32 estimator on the listed
+// pixels: out[0..5] = closest queries, any-hit queries, closest box tests,
+// closest triangle tests, any-hit box tests, any-hit triangle tests.
+void orc_pt_count(const void *h, const float *cam10, int w, int hgt, int spp, int max_depth, int rr_depth,
+                  unsigned long long seed, unsigned offset, const float *env3, int n_pix, const int *pixels,
+                  long long *out);
+
+// Camera basis as the product's host code builds it (double, rounded once).
+static PhysCam make_cam(const float *cam10, int w, int hgt) {
+	PhysCam c;
+	double pos[3], fwd[3], up[3], right[3], upv[3];
+	for (int a = 0; a < 3; a++) {
+		pos[a] = cam10[a];
+		fwd[a] = double(cam10[3 + a]) - cam10[a];
+		up[a] = cam10[6 + a];
+	}
+	auto nrm = [](double v[3]) {
+		double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+		for (int a = 0; a < 3; a++)
+			v[a] /= l;
+	};
+	auto crs = [](const double a[3], const double b[3], double o[3]) {
+		o[0] = a[1] * b[2] - a[2] * b[1];
+		o[1] = a[2] * b[0] - a[0] * b[2];
+		o[2] = a[0] * b[1] - a[1] * b[0];
+	};
+	nrm(fwd);
+	crs(fwd, up, right);
+	nrm(right);
+	crs(right, fwd, upv);
+	for (int a = 0; a < 3; a++) {
+		c.pos[a] = float(pos[a]);
+		c.fwd[a] = float(fwd[a]);
+		c.right[a] = float(right[a]);
+		c.up[a] = float(upv[a]);
+	}
+	c.tan_half = float(std::tan(cam10[9] * 3.14159265358979323846 / 360.0));
+	c.aspect = float(w) / float(hgt);
+	c.w = w;
+	c.h = hgt;
+	return c;
+}
+
+void orc_pt_count(const void *h, const float *cam10, int w, int hgt, int spp, int max_depth, int rr_depth,
+                  unsigned long long seed, unsigned offset, const float *env3, int n_pix, const int *pixels,
+                  long long *out) {
+	const PhysScene &s = *static_cast<const PhysScene *>(h);
+	const PhysCam c = make_cam(cam10, w, hgt);
+	PhysSet st{spp, max_depth, rr_depth, seed, offset, {env3[0], env3[1], env3[2]}};
+	const int count = pixels ? n_pix : w * hgt;
+	long long tot[6] = {0, 0, 0, 0, 0, 0};
+#pragma omp parallel
+	{
+		QueryCounts qc;
+		g_qc = &qc;
+#pragma omp for schedule(dynamic, 16)
+		for (int i = 0; i < count; i++) {
+			uint32_t pix = static_cast<uint32_t>(pixels ? pixels[i] : i);
+			for (int k = 0; k < spp; k++)
+				(void)trace_phys<float>(s, c, st, pix, offset + static_cast<uint32_t>(k));
+		}
+		g_qc = nullptr;
+#pragma omp critical
+		{
+			tot[0] += qc.closest;
+			tot[1] += qc.any;
+			tot[2] += qc.cb.boxes;
+			tot[3] += qc.cb.tris;
+			tot[4] += qc.ab.boxes;
+			tot[5] += qc.ab.tris;
+		}
+	}
+	for (int k = 0; k < 6; k++)
+		out[k] = tot[k];
+}
+
+// cam: pos3, target3, up3, vfov_deg (10 floats), w, h; settings: spp, max_depth, rr_depth, seed, offset, env3.
+// Renders the listed pixels (or all when pixels == NULL) and writes per-pixel SUMS (3 doubles each).
+void orc_pt_render(const void *h, const float *cam10, int w, int hgt, int spp, int max_depth, int rr_depth,
+                   unsigned long long seed, unsigned offset, const float *env3, int n_pix, const int *pixels,
+                   int precision, double *sums) {
+	const PhysScene &s = *static_cast<const PhysScene *>(h);
+	const PhysCam c = make_cam(cam10, w, hgt);
+	PhysSet st{spp, max_depth, rr_depth, seed, offset, {env3[0], env3[1], env3[2]}};
+	const int count = pixels ? n_pix : w * hgt;
+#pragma omp parallel for schedule(dynamic, 16)
+	for (int i = 0; i < count; i++) {
+		uint32_t pix = static_cast<uint32_t>(pixels ? pixels[i] : i);
+		double sx = 0, sy = 0, sz = 0;
+		for (int k = 0; k < spp; k++) {
+			if (precision == 0) {
+				X3<float> L = trace_phys<float>(s, c, st, pix, offset + static_cast<uint32_t>(k));
+				sx += L.x;
+				sy += L.y;
+				sz += L.z;
+			} else {
+				X3<double> L = trace_phys<double>(s, c, st, pix, offset + static_cast<uint32_t>(k));
+				sx += L.x;
+				sy += L.y;
+				sz += L.z;
+			}
+		}
+		sums[3 * i] = sx;
+		sums[3 * i + 1] = sy;
+		sums[3 * i + 2] = sz;
 	}
 }
 

@@ -17,9 +17,9 @@ from typing import Optional, Sequence, Tuple, Union
 import numpy as np
 
 from . import _native
-from ._native import Light, RnError
+from ._native import Camera, Light, RnError, Settings
 
-__all__ = ["RenderMode", "Scene", "Image", "Light", "RnError", "version"]
+__all__ = ["RenderMode", "Scene", "Image", "Light", "Camera", "Settings", "RnError", "version"]
 __version__ = "0.1.2"
 
 
@@ -330,6 +330,38 @@ class Scene:
         _native.check(_native.load().rn_pt_render_reference(self._handle, ctypes.byref(p), 0, None, _ptr(canvas),
                                                             _ptr(mean)), "render_reference")
         return (canvas, mean) if want_mean else canvas
+
+    def render_physical(self, camera: "Camera", settings: "Settings", nearest_first: bool = True,
+                        out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Physical-mode render: per-pixel mean radiance as (height, width, 3) float32."""
+        self._check_open()
+        rgb = out if out is not None else np.empty((camera.height, camera.width, 3), np.float32)
+        flags = _native.RN_PT_ORDER_NEAREST if nearest_first else 0
+        _native.check(_native.load().rn_pt_render(self._handle, ctypes.byref(camera), ctypes.byref(settings), flags,
+                                                  None, _ptr(rgb)), "rn_pt_render")
+        return rgb
+
+    def accumulate(self, camera: "Camera", settings: "Settings", accum: np.ndarray,
+                   nearest_first: bool = True) -> np.ndarray:
+        """Add the per-pixel sum of the settings' samples to ``accum`` (float32, in place)."""
+        self._check_open()
+        if accum.dtype != np.float32 or not accum.flags.c_contiguous or accum.size != camera.width * camera.height * 3:
+            raise ValueError("accum must be a contiguous float32 array of width*height*3 values")
+        flags = _native.RN_PT_ORDER_NEAREST if nearest_first else 0
+        _native.check(_native.load().rn_pt_render_accumulate(self._handle, ctypes.byref(camera),
+                                                             ctypes.byref(settings), flags, None, _ptr(accum)),
+                      "rn_pt_render_accumulate")
+        return accum
+
+    def count_traversal(self, camera: "Camera", settings: "Settings") -> dict:
+        """Reference-traversal test counts over one render's rays (profiling counters)."""
+        self._check_open()
+        out = np.zeros(7, np.int64)
+        _native.check(_native.load().rn_pt_count_traversal(self._handle, ctypes.byref(camera),
+                                                           ctypes.byref(settings), _ptr(out)),
+                      "rn_pt_count_traversal")
+        keys = ("samples", "closest", "any", "closest_boxes", "closest_tris", "any_boxes", "any_tris")
+        return {k: int(v) for k, v in zip(keys, out)}
 
     # ---- lifetime ----------------------------------------------------------------
     @property

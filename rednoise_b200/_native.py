@@ -128,6 +128,60 @@ class RefParams(ctypes.Structure):
     ]
 
 
+class Camera(ctypes.Structure):
+    """rn_pt_camera: pinhole camera with a vertical field of view."""
+
+    _fields_ = [
+        ("position", ctypes.c_float * 3),
+        ("target", ctypes.c_float * 3),
+        ("up", ctypes.c_float * 3),
+        ("vfov_deg", ctypes.c_float),
+        ("width", ctypes.c_int),
+        ("height", ctypes.c_int),
+    ]
+
+    @classmethod
+    def make(cls, position, target, up=(0.0, 1.0, 0.0), vfov_deg=40.0, width=64, height=64) -> "Camera":
+        c = cls()
+        c.position[:] = tuple(float(x) for x in position)
+        c.target[:] = tuple(float(x) for x in target)
+        c.up[:] = tuple(float(x) for x in up)
+        c.vfov_deg = vfov_deg
+        c.width = int(width)
+        c.height = int(height)
+        return c
+
+
+RN_PT_AUTO, RN_PT_MEGAKERNEL, RN_PT_WAVEFRONT = 0, 1, 2
+
+
+class Settings(ctypes.Structure):
+    """rn_pt_settings."""
+
+    _fields_ = [
+        ("spp", ctypes.c_int),
+        ("max_depth", ctypes.c_int),
+        ("rr_depth", ctypes.c_int),
+        ("integrator", ctypes.c_int),
+        ("seed", ctypes.c_ulonglong),
+        ("sample_offset", ctypes.c_uint),
+        ("env", ctypes.c_float * 3),
+    ]
+
+    @classmethod
+    def make(cls, spp=16, max_depth=5, rr_depth=None, integrator=RN_PT_AUTO, seed=0, sample_offset=0,
+             env=(0.0, 0.0, 0.0)) -> "Settings":
+        s = cls()
+        s.spp = int(spp)
+        s.max_depth = int(max_depth)
+        s.rr_depth = int(max_depth if rr_depth is None else rr_depth)
+        s.integrator = int(integrator)
+        s.seed = int(seed)
+        s.sample_offset = int(sample_offset)
+        s.env[:] = tuple(float(x) for x in env)
+        return s
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     # drop-in ABI (include/rednoise/rednoise.h)
@@ -148,6 +202,10 @@ SIGNATURES = {
     "rn_pt_ref_params_init": (None, [ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                      ctypes.c_int]),
     "rn_pt_render_reference": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_uint, vp, vp, vp]),
+    "rn_pt_render": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint, vp, vp]),
+    "rn_pt_render_accumulate": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
+                                               vp, vp]),
+    "rn_pt_count_traversal": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), vp]),
     "rn_pt_last_error": (ctypes.c_char_p, []),
 }
 

@@ -118,6 +118,31 @@ Vec3 loader_face_normal(const float *t) {
 	return {0.0f, 1.0f, 0.0f};
 }
 
+static void cross_d(const float *t, double c[3]) {
+	const double ax = static_cast<double>(t[3]) - t[0], ay = static_cast<double>(t[4]) - t[1],
+	             az = static_cast<double>(t[5]) - t[2];
+	const double bx = static_cast<double>(t[6]) - t[0], by = static_cast<double>(t[7]) - t[1],
+	             bz = static_cast<double>(t[8]) - t[2];
+	c[0] = ay * bz - az * by;
+	c[1] = az * bx - ax * bz;
+	c[2] = ax * by - ay * bx;
+}
+
+Vec3 geometric_normal(const float *t) {
+	double c[3];
+	cross_d(t, c);
+	const double len = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+	if (!(len > 0.0))
+		return {0.0f, 0.0f, 0.0f};
+	return {static_cast<float>(c[0] / len), static_cast<float>(c[1] / len), static_cast<float>(c[2] / len)};
+}
+
+double triangle_area(const float *t) {
+	double c[3];
+	cross_d(t, c);
+	return 0.5 * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+}
+
 namespace {
 
 int materialFor(const std::string &name) {

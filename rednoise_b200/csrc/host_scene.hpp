@@ -68,6 +68,11 @@ void build_reference_bvh(const float *v9, int n, Bvh2 &out);
 // Face normal as the reference OBJ loader computes it (src/ObjLoader.cpp:170-176).
 Vec3 loader_face_normal(const float *v9);
 
+// Unit geometric normal cross(v1 - v0, v2 - v0) (computed in double, rounded
+// once), (0, 0, 0) for a degenerate triangle; and the triangle's area.
+Vec3 geometric_normal(const float *v9);
+double triangle_area(const float *v9);
+
 // Wavefront OBJ/MTL loader with the reference loader's semantics
 // (src/ObjLoader.cpp:23-214): `v` scaled by `scale`, first three face tokens,
 // `usemtl` name -> Material mapping and Kd colour as int(Kd*255).

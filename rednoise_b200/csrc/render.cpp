@@ -1,0 +1,210 @@
+// Physical-mode rendering entry points (rn_pt_render / rn_pt_render_accumulate).
+#include <cmath>
+#include <cstring>
+
+#include "pt_kernels.hpp"
+#include "render_impl.hpp"
+#include "scene_impl.hpp"
+
+namespace rnb {
+
+rn_status make_phys_inputs(rn_scene *s, const rn_pt_camera *c, const rn_pt_settings *st, unsigned flags,
+                           PhysScene &ps, PhysCamera &pc, PhysSettings &pst) {
+	if (!s || !c || !st) {
+		set_last_error("render: NULL argument");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (c->width <= 0 || c->height <= 0 || static_cast<long>(c->width) * c->height > (1L << 28)) {
+		set_last_error("render: camera width/height must be positive and at most 2^28 pixels");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (!(c->vfov_deg > 0.0f && c->vfov_deg < 179.0f)) {
+		set_last_error("render: vfov_deg must be in (0, 179)");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (st->spp < 0 || st->max_depth < 1 || st->max_depth > 64) {
+		set_last_error("render: need spp >= 0 and 1 <= max_depth <= 64");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	rn_status r = prepare_scene(s);
+	if (r != RN_OK)
+		return r;
+	ps.sv = s->view;
+	ps.shade = s->d_phys_shade.as<float4>();
+	ps.emitters = s->d_emitters.as<float4>();
+	ps.n_emitters = s->n_emitters;
+	ps.emit_area_total = s->emit_area_total;
+
+	double pos[3], fwd[3], up[3], right[3], upv[3];
+	for (int a = 0; a < 3; a++) {
+		pos[a] = c->position[a];
+		fwd[a] = static_cast<double>(c->target[a]) - c->position[a];
+		up[a] = c->up[a];
+	}
+	auto nrm = [](double v[3]) {
+		const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+		if (l > 0)
+			for (int a = 0; a < 3; a++)
+				v[a] /= l;
+		return l > 0;
+	};
+	auto crs = [](const double a[3], const double b[3], double o[3]) {
+		o[0] = a[1] * b[2] - a[2] * b[1];
+		o[1] = a[2] * b[0] - a[0] * b[2];
+		o[2] = a[0] * b[1] - a[1] * b[0];
+	};
+	if (!nrm(fwd)) {
+		set_last_error("render: camera target equals its position");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	crs(fwd, up, right);
+	if (!nrm(right)) {
+		set_last_error("render: camera up is parallel to the view direction");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	crs(right, fwd, upv);
+	for (int a = 0; a < 3; a++) {
+		pc.pos[a] = static_cast<float>(pos[a]);
+		pc.fwd[a] = static_cast<float>(fwd[a]);
+		pc.right[a] = static_cast<float>(right[a]);
+		pc.up[a] = static_cast<float>(upv[a]);
+	}
+	pc.tan_half_y = static_cast<float>(std::tan(c->vfov_deg * 3.14159265358979323846 / 360.0));
+	pc.aspect = static_cast<float>(c->width) / static_cast<float>(c->height);
+	pc.width = c->width;
+	pc.height = c->height;
+	pst.spp = st->spp;
+	pst.max_depth = st->max_depth;
+	pst.rr_depth = st->rr_depth;
+	pst.order = (flags & RN_PT_ORDER_NEAREST) ? kOrderNearest : kOrderReference;
+	pst.seed = st->seed;
+	pst.sample_offset = st->sample_offset;
+	for (int a = 0; a < 3; a++)
+		pst.env[a] = st->env[a];
+	return RN_OK;
+}
+
+} // namespace rnb
+
+using namespace rnb;
+
+namespace {
+
+// Run the selected integrator over accum (device, 3 floats per pixel).
+rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, const PhysScene &ps, const PhysCamera &pc,
+                         const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
+	if (st->integrator == RN_PT_WAVEFRONT) {
+		set_last_error("render: the wavefront integrator is not available in this build");
+		return RN_ERR_UNSUPPORTED;
+	}
+	RNB_CUDA(s->d_counter.ensure(256));
+	RNB_CUDA(launch_megakernel(ps, pc, pst, d_accum, s->d_counter.as<unsigned>(), s->d_status.as<int>(), cs));
+	return RN_OK;
+}
+
+rn_status finish_sync(rn_scene *s, cudaStream_t cs, const char *what) {
+	int h = 0;
+	RNB_CUDA(cudaMemcpyAsync(&h, s->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, cs));
+	RNB_CUDA(cudaStreamSynchronize(cs));
+	if (h) {
+		cudaMemsetAsync(s->d_status.p, 0, sizeof(int), cs);
+		set_last_error(std::string(what) + ": device status word reports a traversal error");
+		return RN_ERR_INTERNAL;
+	}
+	return RN_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
+                                  unsigned flags, void *stream, float *accum) {
+	PhysScene ps;
+	PhysCamera pc;
+	PhysSettings pst;
+	rn_status r = make_phys_inputs(scene, camera, settings, flags, ps, pc, pst);
+	if (r != RN_OK)
+		return r;
+	if (!accum) {
+		set_last_error("rn_pt_render_accumulate: NULL accum");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	cudaStream_t cs = pick_stream(scene, stream);
+	const size_t bytes = static_cast<size_t>(camera->width) * camera->height * 3 * sizeof(float);
+	if (flags & RN_PT_DEVICE_POINTERS)
+		return run_integrator(scene, settings, ps, pc, pst, accum, cs);
+	std::lock_guard<std::mutex> lock(scene->scratch_mu);
+	RNB_CUDA(scene->scratch.ensure(bytes));
+	float *d = scene->scratch.as<float>();
+	RNB_CUDA(cudaMemcpyAsync(d, accum, bytes, cudaMemcpyHostToDevice, cs));
+	r = run_integrator(scene, settings, ps, pc, pst, d, cs);
+	if (r != RN_OK)
+		return r;
+	RNB_CUDA(cudaMemcpyAsync(accum, d, bytes, cudaMemcpyDeviceToHost, cs));
+	return finish_sync(scene, cs, "rn_pt_render_accumulate");
+}
+
+rn_status rn_pt_count_traversal(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
+                                long long *counters) {
+	PhysScene ps;
+	PhysCamera pc;
+	PhysSettings pst;
+	rn_status r = make_phys_inputs(scene, camera, settings, 0, ps, pc, pst);
+	if (r != RN_OK)
+		return r;
+	if (!counters) {
+		set_last_error("rn_pt_count_traversal: NULL counters");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	cudaStream_t cs = scene->stream;
+	std::lock_guard<std::mutex> lock(scene->scratch_mu);
+	RNB_CUDA(scene->scratch.ensure(256));
+	unsigned long long *d = scene->scratch.as<unsigned long long>();
+	RNB_CUDA(launch_count(ps, pc, pst, d, scene->d_status.as<int>(), cs));
+	RNB_CUDA(cudaMemcpyAsync(counters, d, 7 * sizeof(long long), cudaMemcpyDeviceToHost, cs));
+	return finish_sync(scene, cs, "rn_pt_count_traversal");
+}
+
+rn_status rn_pt_render(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings, unsigned flags,
+                       void *stream, float *rgb) {
+	PhysScene ps;
+	PhysCamera pc;
+	PhysSettings pst;
+	rn_status r = make_phys_inputs(scene, camera, settings, flags, ps, pc, pst);
+	if (r != RN_OK)
+		return r;
+	if (!rgb) {
+		set_last_error("rn_pt_render: NULL rgb");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	cudaStream_t cs = pick_stream(scene, stream);
+	const long nf = static_cast<long>(camera->width) * camera->height * 3;
+	const size_t bytes = static_cast<size_t>(nf) * sizeof(float);
+	const float inv = settings->spp > 0 ? 1.0f / static_cast<float>(settings->spp) : 0.0f;
+	const bool dev = (flags & RN_PT_DEVICE_POINTERS) != 0;
+	std::unique_lock<std::mutex> lock(scene->scratch_mu, std::defer_lock);
+	float *acc;
+	if (dev) {
+		RNB_CUDA(scene->accum.ensure(bytes));
+		acc = scene->accum.as<float>();
+	} else {
+		lock.lock();
+		RNB_CUDA(scene->scratch.ensure(2 * bytes + 256));
+		acc = scene->scratch.as<float>();
+	}
+	RNB_CUDA(cudaMemsetAsync(acc, 0, bytes, cs));
+	r = run_integrator(scene, settings, ps, pc, pst, acc, cs);
+	if (r != RN_OK)
+		return r;
+	if (dev) {
+		RNB_CUDA(launch_resolve(acc, rgb, nf, inv, cs));
+		return RN_OK;
+	}
+	float *mean = acc + nf + 64;
+	RNB_CUDA(launch_resolve(acc, mean, nf, inv, cs));
+	RNB_CUDA(cudaMemcpyAsync(rgb, mean, bytes, cudaMemcpyDeviceToHost, cs));
+	return finish_sync(scene, cs, "rn_pt_render");
+}
+
+} // extern "C"

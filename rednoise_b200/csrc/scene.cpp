@@ -69,33 +69,35 @@ rn_status prepare_scene(rn_scene *s) {
 	s->internal_nodes = lay.internal_count;
 
 	// Shading records indexed by original triangle.
-	std::vector<F4> ref(static_cast<size_t>(n) * 2), phys(static_cast<size_t>(n) * 2);
+	std::vector<F4> ref(static_cast<size_t>(n) * 2), phys(static_cast<size_t>(n) * 3);
 	const TriangleSet &ts = s->tris;
 	for (int i = 0; i < n; i++) {
 		const size_t k = static_cast<size_t>(i);
 		ref[2 * k] = {ts.normal[3 * k], ts.normal[3 * k + 1], ts.normal[3 * k + 2], as_float(ts.ref_material[k])};
 		ref[2 * k + 1] = {static_cast<float>(ts.rgb[3 * k]), static_cast<float>(ts.rgb[3 * k + 1]),
 		                  static_cast<float>(ts.rgb[3 * k + 2]), ts.roughness[k]};
-		phys[2 * k] = {ts.albedo[3 * k], ts.albedo[3 * k + 1], ts.albedo[3 * k + 2], as_float(ts.phys_material[k])};
-		phys[2 * k + 1] = {ts.emission[3 * k], ts.emission[3 * k + 1], ts.emission[3 * k + 2], ts.phys_param[k]};
+		Vec3 ng = geometric_normal(&ts.v[9 * k]);
+		phys[3 * k] = {ts.albedo[3 * k], ts.albedo[3 * k + 1], ts.albedo[3 * k + 2], as_float(ts.phys_material[k])};
+		phys[3 * k + 1] = {ts.emission[3 * k], ts.emission[3 * k + 1], ts.emission[3 * k + 2], ts.phys_param[k]};
+		phys[3 * k + 2] = {ng.x, ng.y, ng.z, 0.0f};
 	}
-	// Emitters (triangles with any Le > 0) and their area CDF for light sampling.
-	std::vector<int> em;
-	std::vector<float> cdf;
+	// Emitters (triangles with any Le > 0): (v0, tri), (e0, area), (e1, cumulative area).
+	std::vector<F4> em;
 	double acc = 0.0;
 	for (int i = 0; i < n; i++) {
 		const size_t k = static_cast<size_t>(i);
 		if (ts.emission[3 * k] > 0.0f || ts.emission[3 * k + 1] > 0.0f || ts.emission[3 * k + 2] > 0.0f) {
 			const float *t = &ts.v[9 * k];
-			const double ax = t[3] - t[0], ay = t[4] - t[1], az = t[5] - t[2];
-			const double bx = t[6] - t[0], by = t[7] - t[1], bz = t[8] - t[2];
-			const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
-			acc += 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
-			em.push_back(i);
-			cdf.push_back(static_cast<float>(acc));
+			const double area = triangle_area(t);
+			if (!(area > 0.0))
+				continue; // a degenerate emitter can neither be hit nor sampled
+			acc += area;
+			em.push_back({t[0], t[1], t[2], as_float(i)});
+			em.push_back({t[3] - t[0], t[4] - t[1], t[5] - t[2], static_cast<float>(area)});
+			em.push_back({t[6] - t[0], t[7] - t[1], t[8] - t[2], static_cast<float>(acc)});
 		}
 	}
-	s->n_emitters = static_cast<int>(em.size());
+	s->n_emitters = static_cast<int>(em.size() / 3);
 	s->emit_area_total = static_cast<float>(acc);
 
 	if (!s->stream)
@@ -112,8 +114,7 @@ rn_status prepare_scene(rn_scene *s) {
 	RNB_CUDA(up(s->d_tris, lay.tris.data(), lay.tris.size() * sizeof(F4)));
 	RNB_CUDA(up(s->d_ref_shade, ref.data(), ref.size() * sizeof(F4)));
 	RNB_CUDA(up(s->d_phys_shade, phys.data(), phys.size() * sizeof(F4)));
-	RNB_CUDA(up(s->d_emitters, em.data(), em.size() * sizeof(int)));
-	RNB_CUDA(up(s->d_emit_cdf, cdf.data(), cdf.size() * sizeof(float)));
+	RNB_CUDA(up(s->d_emitters, em.data(), em.size() * sizeof(F4)));
 	RNB_CUDA(s->d_status.ensure(256));
 	RNB_CUDA(cudaMemset(s->d_status.p, 0, 256));
 
@@ -320,8 +321,7 @@ rn_status rn_pt_scene_get_info(rn_scene *scene, rn_pt_scene_info *out) {
 	out->internal_nodes = scene->internal_nodes;
 	out->depth = scene->bvh.depth;
 	out->device_bytes = static_cast<long long>(scene->d_nodes.bytes + scene->d_tris.bytes + scene->d_ref_shade.bytes +
-	                                           scene->d_phys_shade.bytes + scene->d_emitters.bytes +
-	                                           scene->d_emit_cdf.bytes);
+	                                           scene->d_phys_shade.bytes + scene->d_emitters.bytes);
 	out->build_ms = scene->build_ms;
 	return RN_OK;
 }

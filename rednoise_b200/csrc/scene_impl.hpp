@@ -24,7 +24,7 @@ struct rn_scene {
 
 	int device = -1;
 	cudaStream_t stream = nullptr;
-	rnb::DevBuf d_nodes, d_tris, d_ref_shade, d_phys_shade, d_emitters, d_emit_cdf;
+	rnb::DevBuf d_nodes, d_tris, d_ref_shade, d_phys_shade, d_emitters;
 	rnb::DevBuf d_status; // error word for asynchronous (device-pointer) calls
 	rnb::SceneView view{};
 	int n_emitters = 0;
@@ -33,6 +33,10 @@ struct rn_scene {
 	// Scratch for host-pointer calls (rays in, results out).
 	std::mutex scratch_mu;
 	rnb::DevBuf scratch;
+	// Work counter of the persistent kernels and the accumulator of
+	// device-pointer renders (calls on one scene are serialised on its stream).
+	rnb::DevBuf d_counter;
+	rnb::DevBuf accum;
 
 	~rn_scene();
 };

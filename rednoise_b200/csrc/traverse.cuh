@@ -332,6 +332,81 @@ __device__ __forceinline__ bool trace_any(const SceneView &s, const RayPre &r, f
 	return false;
 }
 
+// Instrumented emulation of the reference traversal (src/BVH.cpp:77-139) for
+// the algorithmic-bytes counters: both children are pushed and each node's box
+// test is counted when it is popped, exactly as the reference does it, so
+// `boxes` and `tris` are the reference's test counts for this ray. Closest-hit
+// mode (kAny = false) returns the reference's hit in `h`; any-hit mode returns
+// the occlusion flag.
+template <bool kAny>
+__device__ bool count_reference_query(const SceneView &s, const RayPre &r, int ignore, float tmax, HitRec &h,
+                                      unsigned long long &boxes, unsigned long long &tris, int &err) {
+	int st_ref[kStack];
+	float st_te[kStack];
+	int sp = 0;
+	float best = kAny ? tmax : __int_as_float(0x7f800000);
+	h.idx = -1;
+	h.rank = 0;
+	h.t = best;
+	h.u = h.v = 0.0f;
+	if (s.n_tris <= 0)
+		return false;
+	float te;
+	const bool ok = slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te);
+	st_ref[0] = s.root_ref;
+	st_te[0] = ok ? te : __int_as_float(0x7fc00000); // NaN never passes te < best
+	sp = 1;
+	while (sp > 0) {
+		--sp;
+		const int ref = st_ref[sp];
+		const float tent = st_te[sp];
+		boxes++;
+		if (!(tent < best))
+			continue;
+		if (ref < 0) {
+			const int start = leaf_start(ref);
+			const int count = leaf_count(ref);
+			for (int p = start; p < start + count; p++) {
+				const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
+				const float4 a = __ldg(tp + 0);
+				const int ti = __float_as_int(a.w);
+				if (ti == ignore)
+					continue;
+				tris++;
+				const float4 b = __ldg(tp + 1);
+				const float4 c = __ldg(tp + 2);
+				float t, u, v;
+				if (tri_test(a, b, c, r, t, u, v) && t < best) {
+					if (kAny)
+						return true;
+					best = t;
+					h.idx = ti;
+					h.t = t;
+					h.u = u;
+					h.v = v;
+					h.rank = __float_as_int(b.w);
+				}
+			}
+			continue;
+		}
+		if (sp + 2 > kStack) {
+			err = 1;
+			return false;
+		}
+		const float4 *nd = s.nodes + 4 * static_cast<size_t>(ref);
+		const float4 n0 = __ldg(nd + 0), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
+		float tl, tr;
+		const bool hl = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, r, tl);
+		const bool hr = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, r, tr);
+		st_ref[sp] = __float_as_int(n3.x);
+		st_te[sp] = hl ? tl : __int_as_float(0x7fc00000);
+		st_ref[sp + 1] = __float_as_int(n3.y);
+		st_te[sp + 1] = hr ? tr : __int_as_float(0x7fc00000);
+		sp += 2;
+	}
+	return false;
+}
+
 #endif // __CUDACC__
 
 } // namespace rnb

@@ -119,6 +119,24 @@ def test_oracle_reference_render_matches_reference(assets):
     assert np.array_equal(ref_canvas, got)
 
 
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+def test_oracle_light_types_match_reference(assets):
+    """Every visibility branch (src/Renderer.cpp:390-498): oracle == reference build, bit for bit."""
+    import rednoise_b200 as rn
+    from test_refmode_gpu import LIGHT_CASES, _records
+
+    v9 = assets["cornell_v"]
+    m = oracle.RefModel.from_arrays(v9, assets["cornell_rgb"], assets["cornell_material"],
+                                    assets["cornell_roughness"], assets["cornell_normal"])
+    orc = oracle.OrcBvh(v9)
+    for case, kws in sorted(LIGHT_CASES.items()):
+        lights = None if kws is None else _records([rn.Light.default(**kw) for kw in kws])
+        want = m.render(40, 30, 2, lights=lights)
+        got = orc.render_reference(assets["cornell_normal"], assets["cornell_material"], assets["cornell_rgb"],
+                                   assets["cornell_roughness"], 40, 30, 2, lights=lights)
+        assert np.array_equal(want, got), case
+
+
 def test_golden_render_is_reference_c_abi(assets):
     """The golden rn_render image equals the oracle's restatement of renderPathTraced."""
     g = load("render_ref.npz")["rgba_64x48_4"]

@@ -1,0 +1,145 @@
+"""GPU parity of the physical-mode megakernel against the CPU oracle.
+
+The GPU and the oracle draw the same counter-based uniforms for every path, so
+their renders are compared with common random numbers: per-pixel means agree to
+float rounding except where rounding moves a single path (tolerances below).
+Statistical checks (independent seeds, Russian roulette) use per-pixel
+confidence intervals.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import rednoise_b200 as rn
+from rednoise_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def make_scene(sc):
+    return rn.Scene.from_arrays(sc["vertices"], albedo=sc["albedo"], emission=sc["emission"],
+                                material=sc["material"], material_param=sc["material_param"])
+
+
+def cam(w, h):
+    return scenes.camera(w, h)
+
+
+def gpu_render(s, c, spp, depth, rr=None, seed=1, offset=0, nearest=True, integrator=0):
+    camera = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], c["width"], c["height"])
+    st = rn.Settings.make(spp=spp, max_depth=depth, rr_depth=rr, seed=seed, sample_offset=offset,
+                          integrator=integrator)
+    return s.render_physical(camera, st, nearest_first=nearest)
+
+
+def crn_agree(gpu_mean, orc_mean, rel_l1=2e-3, pix_frac=0.01):
+    """Common-random-number agreement: image-level relative L1 and the fraction
+    of pixels whose values differ by more than 1e-3 of the image's peak."""
+    g = gpu_mean.reshape(-1, 3).astype(np.float64)
+    o = orc_mean.reshape(-1, 3)
+    l1 = np.abs(g - o).sum() / max(np.abs(o).sum(), 1e-30)
+    peak = max(o.max(), 1e-30)
+    frac = (np.abs(g - o).max(axis=1) > 1e-3 * peak).mean()
+    assert l1 < rel_l1, f"relative L1 {l1:.2e}"
+    assert frac < pix_frac, f"{frac:.4f} of pixels differ"
+    return l1, frac
+
+
+@pytest.fixture(scope="module")
+def box():
+    return scenes.cornell_box()
+
+
+def test_cornell_box_matches_oracle_crn(box):
+    s = make_scene(box)
+    c = cam(64, 48)
+    spp, depth = 32, 5
+    g = gpu_render(s, c, spp, depth)
+    o = oracle.OrcPhysScene(box).render_sums(c, spp, depth, depth, seed=1) / spp
+    assert g.mean() > 0
+    crn_agree(g, o)
+
+
+def test_fp64_oracle_agrees(box):
+    """FP32 GPU vs the oracle's FP64 estimator on the same samples."""
+    s = make_scene(box)
+    c = cam(48, 36)
+    g = gpu_render(s, c, 32, 5)
+    o = oracle.OrcPhysScene(box).render_sums(c, 32, 5, 5, seed=1, double=True) / 32
+    crn_agree(g, o, rel_l1=5e-3, pix_frac=0.03)
+
+
+def test_mixed_materials_match_oracle_crn():
+    sc = scenes.icosphere_scene(level=3)
+    s = make_scene(sc)
+    c = cam(64, 48)
+    g = gpu_render(s, c, 16, 8, rr=3)
+    o = oracle.OrcPhysScene(sc).render_sums(c, 16, 8, 3, seed=1) / 16
+    crn_agree(g, o, rel_l1=1e-2, pix_frac=0.05)
+
+
+def test_reference_order_equals_nearest_order_renders(box):
+    s = make_scene(box)
+    c = cam(48, 36)
+    a = gpu_render(s, c, 16, 5, nearest=False)
+    b = gpu_render(s, c, 16, 5, nearest=True)
+    crn_agree(a, b, rel_l1=1e-3, pix_frac=0.01)
+
+
+def test_accumulate_resume_is_bit_exact(box):
+    """A render split over sample offsets equals one call, bit for bit."""
+    s = make_scene(box)
+    c = cam(40, 30)
+    camera = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], 40, 30)
+    one = np.zeros(40 * 30 * 3, np.float32)
+    s.accumulate(camera, rn.Settings.make(spp=12, max_depth=5, seed=3), one)
+    two = np.zeros(40 * 30 * 3, np.float32)
+    s.accumulate(camera, rn.Settings.make(spp=5, max_depth=5, seed=3), two)
+    s.accumulate(camera, rn.Settings.make(spp=7, max_depth=5, seed=3, sample_offset=5), two)
+    assert np.array_equal(one.view(np.uint32), two.view(np.uint32))
+
+
+def test_independent_seeds_within_confidence(box):
+    """Two independent estimates agree within a per-pixel 99.9 % interval (Welch)."""
+    s = make_scene(box)
+    c = cam(24, 18)
+    k = 8
+    runs_a = np.stack([gpu_render(s, c, 64, 5, seed=100 + i) for i in range(k)])
+    runs_b = np.stack([gpu_render(s, c, 64, 5, seed=200 + i) for i in range(k)])
+    ma, mb = runs_a.mean(0), runs_b.mean(0)
+    va, vb = runs_a.var(0, ddof=1) / k, runs_b.var(0, ddof=1) / k
+    z = np.abs(ma - mb) / np.sqrt(va + vb + 1e-30)
+    assert (z > 3.29).mean() < 0.01
+
+
+def test_russian_roulette_is_unbiased(box):
+    s = make_scene(box)
+    c = cam(16, 12)
+    a = np.stack([gpu_render(s, c, 256, 8, rr=8, seed=i) for i in range(4)])
+    b = np.stack([gpu_render(s, c, 256, 8, rr=2, seed=50 + i) for i in range(4)])
+    ma, mb = a.mean(), b.mean()
+    assert abs(ma - mb) / ma < 0.03
+
+
+def test_traversal_counters_match_oracle():
+    """The GPU's reference-traversal counters (roofline numerator) match the
+    oracle's instrumented reference traversal over the same estimator's rays."""
+    sc = scenes.icosphere_scene(level=4)
+    s = make_scene(sc)
+    c = cam(64, 48)
+    camera = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], 64, 48)
+    g = s.count_traversal(camera, rn.Settings.make(spp=4, max_depth=8, rr_depth=3, seed=5))
+    o = oracle.OrcPhysScene(sc).count_queries(c, 4, 8, 3, seed=5)
+    assert g["samples"] == 64 * 48 * 4
+    for k in ("closest", "any", "closest_boxes", "closest_tris", "any_boxes", "any_tris"):
+        assert abs(g[k] - o[k]) <= 0.01 * o[k] + 16, (k, g[k], o[k])
+
+
+def test_invalid_settings_rejected(box):
+    s = make_scene(box)
+    c = rn.Camera.make((0, 0, 5), (0, 0, 5), width=8, height=8)
+    with pytest.raises(rn.RnError):
+        s.render_physical(c, rn.Settings.make(spp=1))
+    c = rn.Camera.make((0, 0, 5), (0, 0, 0), width=8, height=8)
+    with pytest.raises(rn.RnError):
+        s.render_physical(c, rn.Settings.make(spp=1, max_depth=0))
