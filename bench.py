@@ -228,7 +228,7 @@ def run_ours(args):
     sptr = ctypes.c_void_p(stream.cuda_stream)
     out = torch.empty(H * W * 3, dtype=torch.float32, device="cuda")
     l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
-    flags = _native.RN_PT_DEVICE_POINTERS | _native.RN_PT_ORDER_NEAREST
+    flags = _native.RN_PT_DEVICE_POINTERS
     step_counter = [0]
 
     def settings():
@@ -279,7 +279,7 @@ def run_ours(args):
 
     # End to end through the C ABI with host buffers: pinned host output, D2H inside the timed region.
     host = torch.empty(H * W * 3, dtype=torch.float32, pin_memory=True)
-    hflags = _native.RN_PT_ORDER_NEAREST
+    hflags = 0
     e2e_steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize()
     if dist:
@@ -319,7 +319,7 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": spp, "max_depth": args.depth,
                    "rr_depth": args.rr, "triangles": info["num_triangles"], "integrator": args.integrator,
-                   "traversal": "nearest-first, reference arithmetic", "l2": "flushed (256 MB write) before each step",
+                   "traversal": "reference order and arithmetic (closest hits bit-exact)", "l2": "flushed (256 MB write) before each step",
                    "parallelism": f"{world} independent ranks, disjoint sample indices"},
         "gpu_launches": 2 * args.steps,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ctypes.sizeof(cam) + ctypes.sizeof(st),

@@ -36,6 +36,7 @@ typedef enum {
 /* flags */
 #define RN_PT_DEVICE_POINTERS 1u /* arrays are device pointers; asynchronous on `stream` */
 #define RN_PT_ORDER_NEAREST 2u   /* closest hit: nearest-child-first traversal (default: reference order) */
+#define RN_PT_WIDTH2 4u          /* ray queries: traverse the 2-wide reference tree (default: its 4-wide collapse) */
 
 /* Physical-mode materials. */
 #define RN_PT_LAMBERT 0
@@ -187,6 +188,37 @@ rn_status rn_pt_render(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_
  * resumable progressive render). */
 rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
                                   unsigned flags, void *stream, float *accum);
+
+/* ---- batched rendering: many scenes / cameras / resolutions in one launch ---- */
+
+typedef struct rn_pt_batch rn_pt_batch;
+
+/* One job: a scene seen through a camera with its own settings (spp, depth,
+ * seed, sample_offset; the integrator field is ignored, the batch's applies). */
+typedef struct {
+	rn_scene *scene;
+	rn_pt_camera camera;
+	rn_pt_settings settings;
+} rn_pt_job;
+
+/* Build a batch. RN_PT_WAVEFRONT packs every job's paths into one wave
+ * schedule whose whole frame is captured once as a CUDA graph and replayed;
+ * RN_PT_MEGAKERNEL renders the jobs one megakernel launch after another;
+ * RN_PT_AUTO lets the autotuner choose. flags: RN_PT_ORDER_NEAREST. The batch
+ * keeps pointers to the scenes, which must outlive it. */
+rn_status rn_pt_batch_create(const rn_pt_job *jobs, int n, int integrator, unsigned flags, rn_pt_batch **out);
+
+/* Render every job once. sample_offset is added to each job's own offset
+ * (progressive frames). out[j] receives job j's mean radiance, width*height*3
+ * floats; with RN_PT_DEVICE_POINTERS the out[j] are device pointers and the
+ * work is enqueued on `stream` without a host synchronisation. */
+rn_status rn_pt_batch_render(rn_pt_batch *batch, unsigned sample_offset, unsigned flags, void *stream,
+                             float *const *out);
+
+/* The integrator the batch runs (after RN_PT_AUTO was resolved). */
+int rn_pt_batch_integrator(const rn_pt_batch *batch);
+
+void rn_pt_batch_free(rn_pt_batch *batch);
 
 /* Profiling counters of the reference traversal algorithm (src/BVH.cpp:77-139,
  * box tests counted when a node is popped) over the rays of one render with

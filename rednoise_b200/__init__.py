@@ -247,8 +247,9 @@ class Scene:
                                                _ptr(links)), "dump_bvh")
         return {"order": order, "bounds": bounds, "links": links}
 
-    def trace_closest(self, origins, directions, ignore=None, nearest_first: bool = False):
-        """Closest hit per ray: (tri, t, u, v) numpy arrays (tri = -1 on a miss)."""
+    def trace_closest(self, origins, directions, ignore=None, nearest_first: bool = False, width2: bool = False):
+        """Closest hit per ray: (tri, t, u, v) numpy arrays (tri = -1 on a miss).
+        ``width2`` traverses the 2-wide reference tree instead of its 4-wide collapse."""
         self._check_open()
         o = _f32(origins, 3).reshape(-1, 3)
         d = _f32(directions, 3).reshape(-1, 3)
@@ -260,12 +261,12 @@ class Scene:
         t = np.empty(n, np.float32)
         u = np.empty(n, np.float32)
         v = np.empty(n, np.float32)
-        flags = _native.RN_PT_ORDER_NEAREST if nearest_first else 0
+        flags = (_native.RN_PT_ORDER_NEAREST if nearest_first else 0) | (_native.RN_PT_WIDTH2 if width2 else 0)
         _native.check(_native.load().rn_pt_trace_closest(self._handle, n, _ptr(o), _ptr(d), _ptr(ig), flags, None,
                                                          _ptr(tri), _ptr(t), _ptr(u), _ptr(v)), "trace_closest")
         return tri, t, u, v
 
-    def trace_any(self, origins, directions, tmax, ignore=None) -> np.ndarray:
+    def trace_any(self, origins, directions, tmax, ignore=None, width2: bool = False) -> np.ndarray:
         """Occlusion per ray (1 if anything is hit strictly before ``tmax``)."""
         self._check_open()
         o = _f32(origins, 3).reshape(-1, 3)
@@ -276,8 +277,9 @@ class Scene:
             raise ValueError("tmax must have one value per ray")
         ig = None if ignore is None else _i32(ignore).reshape(-1)
         occ = np.empty(n, np.int32)
-        _native.check(_native.load().rn_pt_trace_any(self._handle, n, _ptr(o), _ptr(d), _ptr(tm), _ptr(ig), 0, None,
-                                                     _ptr(occ)), "trace_any")
+        flags = _native.RN_PT_WIDTH2 if width2 else 0
+        _native.check(_native.load().rn_pt_trace_any(self._handle, n, _ptr(o), _ptr(d), _ptr(tm), _ptr(ig), flags,
+                                                     None, _ptr(occ)), "trace_any")
         return occ
 
     def render_reference(
@@ -331,7 +333,7 @@ class Scene:
                                                             _ptr(mean)), "render_reference")
         return (canvas, mean) if want_mean else canvas
 
-    def render_physical(self, camera: "Camera", settings: "Settings", nearest_first: bool = True,
+    def render_physical(self, camera: "Camera", settings: "Settings", nearest_first: bool = False,
                         out: Optional[np.ndarray] = None) -> np.ndarray:
         """Physical-mode render: per-pixel mean radiance as (height, width, 3) float32."""
         self._check_open()
@@ -342,7 +344,7 @@ class Scene:
         return rgb
 
     def accumulate(self, camera: "Camera", settings: "Settings", accum: np.ndarray,
-                   nearest_first: bool = True) -> np.ndarray:
+                   nearest_first: bool = False) -> np.ndarray:
         """Add the per-pixel sum of the settings' samples to ``accum`` (float32, in place)."""
         self._check_open()
         if accum.dtype != np.float32 or not accum.flags.c_contiguous or accum.size != camera.width * camera.height * 3:
@@ -396,6 +398,59 @@ class Scene:
         if not self._handle:
             return "<rednoise_b200.Scene closed>"
         return f"<rednoise_b200.Scene handle=0x{self._handle:x}>"
+
+
+class Batch:
+    """Many (scene, camera, settings) jobs rendered per launch (rn_pt_batch_*).
+
+    With ``integrator=RN_PT_WAVEFRONT`` all jobs share one wave schedule whose
+    frame is captured once as a CUDA graph and replayed on every ``render``.
+    """
+
+    def __init__(self, jobs, integrator: int = _native.RN_PT_AUTO, nearest_first: bool = False):
+        self._scenes = [j[0] for j in jobs]  # keep the scenes alive
+        arr = (_native.Job * len(jobs))()
+        for i, (scene, camera, settings) in enumerate(jobs):
+            arr[i].scene = scene.handle
+            arr[i].camera = camera
+            arr[i].settings = settings
+        self._shapes = [(c.height, c.width, 3) for _, c, _ in jobs]
+        out = ctypes.c_void_p()
+        flags = _native.RN_PT_ORDER_NEAREST if nearest_first else 0
+        _native.check(_native.load().rn_pt_batch_create(arr, len(jobs), integrator, flags, ctypes.byref(out)),
+                      "rn_pt_batch_create")
+        self._handle = out.value
+
+    @property
+    def integrator(self) -> int:
+        return int(_native.load().rn_pt_batch_integrator(self._handle))
+
+    def render(self, sample_offset: int = 0, outs=None):
+        """Render every job; returns a list of (h, w, 3) float32 mean images."""
+        outs = outs if outs is not None else [np.empty(s, np.float32) for s in self._shapes]
+        ptrs = (ctypes.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+        _native.check(_native.load().rn_pt_batch_render(self._handle, int(sample_offset), 0, None, ptrs),
+                      "rn_pt_batch_render")
+        return outs
+
+    def render_device(self, outs, stream_handle: int = 0, sample_offset: int = 0) -> None:
+        """Asynchronous render into device buffers (sequence of data pointers)."""
+        ptrs = (ctypes.c_void_p * len(outs))(*outs)
+        _native.check(_native.load().rn_pt_batch_render(self._handle, int(sample_offset),
+                                                        _native.RN_PT_DEVICE_POINTERS,
+                                                        ctypes.c_void_p(stream_handle) if stream_handle else None,
+                                                        ptrs), "rn_pt_batch_render")
+
+    def close(self) -> None:
+        if self._handle and _native._LIB is not None:
+            _native._LIB.rn_pt_batch_free(self._handle)
+        self._handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def version() -> str:

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(_HERE, "librednoise_b200.so")
 RN_OK = 0
 RN_PT_DEVICE_POINTERS = 1
 RN_PT_ORDER_NEAREST = 2
+RN_PT_WIDTH2 = 4
 
 STATUS_NAMES = {
     0: "RN_OK",
@@ -182,6 +183,12 @@ class Settings(ctypes.Structure):
         return s
 
 
+class Job(ctypes.Structure):
+    """rn_pt_job: scene + camera + settings."""
+
+    _fields_ = [("scene", vp), ("camera", Camera), ("settings", Settings)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     # drop-in ABI (include/rednoise/rednoise.h)
@@ -206,6 +213,11 @@ SIGNATURES = {
     "rn_pt_render_accumulate": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                                vp, vp]),
     "rn_pt_count_traversal": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), vp]),
+    "rn_pt_batch_create": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.c_int, ctypes.c_int, ctypes.c_uint,
+                                          ctypes.POINTER(vp)]),
+    "rn_pt_batch_render": (ctypes.c_int, [vp, ctypes.c_uint, ctypes.c_uint, vp, ctypes.POINTER(vp)]),
+    "rn_pt_batch_integrator": (ctypes.c_int, [vp]),
+    "rn_pt_batch_free": (None, [vp]),
     "rn_pt_last_error": (ctypes.c_char_p, []),
 }
 

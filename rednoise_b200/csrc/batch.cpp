@@ -1,0 +1,200 @@
+// Batched rendering of many jobs (scene + camera + settings) per launch.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "pt_kernels.hpp"
+#include "render_impl.hpp"
+#include "scene_impl.hpp"
+
+struct rn_pt_batch {
+	std::vector<rn_pt_job> jobs;
+	std::vector<rnb::WfJob> wf_jobs; // kernel inputs, accum pointers into `accum`
+	std::vector<long> offsets;       // float offset of each job's image in accum / mean
+	rnb::DevBuf accum, mean, status;
+	rnb::WfContext wf;
+	cudaStream_t stream = nullptr;
+	int integrator = RN_PT_WAVEFRONT;
+	int order = 0;
+	int max_depth = 1;
+	int spw = 1;
+	long total_floats = 0;
+	~rn_pt_batch() {
+		if (stream)
+			cudaStreamDestroy(stream);
+	}
+};
+
+using namespace rnb;
+
+namespace {
+
+rn_status batch_enqueue(rn_pt_batch *b, unsigned sample_offset, cudaStream_t cs) {
+	std::vector<WfJob> jobs = b->wf_jobs;
+	for (size_t i = 0; i < jobs.size(); i++)
+		jobs[i].st.sample_offset = b->jobs[i].settings.sample_offset + sample_offset;
+	int *status = b->status.as<int>();
+	if (b->integrator == RN_PT_WAVEFRONT) {
+		rn_status r = b->wf.configure(jobs, b->max_depth, b->order, b->spw, cs);
+		if (r != RN_OK)
+			return r;
+		return b->wf.launch_graph(status, cs);
+	}
+	// Plain GPU baseline: one megakernel launch per job.
+	RNB_CUDA(cudaMemsetAsync(b->accum.p, 0, static_cast<size_t>(b->total_floats) * sizeof(float), cs));
+	for (size_t i = 0; i < jobs.size(); i++) {
+		rn_scene *s = b->jobs[i].scene;
+		RNB_CUDA(s->d_counter.ensure(256));
+		RNB_CUDA(launch_megakernel(jobs[i].sc, jobs[i].cam, jobs[i].st, jobs[i].accum, s->d_counter.as<unsigned>(),
+		                           status, cs));
+		const long nf = static_cast<long>(jobs[i].n_pix) * 3;
+		RNB_CUDA(launch_resolve(jobs[i].accum, b->mean.as<float>() + b->offsets[i], nf,
+		                        jobs[i].spp > 0 ? 1.0f / static_cast<float>(jobs[i].spp) : 0.0f, cs));
+	}
+	return RN_OK;
+}
+
+// Time one frame of each integrator at the batch's own sizes and keep the faster.
+rn_status autotune_batch(rn_pt_batch *b) {
+	float best = 0.0f;
+	int pick = RN_PT_WAVEFRONT;
+	cudaEvent_t e0, e1;
+	RNB_CUDA(cudaEventCreate(&e0));
+	RNB_CUDA(cudaEventCreate(&e1));
+	for (int integ : {RN_PT_MEGAKERNEL, RN_PT_WAVEFRONT}) {
+		b->integrator = integ;
+		rn_status r = batch_enqueue(b, 0x40000000u, b->stream); // warm-up (and graph capture)
+		if (r != RN_OK)
+			return r;
+		RNB_CUDA(cudaEventRecord(e0, b->stream));
+		r = batch_enqueue(b, 0x40000000u, b->stream);
+		if (r != RN_OK)
+			return r;
+		RNB_CUDA(cudaEventRecord(e1, b->stream));
+		RNB_CUDA(cudaEventSynchronize(e1));
+		float ms = 0.0f;
+		RNB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+		if (best == 0.0f || ms < best) {
+			best = ms;
+			pick = integ;
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	b->integrator = pick;
+	return RN_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+rn_status rn_pt_batch_create(const rn_pt_job *jobs, int n, int integrator, unsigned flags, rn_pt_batch **out) {
+	if (!jobs || n <= 0 || !out) {
+		set_last_error("rn_pt_batch_create: need n > 0 jobs and an output pointer");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (integrator != RN_PT_AUTO && integrator != RN_PT_MEGAKERNEL && integrator != RN_PT_WAVEFRONT) {
+		set_last_error("rn_pt_batch_create: unknown integrator");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	*out = nullptr;
+	std::unique_ptr<rn_pt_batch> b(new (std::nothrow) rn_pt_batch());
+	if (!b)
+		return RN_ERR_OUT_OF_MEMORY;
+	b->jobs.assign(jobs, jobs + n);
+	b->order = (flags & RN_PT_ORDER_NEAREST) ? kOrderNearest : kOrderReference;
+	long total = 0;
+	int max_spp = 1;
+	long max_pix = 1;
+	for (int i = 0; i < n; i++) {
+		PhysScene ps;
+		PhysCamera pc;
+		PhysSettings pst;
+		rn_status r = make_phys_inputs(jobs[i].scene, &jobs[i].camera, &jobs[i].settings, flags, ps, pc, pst);
+		if (r != RN_OK)
+			return r;
+		if (pst.max_depth > kWfMaxDepth) {
+			set_last_error("rn_pt_batch_create: max_depth must be <= 64");
+			return RN_ERR_INVALID_ARGUMENT;
+		}
+		WfJob j;
+		j.sc = ps;
+		j.cam = pc;
+		j.st = pst;
+		j.accum = nullptr;
+		j.n_pix = pc.width * pc.height;
+		j.spp = pst.spp;
+		b->wf_jobs.push_back(j);
+		b->offsets.push_back(total);
+		total += static_cast<long>(j.n_pix) * 3;
+		b->max_depth = std::max(b->max_depth, pst.max_depth);
+		max_spp = std::max(max_spp, pst.spp);
+		max_pix = std::max(max_pix, static_cast<long>(j.n_pix));
+	}
+	b->total_floats = total;
+	RNB_CUDA(b->accum.ensure(static_cast<size_t>(total) * sizeof(float)));
+	RNB_CUDA(b->mean.ensure(static_cast<size_t>(total) * sizeof(float)));
+	RNB_CUDA(b->status.ensure(256));
+	RNB_CUDA(cudaMemset(b->status.p, 0, 256));
+	RNB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+	for (int i = 0; i < n; i++)
+		b->wf_jobs[i].accum = b->accum.as<float>() + b->offsets[i];
+	// Paths per wave: about 2^20 in flight, counting every job's pixels.
+	b->spw = default_samples_per_wave(total / 3, max_spp);
+	std::vector<WfContext::Resolve> res;
+	for (int i = 0; i < n; i++)
+		res.push_back({b->wf_jobs[i].accum, b->mean.as<float>() + b->offsets[i],
+		               static_cast<long>(b->wf_jobs[i].n_pix) * 3,
+		               b->wf_jobs[i].spp > 0 ? 1.0f / static_cast<float>(b->wf_jobs[i].spp) : 0.0f});
+	b->wf.set_frame_io(b->accum.as<float>(), static_cast<size_t>(total) * sizeof(float), res);
+	if (integrator == RN_PT_AUTO) {
+		rn_status r = autotune_batch(b.get());
+		if (r != RN_OK)
+			return r;
+	} else {
+		b->integrator = integrator;
+	}
+	*out = b.release();
+	return RN_OK;
+}
+
+rn_status rn_pt_batch_render(rn_pt_batch *b, unsigned sample_offset, unsigned flags, void *stream,
+                             float *const *out) {
+	if (!b || !out) {
+		set_last_error("rn_pt_batch_render: NULL argument");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	for (size_t i = 0; i < b->jobs.size(); i++)
+		if (!out[i]) {
+			set_last_error("rn_pt_batch_render: NULL output for a job");
+			return RN_ERR_INVALID_ARGUMENT;
+		}
+	const bool dev = (flags & RN_PT_DEVICE_POINTERS) != 0;
+	cudaStream_t cs = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+	rn_status r = batch_enqueue(b, sample_offset, cs);
+	if (r != RN_OK)
+		return r;
+	for (size_t i = 0; i < b->jobs.size(); i++) {
+		const size_t bytes = static_cast<size_t>(b->wf_jobs[i].n_pix) * 3 * sizeof(float);
+		RNB_CUDA(cudaMemcpyAsync(out[i], b->mean.as<float>() + b->offsets[i], bytes,
+		                         dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, cs));
+	}
+	if (dev)
+		return RN_OK;
+	int h = 0;
+	RNB_CUDA(cudaMemcpyAsync(&h, b->status.p, sizeof(int), cudaMemcpyDeviceToHost, cs));
+	RNB_CUDA(cudaStreamSynchronize(cs));
+	if (h) {
+		set_last_error("rn_pt_batch_render: device status word reports a traversal error");
+		return RN_ERR_INTERNAL;
+	}
+	return RN_OK;
+}
+
+int rn_pt_batch_integrator(const rn_pt_batch *b) { return b ? b->integrator : -1; }
+
+void rn_pt_batch_free(rn_pt_batch *b) { delete b; }
+
+} // extern "C"

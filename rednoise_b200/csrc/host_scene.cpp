@@ -308,6 +308,80 @@ bool load_obj(const std::string &path, float scale, TriangleSet &ts, std::string
 	return true;
 }
 
+void flatten_bvh4(const Bvh2 &bvh, DeviceLayout4 &out) {
+	out.nodes.clear();
+	if (bvh.root < 0)
+		return;
+	auto as_float = [](int i) {
+		float f;
+		std::memcpy(&f, &i, 4);
+		return f;
+	};
+	auto leaf_ref = [&](const BvhNode &nd) { return ~((nd.start << 3) | nd.count); };
+	const BvhNode &root = bvh.nodes[static_cast<size_t>(bvh.root)];
+	if (root.count > 0) {
+		out.root_ref = leaf_ref(root);
+		return;
+	}
+	// Iterative build: each work item fills node `slot` from reference node `src`.
+	std::vector<std::pair<int, int>> work; // (slot, src)
+	out.nodes.resize(8);
+	work.push_back({0, bvh.root});
+	while (!work.empty()) {
+		const auto [slot, src] = work.back();
+		work.pop_back();
+		const BvhNode &n = bvh.nodes[static_cast<size_t>(src)];
+		// Entries in pop order: right side first, and within a side its right child first.
+		int ent[4];
+		int cnt = 0;
+		for (int c : {n.right, n.left}) {
+			const BvhNode &cn = bvh.nodes[static_cast<size_t>(c)];
+			if (cn.count > 0) {
+				ent[cnt++] = c;
+			} else {
+				ent[cnt++] = cn.right;
+				ent[cnt++] = cn.left;
+			}
+		}
+		float lo[3][4], hi[3][4];
+		int refs[4];
+		for (int k = 0; k < 4; k++) {
+			for (int a = 0; a < 3; a++) {
+				lo[a][k] = 1.0f;
+				hi[a][k] = -1.0f;
+			}
+			refs[k] = 0;
+		}
+		for (int k = 0; k < cnt; k++) {
+			const BvhNode &e = bvh.nodes[static_cast<size_t>(ent[k])];
+			lo[0][k] = e.bmin.x;
+			lo[1][k] = e.bmin.y;
+			lo[2][k] = e.bmin.z;
+			hi[0][k] = e.bmax.x;
+			hi[1][k] = e.bmax.y;
+			hi[2][k] = e.bmax.z;
+			if (e.count > 0) {
+				refs[k] = leaf_ref(e);
+			} else {
+				const int child_slot = static_cast<int>(out.nodes.size() / 8);
+				out.nodes.resize(out.nodes.size() + 8);
+				refs[k] = child_slot;
+				work.push_back({child_slot, ent[k]});
+			}
+		}
+		F4 *o = &out.nodes[static_cast<size_t>(slot) * 8];
+		o[0] = {lo[0][0], lo[0][1], lo[0][2], lo[0][3]};
+		o[1] = {hi[0][0], hi[0][1], hi[0][2], hi[0][3]};
+		o[2] = {lo[1][0], lo[1][1], lo[1][2], lo[1][3]};
+		o[3] = {hi[1][0], hi[1][1], hi[1][2], hi[1][3]};
+		o[4] = {lo[2][0], lo[2][1], lo[2][2], lo[2][3]};
+		o[5] = {hi[2][0], hi[2][1], hi[2][2], hi[2][3]};
+		o[6] = {as_float(refs[0]), as_float(refs[1]), as_float(refs[2]), as_float(refs[3])};
+		o[7] = {as_float(cnt), 0.0f, 0.0f, 0.0f};
+	}
+	out.root_ref = 0;
+}
+
 void flatten_bvh(const TriangleSet &ts, const Bvh2 &bvh, DeviceLayout &out) {
 	const int n = static_cast<int>(ts.size());
 	out.nodes.clear();

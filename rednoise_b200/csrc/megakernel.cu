@@ -27,12 +27,12 @@ __global__ void __launch_bounds__(128) k_megakernel(PhysScene sc, PhysCamera cam
 				PathState ps = camera_path(cam, st, static_cast<uint32_t>(pix), st.sample_offset + static_cast<uint32_t>(s));
 				for (;;) {
 					const RayPre r = make_ray(ps.o.x, ps.o.y, ps.o.z, ps.d.x, ps.d.y, ps.d.z);
-					const HitRec h = trace_closest<kOrder>(sc.sv, r, ps.ignore, err);
+					const HitRec h = trace_closest_best<kOrder>(sc.sv, r, ps.ignore, err);
 					ShadowReq sr;
 					const bool alive = shade_vertex(sc, st, ps, h, sr);
 					if (sr.valid) {
 						const RayPre rs = make_ray(sr.o.x, sr.o.y, sr.o.z, sr.d.x, sr.d.y, sr.d.z);
-						if (!trace_any(sc.sv, rs, sr.tmax, sr.ignore, err))
+						if (!trace_any_best(sc.sv, rs, sr.tmax, sr.ignore, err))
 							ps.L = ps.L + sr.contrib;
 					}
 					if (!alive)

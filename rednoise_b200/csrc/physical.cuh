@@ -136,11 +136,32 @@ __device__ __forceinline__ F3 schlick(F3 f0, float c) {
 	return f0 + (f3(1.0f, 1.0f, 1.0f) - f0) * m5;
 }
 
+// Schlick's (1 - cos)^5 term.
+__device__ __forceinline__ float schlick_m5(float c) {
+	const float m = fminf(fmaxf(1.0f - c, 0.0f), 1.0f);
+	return (m * m) * (m * m) * m;
+}
+
+// d log(weight) / d albedo, per channel, of a vertex whose weight is linear in
+// the albedo (Lambert) or the Schlick Fresnel of F0 = albedo (GGX, m5 given).
+__device__ __forceinline__ F3 albedo_log_derivative(int mat, F3 albedo, float m5) {
+	if (mat == 0)
+		return f3(1.0f / fmaxf(albedo.x, 1e-12f), 1.0f / fmaxf(albedo.y, 1e-12f), 1.0f / fmaxf(albedo.z, 1e-12f));
+	if (mat == 1) {
+		const F3 F = albedo + (f3(1.0f, 1.0f, 1.0f) - albedo) * m5;
+		const float d = 1.0f - m5;
+		return f3(d / fmaxf(F.x, 1e-12f), d / fmaxf(F.y, 1e-12f), d / fmaxf(F.z, 1e-12f));
+	}
+	return f3(0.0f, 0.0f, 0.0f);
+}
+
 // BSDF value times |cos wi| and solid-angle pdf for a non-delta material in the
 // local frame of n (wo, wi on the same side as n). Returns false if zero.
+// m5 receives Schlick's (1 - wo.m)^5 of the GGX half vector (0 for Lambert).
 __device__ __forceinline__ bool bsdf_eval(int mat, F3 albedo, float alpha, F3 n, F3 wo, F3 wi, F3 &f_cos,
-                                          float &pdf) {
+                                          float &pdf, float &m5) {
 	const float ci = dot3(n, wi), co = dot3(n, wo);
+	m5 = 0.0f;
 	if (ci <= 0.0f || co <= 0.0f)
 		return false;
 	if (mat == 0) {
@@ -157,10 +178,26 @@ __device__ __forceinline__ bool bsdf_eval(int mat, F3 albedo, float alpha, F3 n,
 	const float lo = ggx_lambda(co, a2), li = ggx_lambda(ci, a2);
 	const float G2 = 1.0f / (1.0f + lo + li);
 	const float G1 = 1.0f / (1.0f + lo);
+	m5 = schlick_m5(om);
 	f_cos = schlick(albedo, om) * (D * G2 / (4.0f * co));
 	pdf = G1 * D / (4.0f * co);
 	return true;
 }
+
+// What the adjoint replay needs from one vertex (path replay backpropagation):
+// the terms this vertex adds and the log-derivatives of its weights.
+struct VertexGrad {
+	int tri;          // scattering triangle, -1 if none
+	int hit_emitter;  // emitter triangle hit by the incoming ray, -1 if none
+	F3 emit;          // emission added at this vertex
+	F3 Le;            // radiance of the hit emitter
+	bool nee;         // a shadow request was made
+	F3 nee_contrib;   // its contribution (added when unoccluded)
+	F3 nee_dlog;      // d log f(light direction) / d albedo
+	int nee_emitter;  // sampled emitter triangle
+	F3 nee_Le;        // its radiance
+	F3 cont_dlog;     // d log(continuation weight) / d albedo
+};
 
 __device__ __forceinline__ float power_mis(float a, float b) {
 	const float a2 = a * a, b2 = b * b;
@@ -168,10 +205,20 @@ __device__ __forceinline__ float power_mis(float a, float b) {
 }
 
 // Shade the vertex the path's ray hit (h), add emission, build the NEE shadow
-// request, sample the continuation. Returns whether the path continues.
-__device__ __forceinline__ bool shade_vertex(const PhysScene &sc, const PhysSettings &st, PathState &ps,
-                                             const HitRec &h, ShadowReq &sr) {
+// request, sample the continuation. Returns whether the path continues. With
+// kGrad the terms the adjoint replay needs are recorded in *vg; the decisions
+// and arithmetic of the primal are the same either way.
+template <bool kGrad>
+__device__ __forceinline__ bool shade_vertex_t(const PhysScene &sc, const PhysSettings &st, PathState &ps,
+                                               const HitRec &h, ShadowReq &sr, VertexGrad *vg) {
 	sr.valid = false;
+	if (kGrad) {
+		vg->tri = -1;
+		vg->hit_emitter = -1;
+		vg->nee = false;
+		vg->nee_emitter = -1;
+		vg->cont_dlog = f3(0.0f, 0.0f, 0.0f);
+	}
 	if (h.idx < 0) {
 		ps.L = ps.L + ps.beta * f3(st.env[0], st.env[1], st.env[2]);
 		return false;
@@ -191,10 +238,18 @@ __device__ __forceinline__ bool shade_vertex(const PhysScene &sc, const PhysSett
 				const float pdf_light = h.t * h.t / (cos_o_g * sc.emit_area_total);
 				w = power_mis(ps.prev_pdf, pdf_light);
 			}
-			ps.L = ps.L + ps.beta * Le * w;
+			const F3 e = ps.beta * Le * w;
+			ps.L = ps.L + e;
+			if (kGrad) {
+				vg->hit_emitter = h.idx;
+				vg->emit = e;
+				vg->Le = Le;
+			}
 		}
 		return false;
 	}
+	if (kGrad)
+		vg->tri = h.idx;
 	const int mat = __float_as_int(s0.w);
 	const F3 albedo = ld3(s0);
 	const float param = s1.w;
@@ -230,8 +285,8 @@ __device__ __forceinline__ bool shade_vertex(const PhysScene &sc, const PhysSett
 		const F3 ne = ld3(__ldg(sc.shade + 3 * static_cast<size_t>(etri) + 2));
 		const float cos_l = -dot3(ne, wi);
 		F3 f_cos;
-		float pdf_b;
-		if (cos_l > 0.0f && dist > 0.0f && bsdf_eval(mat, albedo, param, n, wo, wi, f_cos, pdf_b)) {
+		float pdf_b, m5;
+		if (cos_l > 0.0f && dist > 0.0f && bsdf_eval(mat, albedo, param, n, wo, wi, f_cos, pdf_b, m5)) {
 			const float pdf_l = dist2 / (cos_l * sc.emit_area_total);
 			const F3 eLe = ld3(__ldg(sc.shade + 3 * static_cast<size_t>(etri) + 1));
 			const float w = power_mis(pdf_l, pdf_b);
@@ -241,6 +296,13 @@ __device__ __forceinline__ bool shade_vertex(const PhysScene &sc, const PhysSett
 			sr.ignore = etri;
 			sr.contrib = ps.beta * f_cos * eLe * (w / pdf_l);
 			sr.valid = true;
+			if (kGrad) {
+				vg->nee = true;
+				vg->nee_contrib = sr.contrib;
+				vg->nee_dlog = albedo_log_derivative(mat, albedo, m5);
+				vg->nee_emitter = etri;
+				vg->nee_Le = eLe;
+			}
 		}
 	}
 	if (ps.bounce + 1 >= st.max_depth)
@@ -263,6 +325,8 @@ __device__ __forceinline__ bool shade_vertex(const PhysScene &sc, const PhysSett
 			return false;
 		weight = albedo;
 		pdf = ci * 0.318309886183791f;
+		if (kGrad)
+			vg->cont_dlog = albedo_log_derivative(0, albedo, 0.0f);
 	} else if (mat == 1) {
 		const float alpha = param, a2 = alpha * alpha;
 		F3 t, bt;
@@ -293,6 +357,8 @@ __device__ __forceinline__ bool shade_vertex(const PhysScene &sc, const PhysSett
 		const float G2 = 1.0f / (1.0f + lo_ + li_);
 		weight = schlick(albedo, om) * (G2 / G1);
 		pdf = G1 * ggx_D(ml.z, a2) / (4.0f * co);
+		if (kGrad)
+			vg->cont_dlog = albedo_log_derivative(1, albedo, schlick_m5(om));
 	} else {
 		// Smooth dielectric: exact Fresnel, choose reflection with probability F.
 		const float eta = param;
@@ -330,6 +396,11 @@ __device__ __forceinline__ bool shade_vertex(const PhysScene &sc, const PhysSett
 	ps.ignore = h.idx;
 	ps.bounce++;
 	return true;
+}
+
+__device__ __forceinline__ bool shade_vertex(const PhysScene &sc, const PhysSettings &st, PathState &ps,
+                                             const HitRec &h, ShadowReq &sr) {
+	return shade_vertex_t<false>(sc, st, ps, h, sr, nullptr);
 }
 
 #endif // __CUDACC__

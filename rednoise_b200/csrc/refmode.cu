@@ -185,7 +185,7 @@ struct Hit {
 
 __device__ __forceinline__ Hit intersect(Ctx &c, V3 o, V3 d, int ignore) {
 	const RayPre r = make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
-	const HitRec h = trace_closest<kOrderReference>(c.sv, r, ignore, c.err);
+	const HitRec h = trace_closest_best<kOrderReference>(c.sv, r, ignore, c.err);
 	Hit out;
 	out.hit = h.idx >= 0;
 	out.idx = h.idx;
@@ -195,7 +195,7 @@ __device__ __forceinline__ Hit intersect(Ctx &c, V3 o, V3 d, int ignore) {
 }
 __device__ __forceinline__ bool occluded(Ctx &c, V3 o, V3 d, float maxd, int ignore) {
 	const RayPre r = make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
-	return trace_any(c.sv, r, maxd, ignore, c.err);
+	return trace_any_best(c.sv, r, maxd, ignore, c.err);
 }
 
 __device__ __forceinline__ V3 l3(const float *a) { return mk(a[0], a[1], a[2]); }

@@ -94,8 +94,25 @@ namespace {
 rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, const PhysScene &ps, const PhysCamera &pc,
                          const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
 	if (st->integrator == RN_PT_WAVEFRONT) {
-		set_last_error("render: the wavefront integrator is not available in this build");
-		return RN_ERR_UNSUPPORTED;
+		if (pst.max_depth > kWfMaxDepth) {
+			set_last_error("render: the wavefront integrator supports max_depth <= 64");
+			return RN_ERR_INVALID_ARGUMENT;
+		}
+		if (!s->wf)
+			s->wf.reset(new WfContext());
+		WfJob job;
+		job.sc = ps;
+		job.cam = pc;
+		job.st = pst;
+		job.accum = d_accum;
+		job.n_pix = pc.width * pc.height;
+		job.spp = pst.spp;
+		s->wf->set_frame_io(nullptr, 0, {});
+		rn_status r = s->wf->configure({job}, pst.max_depth, pst.order, default_samples_per_wave(job.n_pix, job.spp),
+		                               cs);
+		if (r != RN_OK)
+			return r;
+		return s->wf->launch_graph(s->d_status.as<int>(), cs);
 	}
 	RNB_CUDA(s->d_counter.ensure(256));
 	RNB_CUDA(launch_megakernel(ps, pc, pst, d_accum, s->d_counter.as<unsigned>(), s->d_status.as<int>(), cs));

@@ -110,7 +110,10 @@ rn_status prepare_scene(rn_scene *s) {
 			return cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
 		return cudaSuccess;
 	};
+	DeviceLayout4 lay4;
+	flatten_bvh4(s->bvh, lay4);
 	RNB_CUDA(up(s->d_nodes, lay.nodes.data(), lay.nodes.size() * sizeof(F4)));
+	RNB_CUDA(up(s->d_nodes4, lay4.nodes.data(), lay4.nodes.size() * sizeof(F4)));
 	RNB_CUDA(up(s->d_tris, lay.tris.data(), lay.tris.size() * sizeof(F4)));
 	RNB_CUDA(up(s->d_ref_shade, ref.data(), ref.size() * sizeof(F4)));
 	RNB_CUDA(up(s->d_phys_shade, phys.data(), phys.size() * sizeof(F4)));
@@ -120,6 +123,8 @@ rn_status prepare_scene(rn_scene *s) {
 
 	SceneView v{};
 	v.nodes = s->d_nodes.as<float4>();
+	v.nodes4 = lay4.nodes.empty() ? nullptr : s->d_nodes4.as<float4>();
+	v.root4_ref = lay4.root_ref;
 	v.tris = s->d_tris.as<float4>();
 	for (int a = 0; a < 3; a++) {
 		v.root_lo[a] = lay.root_lo[a];
@@ -387,6 +392,9 @@ rn_status rn_pt_trace_closest(rn_scene *scene, int n, const float *origins, cons
 		return st;
 	const int order = (flags & RN_PT_ORDER_NEAREST) ? kOrderNearest : kOrderReference;
 	cudaStream_t cs = pick_stream(scene, stream);
+	SceneView view = scene->view;
+	if (flags & RN_PT_WIDTH2)
+		view.nodes4 = nullptr;
 	std::lock_guard<std::mutex> lock(scene->scratch_mu);
 	const size_t nn = static_cast<size_t>(n);
 	RNB_CUDA(scene->scratch.ensure(nn * 4 * 13 + 256 * 12));
@@ -394,7 +402,7 @@ rn_status rn_pt_trace_closest(rn_scene *scene, int n, const float *origins, cons
 	int *d_err = sg.take<int>(1);
 	RNB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), cs));
 	if (flags & RN_PT_DEVICE_POINTERS) {
-		RNB_CUDA(launch_trace_closest(scene->view, n, origins, directions, ignore, order, tri, t, u, v,
+		RNB_CUDA(launch_trace_closest(view, n, origins, directions, ignore, order, tri, t, u, v,
 		                              scene->d_status.as<int>(), cs));
 		return RN_OK;
 	}
@@ -406,7 +414,7 @@ rn_status rn_pt_trace_closest(rn_scene *scene, int n, const float *origins, cons
 	RNB_CUDA(cudaMemcpyAsync(d_d, directions, 12 * nn, cudaMemcpyHostToDevice, cs));
 	if (d_ig)
 		RNB_CUDA(cudaMemcpyAsync(d_ig, ignore, 4 * nn, cudaMemcpyHostToDevice, cs));
-	RNB_CUDA(launch_trace_closest(scene->view, n, d_o, d_d, d_ig, order, d_tri, d_t, d_u, d_v, d_err, cs));
+	RNB_CUDA(launch_trace_closest(view, n, d_o, d_d, d_ig, order, d_tri, d_t, d_u, d_v, d_err, cs));
 	RNB_CUDA(cudaMemcpyAsync(tri, d_tri, 4 * nn, cudaMemcpyDeviceToHost, cs));
 	if (t)
 		RNB_CUDA(cudaMemcpyAsync(t, d_t, 4 * nn, cudaMemcpyDeviceToHost, cs));
@@ -427,6 +435,9 @@ rn_status rn_pt_trace_any(rn_scene *scene, int n, const float *origins, const fl
 	if (st != RN_OK || n == 0)
 		return st;
 	cudaStream_t cs = pick_stream(scene, stream);
+	SceneView view = scene->view;
+	if (flags & RN_PT_WIDTH2)
+		view.nodes4 = nullptr;
 	std::lock_guard<std::mutex> lock(scene->scratch_mu);
 	const size_t nn = static_cast<size_t>(n);
 	RNB_CUDA(scene->scratch.ensure(nn * 4 * 10 + 256 * 8));
@@ -434,7 +445,7 @@ rn_status rn_pt_trace_any(rn_scene *scene, int n, const float *origins, const fl
 	int *d_err = sg.take<int>(1);
 	RNB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), cs));
 	if (flags & RN_PT_DEVICE_POINTERS) {
-		RNB_CUDA(launch_trace_any(scene->view, n, origins, directions, tmax, ignore, occluded,
+		RNB_CUDA(launch_trace_any(view, n, origins, directions, tmax, ignore, occluded,
 		                          scene->d_status.as<int>(), cs));
 		return RN_OK;
 	}
@@ -446,7 +457,7 @@ rn_status rn_pt_trace_any(rn_scene *scene, int n, const float *origins, const fl
 	RNB_CUDA(cudaMemcpyAsync(d_tm, tmax, 4 * nn, cudaMemcpyHostToDevice, cs));
 	if (d_ig)
 		RNB_CUDA(cudaMemcpyAsync(d_ig, ignore, 4 * nn, cudaMemcpyHostToDevice, cs));
-	RNB_CUDA(launch_trace_any(scene->view, n, d_o, d_d, d_tm, d_ig, d_occ, d_err, cs));
+	RNB_CUDA(launch_trace_any(view, n, d_o, d_d, d_tm, d_ig, d_occ, d_err, cs));
 	RNB_CUDA(cudaMemcpyAsync(occluded, d_occ, 4 * nn, cudaMemcpyDeviceToHost, cs));
 	return check_status_word(d_err, cs, "rn_pt_trace_any");
 }

@@ -3,12 +3,14 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <mutex>
 #include <vector>
 
 #include "common.cuh"
 #include "host_scene.hpp"
 #include "traverse.cuh"
+#include "wavefront_host.hpp"
 
 // Per-triangle shading records, indexed by original triangle index.
 //  ref:  (normal.xyz, reference Material as int bits), (r, g, b in 0..255, roughness)
@@ -24,7 +26,7 @@ struct rn_scene {
 
 	int device = -1;
 	cudaStream_t stream = nullptr;
-	rnb::DevBuf d_nodes, d_tris, d_ref_shade, d_phys_shade, d_emitters;
+	rnb::DevBuf d_nodes, d_nodes4, d_tris, d_ref_shade, d_phys_shade, d_emitters;
 	rnb::DevBuf d_status; // error word for asynchronous (device-pointer) calls
 	rnb::SceneView view{};
 	int n_emitters = 0;
@@ -37,6 +39,8 @@ struct rn_scene {
 	// device-pointer renders (calls on one scene are serialised on its stream).
 	rnb::DevBuf d_counter;
 	rnb::DevBuf accum;
+	// Wavefront pools and the captured frame graph of single-scene renders.
+	std::unique_ptr<rnb::WfContext> wf;
 
 	~rn_scene();
 };

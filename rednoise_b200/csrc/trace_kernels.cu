@@ -13,7 +13,7 @@ __global__ void __launch_bounds__(128) k_trace_closest(SceneView s, int n, const
 		return;
 	const RayPre r = make_ray(o[3 * i], o[3 * i + 1], o[3 * i + 2], d[3 * i], d[3 * i + 1], d[3 * i + 2]);
 	int e = 0;
-	const HitRec h = trace_closest<kOrder>(s, r, ignore ? ignore[i] : -1, e);
+	const HitRec h = trace_closest_best<kOrder>(s, r, ignore ? ignore[i] : -1, e);
 	if (e)
 		atomicOr(err, 1);
 	tri[i] = h.idx;
@@ -33,7 +33,7 @@ __global__ void __launch_bounds__(128) k_trace_any(SceneView s, int n, const flo
 		return;
 	const RayPre r = make_ray(o[3 * i], o[3 * i + 1], o[3 * i + 2], d[3 * i], d[3 * i + 1], d[3 * i + 2]);
 	int e = 0;
-	const bool hit = trace_any(s, r, tmax[i], ignore ? ignore[i] : -1, e);
+	const bool hit = trace_any_best(s, r, tmax[i], ignore ? ignore[i] : -1, e);
 	if (e)
 		atomicOr(err, 1);
 	occ[i] = hit ? 1 : 0;

@@ -31,11 +31,13 @@ namespace rnb {
 constexpr int kStack = 64; // same bound as the reference's int stack[64]
 
 struct SceneView {
-	const float4 *__restrict__ nodes; // 4 float4 per internal node
-	const float4 *__restrict__ tris;  // 3 float4 per triangle position
+	const float4 *__restrict__ nodes;  // 4 float4 per internal node (2-wide)
+	const float4 *__restrict__ nodes4; // 8 float4 per node (4-wide collapse), may be null
+	const float4 *__restrict__ tris;   // 3 float4 per triangle position
 	float root_lo[3];
 	float root_hi[3];
 	int root_ref;
+	int root4_ref;
 	int n_tris;
 };
 
@@ -330,6 +332,176 @@ __device__ __forceinline__ bool trace_any(const SceneView &s, const RayPre &r, f
 		}
 	}
 	return false;
+}
+
+// ---- 4-wide traversal in the reference's order ---------------------------------
+// Entries of a node are stored in the order the reference pops them; entries
+// 1..count-1 are pushed (last first) and entry 0 is descended into at once,
+// which is the reference's push-then-pop. Every box is a reference node box and
+// is tested with the reference's slab arithmetic; a skipped intermediate box is
+// implied by its children's tests (monotone rounding), so closest hit and
+// occlusion equal the reference's. Rays with an infinite 1/d component (a zero
+// or subnormal direction component, where a slab product can be NaN) take the
+// 2-wide path instead.
+
+__device__ __forceinline__ bool finite_inverse(const RayPre &r) {
+	return fabsf(r.ix) < __int_as_float(0x7f800000) && fabsf(r.iy) < __int_as_float(0x7f800000) &&
+	       fabsf(r.iz) < __int_as_float(0x7f800000);
+}
+
+__device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPre &r, int ignore, int &err) {
+	HitRec h;
+	h.idx = -1;
+	h.rank = 0x7fffffff;
+	h.t = __int_as_float(0x7f800000);
+	h.u = 0.0f;
+	h.v = 0.0f;
+	int st_ref[kStack];
+	float st_t[kStack];
+	int sp = 0;
+	float te;
+	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te)) {
+		st_ref[0] = s.root4_ref;
+		st_t[0] = te;
+		sp = 1;
+	}
+	while (sp > 0) {
+		--sp;
+		int ref = st_ref[sp];
+		if (!(st_t[sp] < h.t))
+			continue;
+		while (ref >= 0) {
+			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ref);
+			const float4 lx = __ldg(nd + 0), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
+			const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5), rf = __ldg(nd + 6);
+			const int cnt = __float_as_int(__ldg(nd + 7).x);
+			float t0, t1, t2, t3;
+			const bool b0 = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, t0);
+			const bool b1 = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, t1);
+			const bool b2 = cnt > 2 && slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, t2);
+			const bool b3 = cnt > 3 && slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, t3);
+			if (sp + 3 > kStack) {
+				err = 1;
+				return h;
+			}
+			if (b3) {
+				st_ref[sp] = __float_as_int(rf.w);
+				st_t[sp] = t3;
+				++sp;
+			}
+			if (b2) {
+				st_ref[sp] = __float_as_int(rf.z);
+				st_t[sp] = t2;
+				++sp;
+			}
+			if (b1) {
+				st_ref[sp] = __float_as_int(rf.y);
+				st_t[sp] = t1;
+				++sp;
+			}
+			if (b0 && t0 < h.t) {
+				ref = __float_as_int(rf.x);
+			} else {
+				ref = 0x7fffffff;
+				break;
+			}
+		}
+		if (ref == 0x7fffffff)
+			continue;
+		const int start = leaf_start(ref);
+		const int count = leaf_count(ref);
+		for (int p = start; p < start + count; p++) {
+			const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
+			const float4 a = __ldg(tp + 0);
+			const int ti = __float_as_int(a.w);
+			if (ti == ignore)
+				continue;
+			const float4 b = __ldg(tp + 1);
+			const float4 c = __ldg(tp + 2);
+			float t, u, v;
+			if (tri_test(a, b, c, r, t, u, v) && t < h.t) {
+				h.idx = ti;
+				h.t = t;
+				h.u = u;
+				h.v = v;
+				h.rank = __float_as_int(b.w);
+			}
+		}
+	}
+	return h;
+}
+
+__device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err) {
+	int st[kStack];
+	int sp = 0;
+	float te;
+	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te) &&
+	    te < tmax) {
+		st[0] = s.root4_ref;
+		sp = 1;
+	}
+	while (sp > 0) {
+		int ref = st[--sp];
+		while (ref >= 0) {
+			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ref);
+			const float4 lx = __ldg(nd + 0), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
+			const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5), rf = __ldg(nd + 6);
+			const int cnt = __float_as_int(__ldg(nd + 7).x);
+			float t0, t1, t2, t3;
+			const bool b0 = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, t0) && t0 < tmax;
+			const bool b1 = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, t1) && t1 < tmax;
+			const bool b2 = cnt > 2 && slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, t2) && t2 < tmax;
+			const bool b3 = cnt > 3 && slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, t3) && t3 < tmax;
+			if (sp + 3 > kStack) {
+				err = 1;
+				return false;
+			}
+			if (b3)
+				st[sp++] = __float_as_int(rf.w);
+			if (b2)
+				st[sp++] = __float_as_int(rf.z);
+			if (b1)
+				st[sp++] = __float_as_int(rf.y);
+			if (b0) {
+				ref = __float_as_int(rf.x);
+			} else if (sp > 0) {
+				ref = st[--sp];
+			} else {
+				ref = 0x7fffffff;
+				break;
+			}
+		}
+		if (ref == 0x7fffffff)
+			continue;
+		const int start = leaf_start(ref);
+		const int count = leaf_count(ref);
+		for (int p = start; p < start + count; p++) {
+			const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
+			const float4 a = __ldg(tp + 0);
+			if (__float_as_int(a.w) == ignore)
+				continue;
+			const float4 b = __ldg(tp + 1);
+			const float4 c = __ldg(tp + 2);
+			float t, u, v;
+			if (tri_test(a, b, c, r, t, u, v) && t < tmax)
+				return true;
+		}
+	}
+	return false;
+}
+
+// Closest hit / occlusion with the fastest layout that keeps the reference result.
+template <int kOrder>
+__device__ __forceinline__ HitRec trace_closest_best(const SceneView &s, const RayPre &r, int ignore, int &err) {
+	if (kOrder == kOrderReference && s.nodes4 && finite_inverse(r))
+		return trace_closest4(s, r, ignore, err);
+	return trace_closest<kOrder>(s, r, ignore, err);
+}
+
+__device__ __forceinline__ bool trace_any_best(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err) {
+	if (s.nodes4 && finite_inverse(r))
+		return trace_any4(s, r, tmax, ignore, err);
+	return trace_any(s, r, tmax, ignore, err);
 }
 
 // Instrumented emulation of the reference traversal (src/BVH.cpp:77-139) for

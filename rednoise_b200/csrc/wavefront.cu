@@ -1,0 +1,224 @@
+// Wavefront integrator kernels (see wavefront.cuh).
+#include "wavefront.cuh"
+
+namespace rnb {
+
+namespace {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+	unsigned m;
+	asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+	return m;
+}
+
+// Warp-aggregated append: one atomicAdd per warp for all lanes with pred set.
+__device__ __forceinline__ unsigned warp_append(unsigned *ctr, bool pred) {
+	const unsigned active = __activemask();
+	const unsigned ballot = __ballot_sync(active, pred);
+	const int leader = __ffs(active) - 1;
+	const int lane = threadIdx.x & 31;
+	unsigned base = 0;
+	if (lane == leader && ballot)
+		base = atomicAdd(ctr, static_cast<unsigned>(__popc(ballot)));
+	base = __shfl_sync(active, base, leader);
+	return base + static_cast<unsigned>(__popc(ballot & lanemask_lt()));
+}
+
+// Last entry of a sorted base table that is <= x.
+__device__ __forceinline__ int find_base(const int *bases, int n, int x) {
+	int lo = 0, hi = n - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (bases[mid] <= x)
+			lo = mid;
+		else
+			hi = mid - 1;
+	}
+	return lo;
+}
+
+__global__ void __launch_bounds__(256) k_wf_camera(const WfJob *__restrict__ jobs, WfPool pool, WfWave wave) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < wave.n_slots; i += gridDim.x * blockDim.x) {
+		const int a = find_base(wave.bases, wave.n_jobs, i);
+		const int j = wave.jobs[a];
+		const WfJob &job = jobs[j];
+		const int rel = i - wave.bases[a];
+		const uint32_t pixel = static_cast<uint32_t>(rel % job.n_pix);
+		const uint32_t sample =
+		    job.st.sample_offset + static_cast<uint32_t>(wave.first_sample + rel / job.n_pix);
+		const PathState ps = camera_path(job.cam, job.st, pixel, sample);
+		pool.o[i] = make_float4(ps.o.x, ps.o.y, ps.o.z, __int_as_float(-1));
+		pool.d[i] = make_float4(ps.d.x, ps.d.y, ps.d.z, 0.0f);
+		pool.beta[i] = make_float4(1.0f, 1.0f, 1.0f, __int_as_float(0));
+		pool.L[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(j));
+		pool.pixel[i] = pixel;
+		pool.sample[i] = sample;
+		pool.queue[0][i] = i;
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		pool.counters[kCntRays] = static_cast<unsigned>(wave.n_slots);
+}
+
+template <int kOrder>
+__global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ jobs, WfPool pool, int k, int *status) {
+	const unsigned n = pool.counters[kCntRays + k];
+	const int *__restrict__ q = pool.queue[k & 1];
+	const int lane = threadIdx.x & 31;
+	int err = 0;
+	for (;;) {
+		unsigned base = 0;
+		if (lane == 0)
+			base = atomicAdd(pool.counters + kCntFetchExt + k, 32u);
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if (base >= n)
+			break;
+		const unsigned i = base + lane;
+		if (i < n) {
+			const int slot = q[i];
+			const float4 o = pool.o[slot];
+			const float4 d = pool.d[slot];
+			const int j = __float_as_int(pool.L[slot].w);
+			const RayPre r = make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
+			const HitRec h = trace_closest_best<kOrder>(jobs[j].sc.sv, r, __float_as_int(o.w), err);
+			pool.hit_idx[slot] = h.idx;
+			pool.hit_t[slot] = h.t;
+		}
+	}
+	if (err)
+		atomicOr(status, 1);
+}
+
+__global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k) {
+	const unsigned n = pool.counters[kCntRays + k];
+	const int *__restrict__ q = pool.queue[k & 1];
+	int *__restrict__ qn = pool.queue[(k + 1) & 1];
+	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		const int slot = q[i];
+		const float4 o = pool.o[slot], d = pool.d[slot], b = pool.beta[slot], L = pool.L[slot];
+		const int j = __float_as_int(L.w);
+		const WfJob &job = jobs[j];
+		PathState ps;
+		ps.o = f3(o.x, o.y, o.z);
+		ps.d = f3(d.x, d.y, d.z);
+		ps.beta = f3(b.x, b.y, b.z);
+		ps.L = f3(L.x, L.y, L.z);
+		ps.prev_pdf = d.w;
+		ps.ignore = __float_as_int(o.w);
+		ps.bounce = __float_as_int(b.w);
+		ps.pixel = pool.pixel[slot];
+		ps.sample = pool.sample[slot];
+		HitRec h;
+		h.idx = pool.hit_idx[slot];
+		h.t = pool.hit_t[slot];
+		h.u = h.v = 0.0f;
+		h.rank = 0;
+		ShadowReq sr;
+		const bool alive = shade_vertex(job.sc, job.st, ps, h, sr);
+		const unsigned si = warp_append(pool.counters + kCntShadow + k, sr.valid);
+		if (sr.valid) {
+			pool.sh_o[si] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
+			pool.sh_d[si] = make_float4(sr.d.x, sr.d.y, sr.d.z, __int_as_float(sr.ignore));
+			pool.sh_c[si] = make_float4(sr.contrib.x, sr.contrib.y, sr.contrib.z, __int_as_float(slot));
+		}
+		const unsigned ni = warp_append(pool.counters + kCntRays + k + 1, alive);
+		pool.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, L.w);
+		if (alive) {
+			qn[ni] = slot;
+			pool.o[slot] = make_float4(ps.o.x, ps.o.y, ps.o.z, __int_as_float(ps.ignore));
+			pool.d[slot] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.prev_pdf);
+			pool.beta[slot] = make_float4(ps.beta.x, ps.beta.y, ps.beta.z, __int_as_float(ps.bounce));
+		}
+	}
+}
+
+__global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ jobs, WfPool pool, int k, int *status) {
+	const unsigned n = pool.counters[kCntShadow + k];
+	const int lane = threadIdx.x & 31;
+	int err = 0;
+	for (;;) {
+		unsigned base = 0;
+		if (lane == 0)
+			base = atomicAdd(pool.counters + kCntFetchSh + k, 32u);
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if (base >= n)
+			break;
+		const unsigned i = base + lane;
+		if (i < n) {
+			const float4 so = pool.sh_o[i], sd = pool.sh_d[i];
+			const float4 sc = pool.sh_c[i];
+			const int slot = __float_as_int(sc.w);
+			const int j = __float_as_int(pool.L[slot].w);
+			const RayPre r = make_ray(so.x, so.y, so.z, sd.x, sd.y, sd.z);
+			if (!trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err)) {
+				float4 L = pool.L[slot];
+				L.x += sc.x;
+				L.y += sc.y;
+				L.z += sc.z;
+				pool.L[slot] = L;
+			}
+		}
+	}
+	if (err)
+		atomicOr(status, 1);
+}
+
+// Adds each pixel's samples of this wave to its sum, in sample order.
+__global__ void __launch_bounds__(256) k_wf_accumulate(const WfJob *__restrict__ jobs, WfPool pool, WfWave wave) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < wave.n_pix; i += gridDim.x * blockDim.x) {
+		const int a = find_base(wave.pbases, wave.n_jobs, i);
+		const WfJob &job = jobs[wave.jobs[a]];
+		const int pixel = i - wave.pbases[a];
+		const int base = wave.bases[a] + pixel;
+		float *acc = job.accum + 3 * static_cast<size_t>(pixel);
+		float sx = acc[0], sy = acc[1], sz = acc[2];
+		for (int k = 0; k < wave.nsamp[a]; k++) {
+			const float4 L = pool.L[base + k * job.n_pix];
+			sx = sx + L.x;
+			sy = sy + L.y;
+			sz = sz + L.z;
+		}
+		acc[0] = sx;
+		acc[1] = sy;
+		acc[2] = sz;
+	}
+}
+
+} // namespace
+
+cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave &wave, int max_depth, int order,
+                           int grid_ext, int grid_shade, int grid_sh, int *status, cudaStream_t st) {
+	if (wave.n_slots <= 0)
+		return cudaSuccess;
+	cudaError_t e = cudaMemsetAsync(pool.counters, 0, kCntTotal * sizeof(unsigned), st);
+	if (e != cudaSuccess)
+		return e;
+	const int gcam = (wave.n_slots + 255) / 256 < 148 * 8 ? (wave.n_slots + 255) / 256 : 148 * 8;
+	k_wf_camera<<<gcam, 256, 0, st>>>(d_jobs, pool, wave);
+	for (int k = 0; k < max_depth; k++) {
+		if (order == kOrderNearest)
+			k_wf_extend<kOrderNearest><<<grid_ext, 128, 0, st>>>(d_jobs, pool, k, status);
+		else
+			k_wf_extend<kOrderReference><<<grid_ext, 128, 0, st>>>(d_jobs, pool, k, status);
+		k_wf_shade<<<grid_shade, 128, 0, st>>>(d_jobs, pool, k);
+		k_wf_shadow<<<grid_sh, 128, 0, st>>>(d_jobs, pool, k, status);
+	}
+	const int gacc = (wave.n_pix + 255) / 256 < 148 * 8 ? (wave.n_pix + 255) / 256 : 148 * 8;
+	k_wf_accumulate<<<gacc, 256, 0, st>>>(d_jobs, pool, wave);
+	return cudaGetLastError();
+}
+
+// Persistent grid sizes (blocks resident on all SMs).
+void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh) {
+	int dev = 0, sms = 148;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	int a = 0, b = 0, c = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_wf_extend<kOrderNearest>, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_wf_shade, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_wf_shadow, 128, 0);
+	grid_ext = sms * (a > 0 ? a : 1);
+	grid_shade = sms * (b > 0 ? b : 1);
+	grid_sh = sms * (c > 0 ? c : 1);
+}
+
+} // namespace rnb

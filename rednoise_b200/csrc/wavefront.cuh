@@ -1,0 +1,79 @@
+// Wavefront integrator: path state in structure-of-arrays pools, one kernel
+// per stage, device-side queues with warp-aggregated appends.
+//
+// A "wave" holds one sample of every pixel of every active job (a job is one
+// scene + camera + settings; a single render is a batch of one job). Stages per
+// bounce k (k = 0 .. max_depth-1), all launched with a fixed persistent grid
+// that reads its queue length from device memory, so the whole per-frame
+// sequence can be captured once as a CUDA graph:
+//   extend  : closest hit for every queued ray        (traversal only, few registers)
+//   shade   : vertex shading, NEE shadow-ray append, continuation append
+//   shadow  : any-hit for every shadow record, radiance added to the path
+// then `accumulate` adds each path's radiance to its pixel sum. Samples are
+// added in sample order per pixel, so results equal the megakernel's.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "physical.cuh"
+
+namespace rnb {
+
+constexpr int kWfMaxDepth = 64;
+
+struct WfJob {
+	PhysScene sc;
+	PhysCamera cam;
+	PhysSettings st;
+	float *accum; // 3 floats per pixel (sums)
+	int n_pix;
+	int spp;
+};
+
+// Pools of `capacity` path slots.
+struct WfPool {
+	float4 *o;    // origin.xyz, ignore (int bits)
+	float4 *d;    // direction.xyz, prev_pdf
+	float4 *beta; // throughput.xyz, bounce (int bits)
+	float4 *L;    // radiance.xyz, job (int bits)
+	uint32_t *pixel;
+	uint32_t *sample;
+	int *hit_idx;
+	float *hit_t;
+	int *rank;     // hit rank (unused by shading; kept for the closest-hit record)
+	int *queue[2]; // ray queues, alternating by bounce parity
+	float4 *sh_o;  // shadow origin.xyz, tmax
+	float4 *sh_d;  // shadow direction.xyz, ignore (int bits)
+	float4 *sh_c;  // contribution.xyz, slot (int bits)
+	// counters: [0, kWfMaxDepth] ray-queue lengths per bounce, [kWfMaxDepth+1 ...] shadow
+	// lengths per bounce, then per-bounce fetch counters of extend and shadow.
+	unsigned *counters;
+	int capacity;
+};
+
+constexpr int kCntRays = 0;
+constexpr int kCntShadow = kWfMaxDepth + 1;
+constexpr int kCntFetchExt = 2 * (kWfMaxDepth + 1);
+constexpr int kCntFetchSh = 3 * (kWfMaxDepth + 1);
+constexpr int kCntTotal = 4 * (kWfMaxDepth + 1);
+
+// One wave's generation table. A wave holds `spw` consecutive samples of every
+// pixel of each active job, laid out sample-major per job:
+//   slot = bases[a] + k * n_pix + pixel,  k < nsamp[a]
+// and is accumulated per pixel over k in sample order.
+struct WfWave {
+	const int *jobs;    // active job ids
+	const int *bases;   // first slot of each active job
+	const int *pbases;  // first accumulate index of each active job
+	const int *nsamp;   // samples of each active job in this wave
+	int n_jobs;
+	int n_slots;        // paths in the wave
+	int n_pix;          // pixels in the wave (sum of active jobs' pixels)
+	int first_sample;   // sample index of k = 0, relative to each job's sample_offset
+};
+
+cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave &wave, int max_depth, int order,
+                           int grid_ext, int grid_shade, int grid_sh, int *status, cudaStream_t st);
+
+} // namespace rnb

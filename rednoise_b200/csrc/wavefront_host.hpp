@@ -1,0 +1,71 @@
+// Host side of the wavefront integrator: pools, job tables, wave schedule and
+// the CUDA graph that replays a whole frame.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "wavefront.cuh"
+
+namespace rnb {
+
+void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh);
+
+// Samples per wave that keep about 2^20 paths in flight (at least 1, at most spp).
+inline int default_samples_per_wave(long n_pix, int spp) {
+	long k = n_pix > 0 ? (1L << 20) / n_pix : 1;
+	if (k < 1)
+		k = 1;
+	if (k > spp)
+		k = spp;
+	return static_cast<int>(k < 1 ? 1 : k);
+}
+
+class WfContext {
+public:
+	~WfContext();
+	// Set up pools, job table and the wave schedule for these jobs (host copies
+	// of the job descriptors; their accum pointers are device pointers). Each wave
+	// holds `spw` samples of every pixel of every active job.
+	rn_status configure(const std::vector<WfJob> &jobs, int max_depth, int order, int spw, cudaStream_t st);
+	// Optional frame prologue / epilogue captured with the waves: zero the
+	// accumulators first, then write means = sums * inv_spp per segment.
+	struct Resolve {
+		const float *accum;
+		float *mean;
+		long n_floats;
+		float inv_spp;
+	};
+	void set_frame_io(float *zero_ptr, size_t zero_bytes, const std::vector<Resolve> &resolves);
+	// Enqueue every wave of the frame on st (direct launches).
+	rn_status enqueue(int *status, cudaStream_t st);
+	// Capture the frame into a CUDA graph on first use, then launch it.
+	rn_status launch_graph(int *status, cudaStream_t st);
+	int capacity() const { return capacity_; }
+
+private:
+	rn_status ensure_pool(int capacity);
+	void release_graph();
+
+	DevBuf o_, d_, beta_, L_, pixel_, sample_, hit_idx_, hit_t_, q0_, q1_, sh_o_, sh_d_, sh_c_, counters_;
+	DevBuf d_jobs_, d_wave_tab_;
+	WfPool pool_{};
+	int capacity_ = 0;
+	int max_depth_ = 0;
+	int order_ = 0;
+	int grid_ext_ = 0, grid_shade_ = 0, grid_sh_ = 0;
+	std::vector<WfWave> waves_;
+	std::vector<WfJob> host_jobs_; // staging copies kept alive for the asynchronous uploads
+	std::vector<int> host_tab_;
+	std::vector<long> key_;
+	float *zero_ptr_ = nullptr;
+	size_t zero_bytes_ = 0;
+	std::vector<Resolve> resolves_;
+	cudaGraph_t graph_ = nullptr;
+	cudaGraphExec_t exec_ = nullptr;
+	int *graph_status_ = nullptr;
+};
+
+} // namespace rnb

@@ -87,7 +87,7 @@ def _box(center, size, angle_deg):
     return tris
 
 
-def _room():
+def _room(light_scale: float = 1.0):
     h = HALF
     walls, albedo = [], []
     grey = (0.725, 0.725, 0.725)
@@ -104,7 +104,7 @@ def _room():
         (-0.95, -h + 1.65, -0.9), (1.65, 3.30, 1.65), 18.0
     )
     albedo += [grey] * len(boxes)
-    lw, ld = 0.13 / 2.0, 0.105 / 2.0
+    lw, ld = 0.13 / 2.0 * light_scale, 0.105 / 2.0 * light_scale
     y = h - 1e-3
     light = _quad((-lw, y, -ld), (lw, y, -ld), (lw, y, ld), (-lw, y, ld))  # normal -y (faces down)
     tris = walls + boxes + light
@@ -142,9 +142,11 @@ def _finish(v, albedo, emission, material, param) -> Dict:
     }
 
 
-def cornell_box() -> Dict:
-    """The 36-triangle Cornell box (all Lambertian, one emitter quad)."""
-    v, alb, em = _room()
+def cornell_box(light_scale: float = 1.0) -> Dict:
+    """The 36-triangle Cornell box (all Lambertian, one emitter quad).
+    ``light_scale`` scales the light quad's sides (1 = the 0.13 x 0.105 m quad;
+    statistical tests use 10 for a low-variance image)."""
+    v, alb, em = _room(light_scale)
     n = v.shape[0]
     return _finish(v, alb, em, np.zeros(n, np.int32), np.full(n, 0.2, np.float32))
 

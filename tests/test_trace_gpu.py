@@ -39,45 +39,49 @@ def ulp_distance(a, b):
 def nearest_consistent(idx, t, ref_idx, ref_t, max_frac=0.01):
     """Nearest-first traversal returns the (t, rank)-minimal hit. It departs from
     the reference only where the reference's float slab test pruned a leaf whose
-    triangle lies a few ULP nearer (coplanar or edge-sharing triangles): there
-    the hit must be no farther than the reference's and within 4 ULP of it."""
+    triangle lies a hair nearer (coplanar triangles, rays through a shared edge or
+    vertex, where the two triangles' t differ by their rounding): there the hit
+    must be no farther than the reference's and within 64 ULP of it."""
     bad = np.nonzero(idx != ref_idx)[0]
     assert bad.size <= max_frac * idx.size, bad.size
     assert (ref_idx[bad] >= 0).all() and (idx[bad] >= 0).all()
     assert (t[bad] <= ref_t[bad]).all()
-    assert (ulp_distance(t[bad], ref_t[bad]) <= 4).all()
+    assert (ulp_distance(t[bad], ref_t[bad]) <= 64).all()
     same = idx == ref_idx
     assert np.array_equal(t[same].view(np.uint32), ref_t[same].view(np.uint32))
     return bad.size
 
 
 @pytest.mark.parametrize("name", ["cornell", "sphere", "box"])
-@pytest.mark.parametrize("nearest", [False, True])
-def test_closest_hit_matches_reference_golden(gold, name, nearest):
+@pytest.mark.parametrize("mode", ["width4", "width2", "nearest"])
+def test_closest_hit_matches_reference_golden(gold, name, mode):
     trace, assets = gold
     s = rn.Scene.from_arrays(_v9(name, assets))
     o, d = trace[f"{name}_o"], trace[f"{name}_d"]
-    idx, t, u, v = s.trace_closest(o, d, nearest_first=nearest)
-    if nearest:
+    kw = {"nearest_first": mode == "nearest", "width2": mode == "width2"}
+    idx, t, u, v = s.trace_closest(o, d, **kw)
+    if mode == "nearest":
         nearest_consistent(idx, t, trace[f"{name}_idx"], trace[f"{name}_t"].view(np.float32))
         return
-    # Reference order: bit-exact by construction.
+    # Reference order, 2-wide or 4-wide layout: bit-exact.
     assert np.array_equal(idx, trace[f"{name}_idx"]), np.nonzero(idx != trace[f"{name}_idx"])[0][:10]
     assert np.array_equal(t.view(np.uint32), trace[f"{name}_t"])
     assert np.array_equal(u.view(np.uint32), trace[f"{name}_u"])
     assert np.array_equal(v.view(np.uint32), trace[f"{name}_v"])
     if name != "box":
         ig = trace[f"{name}_ignore"]
-        idx_i, t_i, _, _ = s.trace_closest(o, d, ignore=ig, nearest_first=nearest)
+        idx_i, t_i, _, _ = s.trace_closest(o, d, ignore=ig, **kw)
         assert np.array_equal(idx_i, trace[f"{name}_idx_ig"])
         assert np.array_equal(t_i.view(np.uint32), trace[f"{name}_t_ig"])
 
 
 @pytest.mark.parametrize("name", ["cornell", "sphere", "box"])
-def test_any_hit_matches_reference_golden(gold, name):
+@pytest.mark.parametrize("width2", [False, True])
+def test_any_hit_matches_reference_golden(gold, name, width2):
     trace, assets = gold
     s = rn.Scene.from_arrays(_v9(name, assets))
-    occ = s.trace_any(trace[f"{name}_o"], trace[f"{name}_d"], trace[f"{name}_tmax"], trace[f"{name}_ignore"])
+    occ = s.trace_any(trace[f"{name}_o"], trace[f"{name}_d"], trace[f"{name}_tmax"], trace[f"{name}_ignore"],
+                      width2=width2)
     assert np.array_equal(occ, trace[f"{name}_occ"])
 
 
@@ -115,15 +119,18 @@ def test_large_soup_matches_oracle(count, seed):
     orc = oracle.OrcBvh(v9)
     ri, rt, ru, rv = orc.intersect(o, d)
     s = rn.Scene.from_arrays(v9)
-    gi, gt, gu, gv = s.trace_closest(o, d)
-    bad = np.nonzero(gi != ri)[0]
-    assert bad.size == 0, bad[:10]
-    assert np.array_equal(gt.view(np.uint32), rt.view(np.uint32))
-    assert np.array_equal(gu.view(np.uint32), ru.view(np.uint32))
+    for width2 in (False, True):
+        gi, gt, gu, gv = s.trace_closest(o, d, width2=width2)
+        bad = np.nonzero(gi != ri)[0]
+        assert bad.size == 0, (width2, bad[:10])
+        assert np.array_equal(gt.view(np.uint32), rt.view(np.uint32))
+        assert np.array_equal(gu.view(np.uint32), ru.view(np.uint32))
     gi, gt, _, _ = s.trace_closest(o, d, nearest_first=True)
     nearest_consistent(gi, gt, ri, rt)
     tmax = np.random.default_rng(seed).random(o.shape[0]).astype(np.float32) * 5
-    assert np.array_equal(s.trace_any(o, d, tmax), orc.occluded(o, d, tmax))
+    want = orc.occluded(o, d, tmax)
+    assert np.array_equal(s.trace_any(o, d, tmax), want)
+    assert np.array_equal(s.trace_any(o, d, tmax, width2=True), want)
 
 
 def test_device_pointer_path_with_torch():
