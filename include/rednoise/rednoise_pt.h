@@ -189,6 +189,25 @@ rn_status rn_pt_render(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_
 rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
                                   unsigned flags, void *stream, float *accum);
 
+/* ---- differentiable rendering ---- */
+
+/* Overwrite per-triangle albedo (3 floats per triangle) and / or emitted
+ * radiance (3 floats per triangle; only triangles that were emitters when the
+ * scene was prepared keep emitting). Either pointer may be NULL. */
+rn_status rn_pt_scene_set_materials(rn_scene *scene, const float *albedo, const float *emission, unsigned flags,
+                                    void *stream);
+
+/* Path-replay adjoint of rn_pt_render over n_views camera views of one scene:
+ * given d_images[v] = dL/d(mean image of view v) (width*height*3 floats), write
+ * d_albedo = dL/d(albedo) and d_emission = dL/d(emitted radiance), 3 floats per
+ * triangle each (overwritten; either may be NULL). Each view's settings give its
+ * adjoint samples (spp, seed, sample_offset, depth, roulette). Every path is
+ * regenerated from its RNG key and traced twice, so memory stays O(pixels).
+ * Roulette probabilities are treated as constants. */
+rn_status rn_pt_backward(rn_scene *scene, int n_views, const rn_pt_camera *cameras, const rn_pt_settings *settings,
+                         const float *const *d_images, unsigned flags, void *stream, float *d_albedo,
+                         float *d_emission);
+
 /* ---- batched rendering: many scenes / cameras / resolutions in one launch ---- */
 
 typedef struct rn_pt_batch rn_pt_batch;

@@ -87,6 +87,8 @@ def orc() -> ctypes.CDLL:
             "orc_pt_render": (None, [vp, vp, ci, ci, ci, ci, ci, ctypes.c_ulonglong, ctypes.c_uint, vp, ci, vp, ci,
                                      vp]),
             "orc_pt_count": (None, [vp, vp, ci, ci, ci, ci, ci, ctypes.c_ulonglong, ctypes.c_uint, vp, ci, vp, vp]),
+            "orc_pt_backward": (None, [vp, vp, ci, ci, ci, ci, ci, ctypes.c_ulonglong, ctypes.c_uint, vp, vp, ci,
+                                       vp, vp]),
         }
         for k, (r, a) in sig.items():
             getattr(lib, k).restype = r
@@ -295,6 +297,19 @@ class OrcPhysScene:
         orc().orc_pt_render(self.h, P(c10), w, h, spp, max_depth, rr_depth, seed, offset, P(envv),
                             0 if px is None else px.size, P(px), 1 if double else 0, P(out))
         return out
+
+    def backward(self, cam: dict, spp: int, max_depth: int, rr_depth: int, seed: int, d_image, offset: int = 0,
+                 env=(0.0, 0.0, 0.0), double: bool = True):
+        """Path-replay gradient: (dL/d albedo, dL/d emission), float64 (n, 3) each."""
+        c10 = np.array(list(cam["position"]) + list(cam["target"]) + list(cam["up"]) + [cam["vfov_deg"]], np.float32)
+        envv = np.asarray(env, np.float32)
+        g = np.ascontiguousarray(d_image, np.float32).reshape(-1)
+        n = self._keep[0].shape[0]
+        ga = np.zeros((n, 3), np.float64)
+        ge = np.zeros((n, 3), np.float64)
+        orc().orc_pt_backward(self.h, P(c10), cam["width"], cam["height"], spp, max_depth, rr_depth, seed, offset,
+                              P(envv), P(g), 1 if double else 0, P(ga), P(ge))
+        return ga, ge
 
     def count_queries(self, cam: dict, spp: int, max_depth: int, rr_depth: int, seed: int, offset: int = 0,
                       env=(0.0, 0.0, 0.0), pixels=None) -> dict:

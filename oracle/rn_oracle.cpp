@@ -675,7 +675,12 @@ template <typename T> X3<T> schlick_t(X3<T> f0, T c) {
 	T m5 = (m * m) * (m * m) * m;
 	return f0 + (x3<T>(1, 1, 1) - f0) * m5;
 }
-template <typename T> bool eval_t(int mat, X3<T> alb, T alpha, X3<T> n, X3<T> wo, X3<T> wi, X3<T> &fc, T &pdf) {
+template <typename T> T m5_t(T c) {
+	T m = std::min(std::max(1 - c, T(0)), T(1));
+	return (m * m) * (m * m) * m;
+}
+template <typename T>
+bool eval_t(int mat, X3<T> alb, T alpha, X3<T> n, X3<T> wo, X3<T> wi, X3<T> &fc, T &pdf, T *m5 = nullptr) {
 	T ci = dt(n, wi), co = dt(n, wo);
 	if (ci <= 0 || co <= 0)
 		return false;
@@ -694,12 +699,46 @@ template <typename T> bool eval_t(int mat, X3<T> alb, T alpha, X3<T> n, X3<T> wo
 	T G2 = 1 / (1 + lo + li), G1 = 1 / (1 + lo);
 	fc = schlick_t(alb, om) * (D * G2 / (4 * co));
 	pdf = G1 * D / (4 * co);
+	if (m5)
+		*m5 = m5_t(om);
 	return true;
 }
 template <typename T> T mis_t(T a, T b) { return a * a / (a * a + b * b); }
 
-template <typename T> X3<T> trace_phys(const PhysScene &s, const PhysCam &c, const PhysSet &st, uint32_t pix,
-                                       uint32_t sample) {
+// d log(weight) / d albedo of a Lambert (1 / albedo) or GGX-Schlick ((1 - m5) / F) vertex.
+template <typename T> X3<T> dlog_t(int mat, X3<T> alb, T m5) {
+	if (mat == 0)
+		return x3<T>(1 / std::max(alb.x, T(1e-12)), 1 / std::max(alb.y, T(1e-12)), 1 / std::max(alb.z, T(1e-12)));
+	if (mat == 1) {
+		X3<T> F = alb + (x3<T>(1, 1, 1) - alb) * m5;
+		T d = 1 - m5;
+		return x3<T>(d / std::max(F.x, T(1e-12)), d / std::max(F.y, T(1e-12)), d / std::max(F.z, T(1e-12)));
+	}
+	return x3<T>(0, 0, 0);
+}
+
+// Gradient sink of the replay pass (path replay backpropagation): g = dL/dI / spp,
+// C = the path's radiance from the first pass, P = radiance gathered so far.
+template <typename T> struct GradSink {
+	X3<T> g, C, P;
+	double *galb, *gem;
+	void add(double *buf, int tri, X3<T> v) {
+		double *p = buf + 3 * static_cast<size_t>(tri);
+#pragma omp atomic
+		p[0] += static_cast<double>(v.x);
+#pragma omp atomic
+		p[1] += static_cast<double>(v.y);
+#pragma omp atomic
+		p[2] += static_cast<double>(v.z);
+	}
+};
+template <typename T> X3<T> sdiv(X3<T> a, X3<T> b) {
+	return x3<T>(b.x > 0 ? a.x / b.x : T(0), b.y > 0 ? a.y / b.y : T(0), b.z > 0 ? a.z / b.z : T(0));
+}
+
+template <typename T>
+X3<T> trace_phys(const PhysScene &s, const PhysCam &c, const PhysSet &st, uint32_t pix, uint32_t sample,
+                 GradSink<T> *gs = nullptr) {
 	const T two_pi = T(6.28318530717958647692);
 	orc::U4 r0 = prand(st.seed, pix, sample, 0);
 	int px = static_cast<int>(pix % static_cast<uint32_t>(c.w)), py = static_cast<int>(pix / static_cast<uint32_t>(c.w));
@@ -730,7 +769,12 @@ template <typename T> X3<T> trace_phys(const PhysScene &s, const PhysCam &c, con
 				T w = 1;
 				if (prev_pdf > 0)
 					w = mis_t(prev_pdf, h.t * h.t / (cog * T(s.area_total)));
-				L = L + beta * Le * w;
+				X3<T> e = beta * Le * w;
+				L = L + e;
+				if (gs) {
+					gs->P = gs->P + e;
+					gs->add(gs->gem, h.idx, gs->g * sdiv(e, Le));
+				}
 			}
 			break;
 		}
@@ -763,17 +807,25 @@ template <typename T> X3<T> trace_phys(const PhysScene &s, const PhysCam &c, con
 			T cos_l = -dt(ne, wi);
 			X3<T> fc;
 			T pb;
-			if (cos_l > 0 && dist > 0 && eval_t<T>(mat, alb, param, n, wo, wi, fc, pb)) {
+			T m5l = 0;
+			if (cos_l > 0 && dist > 0 && eval_t<T>(mat, alb, param, n, wo, wi, fc, pb, &m5l)) {
 				T pl = dist2 / (cos_l * T(s.area_total));
 				X3<T> eLe = x3<T>(s.emission[3 * ek], s.emission[3 * ek + 1], s.emission[3 * ek + 2]);
 				T w = mis_t(pl, pb);
-				if (!occluded_t<T>(s, p + n * eps, wi, dist, E.tri))
-					L = L + beta * fc * eLe * (w / pl);
+				if (!occluded_t<T>(s, p + n * eps, wi, dist, E.tri)) {
+					X3<T> nee = beta * fc * eLe * (w / pl);
+					L = L + nee;
+					if (gs) {
+						gs->P = gs->P + nee;
+						gs->add(gs->galb, h.idx, gs->g * nee * dlog_t(mat, alb, m5l));
+						gs->add(gs->gem, E.tri, gs->g * sdiv(nee, eLe));
+					}
+				}
 			}
 		}
 		if (bounce + 1 >= st.max_depth)
 			break;
-		X3<T> wi, weight;
+		X3<T> wi, weight, cont_dlog = x3<T>(0, 0, 0);
 		T pdf = 0;
 		if (mat == 0) {
 			T r = std::sqrt(T(orc::u01(rB.x)));
@@ -787,6 +839,7 @@ template <typename T> X3<T> trace_phys(const PhysScene &s, const PhysCam &c, con
 				break;
 			weight = alb;
 			pdf = ci * T(0.318309886183790671537767526745);
+			cont_dlog = dlog_t(0, alb, T(0));
 		} else if (mat == 1) {
 			T alpha = param, a2 = alpha * alpha;
 			X3<T> t, bt;
@@ -813,6 +866,7 @@ template <typename T> X3<T> trace_phys(const PhysScene &s, const PhysCam &c, con
 			T G1 = 1 / (1 + lo_), G2 = 1 / (1 + lo_ + li_);
 			weight = schlick_t(alb, om) * (G2 / G1);
 			pdf = G1 * ggx_D_t(ml.z, a2) / (4 * co);
+			cont_dlog = dlog_t(1, alb, m5_t(om));
 		} else {
 			T eta = param;
 			bool entering = cog > 0;
@@ -839,6 +893,8 @@ template <typename T> X3<T> trace_phys(const PhysScene &s, const PhysCam &c, con
 				break;
 			beta = beta * (T(1) / q);
 		}
+		if (gs)
+			gs->add(gs->galb, h.idx, gs->g * (gs->C - gs->P) * cont_dlog);
 		T side = dt(wi, ng) >= 0 ? T(1) : T(-1);
 		o = p + ng * (side * eps);
 		d = wi;
@@ -1144,6 +1200,45 @@ void orc_pt_count(const void *h, const float *cam10, int w, int hgt, int spp, in
 	}
 	for (int k = 0; k < 6; k++)
 		out[k] = tot[k];
+}
+
+// Path-replay gradient of the estimator: dimg = dL/d(mean image) (w*h*3 floats),
+// galb / gem receive dL/d albedo and dL/d emission (n*3 doubles, overwritten).
+// Each sample is traced once for its radiance and once more to scatter derivatives.
+void orc_pt_backward(const void *h, const float *cam10, int w, int hgt, int spp, int max_depth, int rr_depth,
+                     unsigned long long seed, unsigned offset, const float *env3, const float *dimg, int precision,
+                     double *galb, double *gem) {
+	const PhysScene &s = *static_cast<const PhysScene *>(h);
+	const PhysCam c = make_cam(cam10, w, hgt);
+	PhysSet st{spp, max_depth, rr_depth, seed, offset, {env3[0], env3[1], env3[2]}};
+	const size_t n = s.bvh.tris.size();
+	std::fill(galb, galb + 3 * n, 0.0);
+	std::fill(gem, gem + 3 * n, 0.0);
+	const int count = w * hgt;
+#pragma omp parallel for schedule(dynamic, 16)
+	for (int i = 0; i < count; i++) {
+		const double inv = spp > 0 ? 1.0 / spp : 0.0;
+		for (int k = 0; k < spp; k++) {
+			const uint32_t smp = offset + static_cast<uint32_t>(k);
+			if (precision == 0) {
+				GradSink<float> gs;
+				gs.g = x3<float>(float(dimg[3 * i] * inv), float(dimg[3 * i + 1] * inv), float(dimg[3 * i + 2] * inv));
+				gs.C = trace_phys<float>(s, c, st, static_cast<uint32_t>(i), smp);
+				gs.P = x3<float>(0, 0, 0);
+				gs.galb = galb;
+				gs.gem = gem;
+				(void)trace_phys<float>(s, c, st, static_cast<uint32_t>(i), smp, &gs);
+			} else {
+				GradSink<double> gs;
+				gs.g = x3<double>(dimg[3 * i] * inv, dimg[3 * i + 1] * inv, dimg[3 * i + 2] * inv);
+				gs.C = trace_phys<double>(s, c, st, static_cast<uint32_t>(i), smp);
+				gs.P = x3<double>(0, 0, 0);
+				gs.galb = galb;
+				gs.gem = gem;
+				(void)trace_phys<double>(s, c, st, static_cast<uint32_t>(i), smp, &gs);
+			}
+		}
+	}
 }
 
 // cam: pos3, target3, up3, vfov_deg (10 floats), w, h; settings: spp, max_depth, rr_depth, seed, offset, env3.

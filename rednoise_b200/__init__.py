@@ -355,6 +355,37 @@ class Scene:
                       "rn_pt_render_accumulate")
         return accum
 
+    def set_materials(self, albedo=None, emission=None) -> None:
+        """Overwrite per-triangle albedo and / or emitted radiance (host arrays, n x 3)."""
+        self._check_open()
+        a = None if albedo is None else _f32(albedo).reshape(-1)
+        e = None if emission is None else _f32(emission).reshape(-1)
+        n3 = 3 * self.triangle_count
+        for x in (a, e):
+            if x is not None and x.size != n3:
+                raise ValueError(f"expected {n3} values")
+        _native.check(_native.load().rn_pt_scene_set_materials(self._handle, _ptr(a), _ptr(e), 0, None),
+                      "rn_pt_scene_set_materials")
+
+    def backward(self, views, d_images):
+        """Path-replay adjoint over views [(camera, settings)] given dL/d(mean image) per
+        view (host arrays, h x w x 3). Returns (d_albedo, d_emission), each n x 3 float32."""
+        self._check_open()
+        nv = len(views)
+        cams = (_native.Camera * nv)(*[v[0] for v in views])
+        sets = (_native.Settings * nv)(*[v[1] for v in views])
+        imgs = [_f32(g).reshape(-1) for g in d_images]
+        for (c, _), g in zip(views, imgs):
+            if g.size != c.width * c.height * 3:
+                raise ValueError("image gradient size does not match its camera")
+        ptrs = (ctypes.c_void_p * nv)(*[g.ctypes.data for g in imgs])
+        n = self.triangle_count
+        ga = np.zeros((n, 3), np.float32)
+        ge = np.zeros((n, 3), np.float32)
+        _native.check(_native.load().rn_pt_backward(self._handle, nv, cams, sets, ptrs, 0, None, _ptr(ga), _ptr(ge)),
+                      "rn_pt_backward")
+        return ga, ge
+
     def count_traversal(self, camera: "Camera", settings: "Settings") -> dict:
         """Reference-traversal test counts over one render's rays (profiling counters)."""
         self._check_open()

@@ -213,6 +213,9 @@ SIGNATURES = {
     "rn_pt_render_accumulate": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                                vp, vp]),
     "rn_pt_count_traversal": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), vp]),
+    "rn_pt_scene_set_materials": (ctypes.c_int, [vp, vp, vp, ctypes.c_uint, vp]),
+    "rn_pt_backward": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(Camera), ctypes.POINTER(Settings),
+                                      ctypes.POINTER(vp), ctypes.c_uint, vp, vp, vp]),
     "rn_pt_batch_create": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.c_int, ctypes.c_int, ctypes.c_uint,
                                           ctypes.POINTER(vp)]),
     "rn_pt_batch_render": (ctypes.c_int, [vp, ctypes.c_uint, ctypes.c_uint, vp, ctypes.POINTER(vp)]),

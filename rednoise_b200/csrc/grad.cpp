@@ -1,0 +1,125 @@
+// Differentiable-rendering entry points: material updates and the adjoint.
+#include <cstring>
+#include <vector>
+
+#include "adjoint.hpp"
+#include "render_impl.hpp"
+#include "scene_impl.hpp"
+
+using namespace rnb;
+
+extern "C" {
+
+rn_status rn_pt_scene_set_materials(rn_scene *scene, const float *albedo, const float *emission, unsigned flags,
+                                    void *stream) {
+	if (!scene) {
+		set_last_error("rn_pt_scene_set_materials: NULL scene");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	rn_status r = prepare_scene(scene);
+	if (r != RN_OK)
+		return r;
+	const int n = static_cast<int>(scene->tris.size());
+	cudaStream_t cs = pick_stream(scene, stream);
+	if (flags & RN_PT_DEVICE_POINTERS)
+		return launch_set_materials(scene->d_phys_shade.as<float4>(), n, albedo, emission, cs) == cudaSuccess
+		           ? RN_OK
+		           : cuda_fail(cudaGetLastError(), "launch_set_materials");
+	// Host arrays: keep the host copies in step and stage the upload.
+	const size_t bytes = static_cast<size_t>(n) * 3 * sizeof(float);
+	std::lock_guard<std::mutex> lock(scene->scratch_mu);
+	RNB_CUDA(scene->scratch.ensure(2 * bytes + 256));
+	float *d_a = albedo ? scene->scratch.as<float>() : nullptr;
+	float *d_e = emission ? scene->scratch.as<float>() + 3 * static_cast<size_t>(n) + 64 : nullptr;
+	if (albedo) {
+		std::memcpy(scene->tris.albedo.data(), albedo, bytes);
+		RNB_CUDA(cudaMemcpyAsync(d_a, albedo, bytes, cudaMemcpyHostToDevice, cs));
+	}
+	if (emission) {
+		RNB_CUDA(cudaMemcpyAsync(d_e, emission, bytes, cudaMemcpyHostToDevice, cs));
+	}
+	RNB_CUDA(launch_set_materials(scene->d_phys_shade.as<float4>(), n, d_a, d_e, cs));
+	RNB_CUDA(cudaStreamSynchronize(cs));
+	return RN_OK;
+}
+
+rn_status rn_pt_backward(rn_scene *scene, int n_views, const rn_pt_camera *cameras, const rn_pt_settings *settings,
+                         const float *const *d_images, unsigned flags, void *stream, float *d_albedo,
+                         float *d_emission) {
+	if (!scene || n_views <= 0 || !cameras || !settings || !d_images) {
+		set_last_error("rn_pt_backward: invalid argument");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	std::vector<AdjView> views(static_cast<size_t>(n_views));
+	PhysScene ps{};
+	long total = 0;
+	for (int v = 0; v < n_views; v++) {
+		PhysCamera pc;
+		PhysSettings pst;
+		rn_status r = make_phys_inputs(scene, &cameras[v], &settings[v], 0, ps, pc, pst);
+		if (r != RN_OK)
+			return r;
+		if (!d_images[v]) {
+			set_last_error("rn_pt_backward: NULL image gradient");
+			return RN_ERR_INVALID_ARGUMENT;
+		}
+		views[v].cam = pc;
+		views[v].st = pst;
+		views[v].n_pix = pc.width * pc.height;
+		views[v].pix_base = static_cast<int>(total);
+		total += views[v].n_pix;
+	}
+	if (total > (1L << 30)) {
+		set_last_error("rn_pt_backward: more than 2^30 pixels");
+		return RN_ERR_CAPACITY;
+	}
+	const int n = static_cast<int>(scene->tris.size());
+	const bool dev = (flags & RN_PT_DEVICE_POINTERS) != 0;
+	cudaStream_t cs = pick_stream(scene, stream);
+	const size_t gbytes = static_cast<size_t>(n) * 3 * sizeof(float);
+	std::unique_lock<std::mutex> lock(scene->scratch_mu);
+	// Scratch: view table, gradient buffers, and (host mode) the image gradients.
+	const size_t vbytes = (views.size() * sizeof(AdjView) + 255) & ~size_t(255);
+	const size_t gb = (gbytes + 255) & ~size_t(255);
+	const size_t ib = dev ? 0 : static_cast<size_t>(total) * 3 * sizeof(float);
+	// Device mode returns without a host synchronisation, so its view table lives in
+	// a buffer of its own (calls on one scene are ordered on the caller's stream).
+	DevBuf &buf = dev ? scene->adj : scene->scratch;
+	RNB_CUDA(buf.ensure(vbytes + 2 * gb + ib + 256));
+	char *base = buf.as<char>();
+	AdjView *d_views = reinterpret_cast<AdjView *>(base);
+	float *g_alb = (dev && d_albedo) ? d_albedo : reinterpret_cast<float *>(base + vbytes);
+	float *g_em = (dev && d_emission) ? d_emission : reinterpret_cast<float *>(base + vbytes + gb);
+	float *imgs = reinterpret_cast<float *>(base + vbytes + 2 * gb);
+	for (int v = 0; v < n_views; v++) {
+		if (dev) {
+			views[v].dimg = d_images[v];
+		} else {
+			float *dst = imgs + 3 * static_cast<size_t>(views[v].pix_base);
+			RNB_CUDA(cudaMemcpyAsync(dst, d_images[v], static_cast<size_t>(views[v].n_pix) * 12,
+			                         cudaMemcpyHostToDevice, cs));
+			views[v].dimg = dst;
+		}
+	}
+	RNB_CUDA(cudaMemcpyAsync(d_views, views.data(), views.size() * sizeof(AdjView), cudaMemcpyHostToDevice, cs));
+	RNB_CUDA(cudaMemsetAsync(g_alb, 0, gbytes, cs));
+	RNB_CUDA(cudaMemsetAsync(g_em, 0, gbytes, cs));
+	RNB_CUDA(launch_adjoint(ps, d_views, n_views, static_cast<int>(total), g_alb, g_em, n, scene->d_status.as<int>(),
+	                        cs));
+	if (dev)
+		return RN_OK;
+	if (d_albedo)
+		RNB_CUDA(cudaMemcpyAsync(d_albedo, g_alb, gbytes, cudaMemcpyDeviceToHost, cs));
+	if (d_emission)
+		RNB_CUDA(cudaMemcpyAsync(d_emission, g_em, gbytes, cudaMemcpyDeviceToHost, cs));
+	int h = 0;
+	RNB_CUDA(cudaMemcpyAsync(&h, scene->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, cs));
+	RNB_CUDA(cudaStreamSynchronize(cs));
+	if (h) {
+		set_last_error("rn_pt_backward: device status word reports a traversal error");
+		return RN_ERR_INTERNAL;
+	}
+	return RN_OK;
+}
+
+} // extern "C"

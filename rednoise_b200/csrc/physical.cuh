@@ -26,7 +26,7 @@ namespace rnb {
 
 struct PhysScene {
 	SceneView sv;
-	const float4 *__restrict__ shade;    // 3 per triangle: (albedo, material), (Le, param), (normal, 0)
+	const float4 *__restrict__ shade;    // 3 per triangle: (albedo, material), (Le, param), (normal, emitter flag)
 	const float4 *__restrict__ emitters; // 3 per emitter: (v0, tri), (e0, area), (e1, cdf)
 	int n_emitters;
 	float emit_area_total;
@@ -231,7 +231,7 @@ __device__ __forceinline__ bool shade_vertex_t(const PhysScene &sc, const PhysSe
 	const F3 wo = -ps.d;
 	const float cos_o_g = dot3(ng, wo);
 	const F3 Le = ld3(s1);
-	if (Le.x > 0.0f || Le.y > 0.0f || Le.z > 0.0f) {
+	if (s2.w != 0.0f) { // emitter flag, fixed when the scene was prepared
 		if (cos_o_g > 0.0f) {
 			float w = 1.0f;
 			if (ps.prev_pdf > 0.0f) {

@@ -81,6 +81,7 @@ rn_status prepare_scene(rn_scene *s) {
 		phys[3 * k + 1] = {ts.emission[3 * k], ts.emission[3 * k + 1], ts.emission[3 * k + 2], ts.phys_param[k]};
 		phys[3 * k + 2] = {ng.x, ng.y, ng.z, 0.0f};
 	}
+	// The emitter flag marks the triangles that are in the light-sampling table.
 	// Emitters (triangles with any Le > 0): (v0, tri), (e0, area), (e1, cumulative area).
 	std::vector<F4> em;
 	double acc = 0.0;
@@ -92,6 +93,7 @@ rn_status prepare_scene(rn_scene *s) {
 			if (!(area > 0.0))
 				continue; // a degenerate emitter can neither be hit nor sampled
 			acc += area;
+			phys[3 * k + 2].w = 1.0f;
 			em.push_back({t[0], t[1], t[2], as_float(i)});
 			em.push_back({t[3] - t[0], t[4] - t[1], t[5] - t[2], static_cast<float>(area)});
 			em.push_back({t[6] - t[0], t[7] - t[1], t[8] - t[2], static_cast<float>(acc)});

@@ -39,6 +39,7 @@ struct rn_scene {
 	// device-pointer renders (calls on one scene are serialised on its stream).
 	rnb::DevBuf d_counter;
 	rnb::DevBuf accum;
+	rnb::DevBuf adj; // view table and gradient buffers of device-pointer adjoint calls
 	// Wavefront pools and the captured frame graph of single-scene renders.
 	std::unique_ptr<rnb::WfContext> wf;
 

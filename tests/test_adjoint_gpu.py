@@ -1,0 +1,150 @@
+"""GPU checks of the path-replay adjoint (rn_pt_backward, torch.autograd).
+
+* central finite differences with common random numbers (eps 1e-3) on seeded
+  parameters: the adjoint differentiates the same fixed-sample estimator the
+  FD evaluates, bar: 2 % relative error (Russian roulette off, as the decisions
+  must not depend on the parameters);
+* the oracle's FP64 path-replay gradient on the same samples.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import rednoise_b200 as rn
+from rednoise_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+SPP, DEPTH = 16, 6
+
+
+def make_scene(sc):
+    return rn.Scene.from_arrays(sc["vertices"], albedo=sc["albedo"], emission=sc["emission"],
+                                material=sc["material"], material_param=sc["material_param"])
+
+
+def view(w, h, seed=3, spp=SPP, depth=DEPTH):
+    c = scenes.camera(w, h)
+    return (rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], w, h),
+            rn.Settings.make(spp=spp, max_depth=depth, rr_depth=depth, seed=seed, integrator=1))
+
+
+def loss_and_grad(s, sc, target, v):
+    img = s.render_physical(v[0], v[1]).astype(np.float64)
+    L = ((img - target) ** 2).sum()
+    return L, 2 * (img - target)
+
+
+@pytest.fixture(scope="module")
+def setup():
+    sc = scenes.cornell_box(light_scale=4.0)
+    rng = np.random.default_rng(0)
+    tgt = dict(sc)
+    tgt["albedo"] = np.clip(sc["albedo"] + rng.normal(0, 0.1, sc["albedo"].shape), 0.05, 0.95).astype(np.float32)
+    v = view(48, 36)
+    target = make_scene(tgt).render_physical(v[0], v[1]).astype(np.float64)
+    return sc, target, v
+
+
+def test_albedo_gradient_matches_central_differences(setup):
+    sc, target, v = setup
+    s = make_scene(sc)
+    L0, dI = loss_and_grad(s, sc, target, v)
+    ga, ge = s.backward([v], [dI.astype(np.float32)])
+    rng = np.random.default_rng(1)
+    eps = 1e-3
+    errs = []
+    for _ in range(24):
+        tri, ch = int(rng.integers(0, 34)), int(rng.integers(0, 3))
+        alb = sc["albedo"].copy()
+        alb[tri, ch] += eps
+        s.set_materials(albedo=alb)
+        Lp, _ = loss_and_grad(s, sc, target, v)
+        alb[tri, ch] -= 2 * eps
+        s.set_materials(albedo=alb)
+        Lm, _ = loss_and_grad(s, sc, target, v)
+        s.set_materials(albedo=sc["albedo"])
+        fd = (Lp - Lm) / (2 * eps)
+        if abs(fd) > 1e-7:
+            errs.append(abs(fd - ga[tri, ch]) / abs(fd))
+    assert len(errs) >= 8
+    assert np.median(errs) < 0.02 and max(errs) < 0.1, errs
+
+
+def test_emission_gradient_matches_central_differences(setup):
+    sc, target, v = setup
+    s = make_scene(sc)
+    _, dI = loss_and_grad(s, sc, target, v)
+    _, ge = s.backward([v], [dI.astype(np.float32)])
+    eps = 1e-2
+    for tri in (34, 35):
+        for ch in range(3):
+            em = sc["emission"].copy()
+            em[tri, ch] += eps
+            s.set_materials(emission=em)
+            Lp, _ = loss_and_grad(s, sc, target, v)
+            em[tri, ch] -= 2 * eps
+            s.set_materials(emission=em)
+            Lm, _ = loss_and_grad(s, sc, target, v)
+            s.set_materials(emission=sc["emission"])
+            fd = (Lp - Lm) / (2 * eps)
+            assert abs(fd - ge[tri, ch]) <= 0.02 * abs(fd) + 1e-9, (tri, ch, fd, ge[tri, ch])
+
+
+def test_gradient_matches_fp64_oracle(setup):
+    sc, target, v = setup
+    s = make_scene(sc)
+    _, dI = loss_and_grad(s, sc, target, v)
+    ga, ge = s.backward([v], [dI.astype(np.float32)])
+    c = scenes.camera(48, 36)
+    oa, oe = oracle.OrcPhysScene(sc).backward(c, SPP, DEPTH, DEPTH, 3, dI.astype(np.float32), double=True)
+    big = np.abs(oa) > 1e-3 * np.abs(oa).max()
+    rel = np.abs(ga[big] - oa[big]) / np.abs(oa[big])
+    assert np.median(rel) < 1e-3 and rel.max() < 0.05, rel.max()
+    assert np.allclose(ge[34:], oe[34:], rtol=5e-3, atol=1e-9 * np.abs(oe).max())
+
+
+def test_mixed_materials_gradient_matches_oracle():
+    """GGX (Schlick F0 = albedo) and dielectric vertices on the replayed paths."""
+    sc = scenes.icosphere_scene(level=2)
+    s = make_scene(sc)
+    v = view(40, 30, depth=6)
+    img = s.render_physical(v[0], v[1]).astype(np.float64)
+    dI = (2 * (img - 0.5 * img)).astype(np.float32)
+    ga, _ = s.backward([v], [dI])
+    c = scenes.camera(40, 30)
+    oa, _ = oracle.OrcPhysScene(sc).backward(c, SPP, 6, 6, 3, dI, double=True)
+    big = np.abs(oa) > 1e-3 * np.abs(oa).max()
+    rel = np.abs(ga[big] - oa[big]) / np.abs(oa[big])
+    assert np.median(rel) < 1e-3 and np.mean(rel < 0.02) > 0.97
+
+
+def test_torch_autograd_function(setup):
+    torch = pytest.importorskip("torch")
+    from rednoise_b200 import torch_ops
+
+    sc, target, v = setup
+    s = make_scene(sc)
+    alb = torch.tensor(sc["albedo"], device="cuda", requires_grad=True)
+    em = torch.tensor(sc["emission"], device="cuda", requires_grad=True)
+    tgt = torch.tensor(target, dtype=torch.float32, device="cuda")
+    (img,) = torch_ops.render(alb, em, s, [v])
+    loss = ((img - tgt) ** 2).sum()
+    loss.backward()
+    _, dI = loss_and_grad(s, sc, target, v)
+    ga, ge = s.backward([v], [dI.astype(np.float32)])
+    assert np.allclose(alb.grad.cpu().numpy(), ga, rtol=1e-3, atol=1e-9)
+    assert np.allclose(em.grad.cpu().numpy(), ge, rtol=1e-3, atol=1e-9)
+
+
+def test_multi_view_backward_sums_views(setup):
+    sc, target, v = setup
+    s = make_scene(sc)
+    v2 = view(32, 24, seed=9)
+    g1 = np.random.default_rng(2).normal(size=(36, 48, 3)).astype(np.float32)
+    g2 = np.random.default_rng(3).normal(size=(24, 32, 3)).astype(np.float32)
+    a1, e1 = s.backward([v], [g1])
+    a2, e2 = s.backward([v2], [g2])
+    a12, e12 = s.backward([v, v2], [g1, g2])
+    assert np.allclose(a12, a1 + a2, rtol=1e-4, atol=1e-7)
+    assert np.allclose(e12, e1 + e2, rtol=1e-4, atol=1e-7)
