@@ -246,6 +246,16 @@ def run_ours(args):
     bytes_per_sample = (24.0 * (counts["closest_boxes"] + counts["any_boxes"]) +
                         36.0 * (counts["closest_tris"] + counts["any_tris"])) / counts["samples"]
 
+    # The autotuner picks megakernel vs wavefront (and the wavefront queue capacity) for
+    # this frame; the timed RN_PT_AUTO renders below use its choice.
+    tuned = scene.autotune(cam, rn.Settings.make(spp=spp, max_depth=args.depth, rr_depth=args.rr, seed=1))
+    if integ == 1 or (integ == 0 and tuned["integrator"] == 1):
+        launches_per_step = 2  # megakernel + resolve
+    else:
+        spw = tuned["samples_per_wave"] if integ == 0 else max(1, min(spp, (1 << 20) // (W * H)))
+        waves = (spp + spw - 1) // spw
+        launches_per_step = waves * (2 + 3 * args.depth) + 1  # camera, 3 stages per bounce, accumulate; resolve
+
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             l2.zero_()
@@ -276,6 +286,31 @@ def run_ours(args):
     ms_per_step = total_ms / args.steps
     samples_per_step = W * H * spp
     value = world * samples_per_step / (ms_per_step / 1e3)
+
+    # The two integrators side by side on the same frame (same estimator, same samples):
+    # the plain megakernel and the wavefront (SoA queues, CUDA-graph frame).
+    compare = {}
+    with torch.cuda.stream(stream):
+        for name, code in (("megakernel", 1), ("wavefront", 2)):
+            def one():
+                st = settings()
+                st.integrator = code
+                render(st)
+            l2.zero_()
+            one()  # warm-up (captures the wavefront graph for this frame shape)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ts = []
+            for _ in range(2):
+                l2.zero_()
+                e0.record(stream)
+                one()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            compare[name] = samples_per_step / (min(ts) / 1e3)
+    compare["wavefront_over_megakernel"] = compare["wavefront"] / compare["megakernel"]
+    compare["auto_choice"] = {1: "megakernel", 2: "wavefront"}.get(tuned["integrator"], "?")
+    compare["auto_samples_per_wave"] = tuned["samples_per_wave"]
 
     # End to end through the C ABI with host buffers: pinned host output, D2H inside the timed region.
     host = torch.empty(H * W * 3, dtype=torch.float32, pin_memory=True)
@@ -321,7 +356,7 @@ def run_ours(args):
                    "rr_depth": args.rr, "triangles": info["num_triangles"], "integrator": args.integrator,
                    "traversal": "reference order and arithmetic (closest hits bit-exact)", "l2": "flushed (256 MB write) before each step",
                    "parallelism": f"{world} independent ranks, disjoint sample indices"},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": launches_per_step * args.steps,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ctypes.sizeof(cam) + ctypes.sizeof(st),
                 "d2h_bytes_per_step": H * W * 3 * 4, "api": "rn_pt_render with host output buffer"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -332,6 +367,7 @@ def run_ours(args):
                      "kernel_ms": kernel_ms},
         "clocks": clk,
         "rmse_vs_fp64_64spp": rmse,
+        "integrators_samples_per_s": compare,
         "scene_build_ms": info["build_ms"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

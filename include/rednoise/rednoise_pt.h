@@ -189,6 +189,25 @@ rn_status rn_pt_render(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_
 rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
                                   unsigned flags, void *stream, float *accum);
 
+/* ---- autotuning ---- */
+
+/* Result of rn_pt_autotune: the chosen integrator and samples per wave (the
+ * wavefront's path-queue capacity in samples of every pixel), with the measured
+ * throughput of each candidate. */
+typedef struct {
+	int integrator;        /* RN_PT_MEGAKERNEL or RN_PT_WAVEFRONT */
+	int samples_per_wave;  /* wavefront queue capacity = width*height*samples_per_wave paths */
+	double megakernel_sps; /* samples per second of the megakernel */
+	double wavefront_sps;  /* samples per second of the best wavefront configuration */
+} rn_pt_tuning;
+
+/* Time short renders of this scene/camera/settings (a few samples per pixel)
+ * with the megakernel and with the wavefront at several queue capacities, keep
+ * the fastest, and remember it for RN_PT_AUTO renders of the same scene and
+ * image size. `out` may be NULL. */
+rn_status rn_pt_autotune(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings, unsigned flags,
+                         rn_pt_tuning *out);
+
 /* ---- differentiable rendering ---- */
 
 /* Overwrite per-triangle albedo (3 floats per triangle) and / or emitted

@@ -355,6 +355,16 @@ class Scene:
                       "rn_pt_render_accumulate")
         return accum
 
+    def autotune(self, camera: "Camera", settings: "Settings", nearest_first: bool = False) -> dict:
+        """Measure megakernel vs wavefront (and wavefront queue capacities) for this
+        camera / settings; RN_PT_AUTO renders then use the fastest."""
+        self._check_open()
+        t = _native.Tuning()
+        flags = _native.RN_PT_ORDER_NEAREST if nearest_first else 0
+        _native.check(_native.load().rn_pt_autotune(self._handle, ctypes.byref(camera), ctypes.byref(settings), flags,
+                                                    ctypes.byref(t)), "rn_pt_autotune")
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
     def set_materials(self, albedo=None, emission=None) -> None:
         """Overwrite per-triangle albedo and / or emitted radiance (host arrays, n x 3)."""
         self._check_open()

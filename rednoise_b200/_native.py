@@ -183,6 +183,17 @@ class Settings(ctypes.Structure):
         return s
 
 
+class Tuning(ctypes.Structure):
+    """rn_pt_tuning."""
+
+    _fields_ = [
+        ("integrator", ctypes.c_int),
+        ("samples_per_wave", ctypes.c_int),
+        ("megakernel_sps", ctypes.c_double),
+        ("wavefront_sps", ctypes.c_double),
+    ]
+
+
 class Job(ctypes.Structure):
     """rn_pt_job: scene + camera + settings."""
 
@@ -213,6 +224,8 @@ SIGNATURES = {
     "rn_pt_render_accumulate": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                                vp, vp]),
     "rn_pt_count_traversal": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), vp]),
+    "rn_pt_autotune": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
+                                      ctypes.POINTER(Tuning)]),
     "rn_pt_scene_set_materials": (ctypes.c_int, [vp, vp, vp, ctypes.c_uint, vp]),
     "rn_pt_backward": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(Camera), ctypes.POINTER(Settings),
                                       ctypes.POINTER(vp), ctypes.c_uint, vp, vp, vp]),

@@ -90,10 +90,11 @@ using namespace rnb;
 
 namespace {
 
-// Run the selected integrator over accum (device, 3 floats per pixel).
-rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, const PhysScene &ps, const PhysCamera &pc,
-                         const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
-	if (st->integrator == RN_PT_WAVEFRONT) {
+// Run one integrator over accum (device, 3 floats per pixel). spw <= 0 picks the
+// default samples per wave.
+rn_status run_fixed(rn_scene *s, int integrator, int spw, const PhysScene &ps, const PhysCamera &pc,
+                    const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
+	if (integrator == RN_PT_WAVEFRONT) {
 		if (pst.max_depth > kWfMaxDepth) {
 			set_last_error("render: the wavefront integrator supports max_depth <= 64");
 			return RN_ERR_INVALID_ARGUMENT;
@@ -108,8 +109,9 @@ rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, const PhysScene 
 		job.n_pix = pc.width * pc.height;
 		job.spp = pst.spp;
 		s->wf->set_frame_io(nullptr, 0, {});
-		rn_status r = s->wf->configure({job}, pst.max_depth, pst.order, default_samples_per_wave(job.n_pix, job.spp),
-		                               cs);
+		if (spw <= 0)
+			spw = default_samples_per_wave(job.n_pix, job.spp);
+		rn_status r = s->wf->configure({job}, pst.max_depth, pst.order, spw, cs);
 		if (r != RN_OK)
 			return r;
 		return s->wf->launch_graph(s->d_status.as<int>(), cs);
@@ -117,6 +119,81 @@ rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, const PhysScene 
 	RNB_CUDA(s->d_counter.ensure(256));
 	RNB_CUDA(launch_megakernel(ps, pc, pst, d_accum, s->d_counter.as<unsigned>(), s->d_status.as<int>(), cs));
 	return RN_OK;
+}
+
+std::tuple<int, int, int, int> tune_key(const PhysCamera &pc, const PhysSettings &pst) {
+	return {pc.width, pc.height, pst.max_depth, pst.order};
+}
+
+// Measure the candidates on a few samples per pixel and remember the fastest.
+rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc, const PhysSettings &pst,
+                         rn_pt_tuning &out) {
+	PhysSettings probe = pst;
+	probe.spp = pst.spp < 4 ? (pst.spp > 0 ? pst.spp : 1) : 4;
+	probe.sample_offset = 0x40000000u;
+	const size_t bytes = static_cast<size_t>(pc.width) * pc.height * 3 * sizeof(float);
+	RNB_CUDA(s->tune_accum.ensure(bytes));
+	float *acc = s->tune_accum.as<float>();
+	cudaStream_t cs = s->stream;
+	cudaEvent_t e0, e1;
+	RNB_CUDA(cudaEventCreate(&e0));
+	RNB_CUDA(cudaEventCreate(&e1));
+	const double samples = static_cast<double>(pc.width) * pc.height * probe.spp;
+	auto time_one = [&](int integ, int spw, double &sps) -> rn_status {
+		for (int rep = 0; rep < 2; rep++) { // the first run warms caches and captures graphs
+			RNB_CUDA(cudaMemsetAsync(acc, 0, bytes, cs));
+			RNB_CUDA(cudaEventRecord(e0, cs));
+			rn_status r = run_fixed(s, integ, spw, ps, pc, probe, acc, cs);
+			if (r != RN_OK)
+				return r;
+			RNB_CUDA(cudaEventRecord(e1, cs));
+		}
+		RNB_CUDA(cudaEventSynchronize(e1));
+		float ms = 0.0f;
+		RNB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+		sps = ms > 0.0f ? samples / (ms * 1e-3) : 0.0;
+		return RN_OK;
+	};
+	rn_status r = time_one(RN_PT_MEGAKERNEL, 0, out.megakernel_sps);
+	if (r != RN_OK)
+		return r;
+	out.wavefront_sps = 0.0;
+	out.samples_per_wave = 1;
+	const int d = default_samples_per_wave(static_cast<long>(pc.width) * pc.height, probe.spp);
+	for (int spw : {d, 2 * d, 4 * d}) {
+		if (spw > probe.spp)
+			break;
+		double sps = 0.0;
+		r = time_one(RN_PT_WAVEFRONT, spw, sps);
+		if (r != RN_OK)
+			return r;
+		if (sps > out.wavefront_sps) {
+			out.wavefront_sps = sps;
+			out.samples_per_wave = spw;
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	out.integrator = out.wavefront_sps > out.megakernel_sps ? RN_PT_WAVEFRONT : RN_PT_MEGAKERNEL;
+	s->tuned[tune_key(pc, pst)] = {out.integrator, out.samples_per_wave};
+	return RN_OK;
+}
+
+// Run the integrator the settings ask for; RN_PT_AUTO uses (and on first use
+// measures) the scene's tuned choice for this image size.
+rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, const PhysScene &ps, const PhysCamera &pc,
+                         const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
+	if (st->integrator == RN_PT_MEGAKERNEL || st->integrator == RN_PT_WAVEFRONT)
+		return run_fixed(s, st->integrator, 0, ps, pc, pst, d_accum, cs);
+	auto it = s->tuned.find(tune_key(pc, pst));
+	if (it == s->tuned.end()) {
+		rn_pt_tuning t{};
+		rn_status r = autotune_scene(s, ps, pc, pst, t);
+		if (r != RN_OK)
+			return r;
+		it = s->tuned.find(tune_key(pc, pst));
+	}
+	return run_fixed(s, it->second.first, it->second.second, ps, pc, pst, d_accum, cs);
 }
 
 rn_status finish_sync(rn_scene *s, cudaStream_t cs, const char *what) {
@@ -160,6 +237,23 @@ rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, c
 		return r;
 	RNB_CUDA(cudaMemcpyAsync(accum, d, bytes, cudaMemcpyDeviceToHost, cs));
 	return finish_sync(scene, cs, "rn_pt_render_accumulate");
+}
+
+rn_status rn_pt_autotune(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings, unsigned flags,
+                         rn_pt_tuning *out) {
+	PhysScene ps;
+	PhysCamera pc;
+	PhysSettings pst;
+	rn_status r = make_phys_inputs(scene, camera, settings, flags, ps, pc, pst);
+	if (r != RN_OK)
+		return r;
+	rn_pt_tuning t{};
+	r = autotune_scene(scene, ps, pc, pst, t);
+	if (r != RN_OK)
+		return r;
+	if (out)
+		*out = t;
+	return RN_OK;
 }
 
 rn_status rn_pt_count_traversal(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
