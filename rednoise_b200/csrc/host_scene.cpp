@@ -370,12 +370,11 @@ void flatten_bvh4(const Bvh2 &bvh, DeviceLayout4 &out) {
 			}
 		}
 		F4 *o = &out.nodes[static_cast<size_t>(slot) * 8];
-		o[0] = {lo[0][0], lo[0][1], lo[0][2], lo[0][3]};
-		o[1] = {hi[0][0], hi[0][1], hi[0][2], hi[0][3]};
-		o[2] = {lo[1][0], lo[1][1], lo[1][2], lo[1][3]};
-		o[3] = {hi[1][0], hi[1][1], hi[1][2], hi[1][3]};
-		o[4] = {lo[2][0], lo[2][1], lo[2][2], lo[2][3]};
-		o[5] = {hi[2][0], hi[2][1], hi[2][2], hi[2][3]};
+		// (lo, hi) pairs per axis and entry, two entries per float4.
+		for (int a = 0; a < 3; a++) {
+			o[2 * a] = {lo[a][0], hi[a][0], lo[a][1], hi[a][1]};
+			o[2 * a + 1] = {lo[a][2], hi[a][2], lo[a][3], hi[a][3]};
+		}
 		o[6] = {as_float(refs[0]), as_float(refs[1]), as_float(refs[2]), as_float(refs[3])};
 		o[7] = {as_float(cnt), 0.0f, 0.0f, 0.0f};
 	}

@@ -104,14 +104,15 @@ void flatten_bvh(const TriangleSet &ts, const Bvh2 &bvh, DeviceLayout &out);
 
 // Four-wide collapse of the same tree for the fast traversal. A node holds the
 // children of one reference node, with every internal child replaced by its own
-// two children (so up to four entries), in the order the reference pops them:
-//   8 float4 per node: lo.x[4], hi.x[4], lo.y[4], hi.y[4], lo.z[4], hi.z[4],
-//   refs[4] (int bits; >= 0 node, < 0 leaf as in the 2-wide layout), (count, 0, 0, 0).
+// two children (so up to four entries), in the order the reference pops them;
+// refs are int bits (>= 0 node, < 0 leaf as in the 2-wide layout).
 // Boxes are the reference's own node boxes. Because float subtraction and
 // multiplication round monotonically, a grandchild's slab interval lies inside
 // its parent's, so skipping the parent's test never admits a node the
 // reference would prune (rays with an infinite 1/d component excepted: those
 // use the 2-wide layout).
+// Node rows: [2a] = (lo_a[0], hi_a[0], lo_a[1], hi_a[1]), [2a+1] = entries 2, 3,
+// for axis a = x, y, z; [6] = refs[4]; [7] = (count, 0, 0, 0).
 struct DeviceLayout4 {
 	std::vector<F4> nodes;
 	int root_ref = 0; // node index, or a leaf ref when the reference root is a leaf

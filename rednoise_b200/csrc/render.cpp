@@ -129,7 +129,7 @@ std::tuple<int, int, int, int> tune_key(const PhysCamera &pc, const PhysSettings
 rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc, const PhysSettings &pst,
                          rn_pt_tuning &out) {
 	PhysSettings probe = pst;
-	probe.spp = pst.spp < 4 ? (pst.spp > 0 ? pst.spp : 1) : 4;
+	probe.spp = pst.spp < 16 ? (pst.spp > 0 ? pst.spp : 1) : 16;
 	probe.sample_offset = 0x40000000u;
 	const size_t bytes = static_cast<size_t>(pc.width) * pc.height * 3 * sizeof(float);
 	RNB_CUDA(s->tune_accum.ensure(bytes));
@@ -160,7 +160,7 @@ rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc,
 	out.wavefront_sps = 0.0;
 	out.samples_per_wave = 1;
 	const int d = default_samples_per_wave(static_cast<long>(pc.width) * pc.height, probe.spp);
-	for (int spw : {d, 2 * d, 4 * d}) {
+	for (int spw : {d, 2 * d, 4 * d, 8 * d, 16 * d}) {
 		if (spw > probe.spp)
 			break;
 		double sps = 0.0;

@@ -344,61 +344,108 @@ __device__ __forceinline__ bool trace_any(const SceneView &s, const RayPre &r, f
 // or subnormal direction component, where a slab product can be NaN) take the
 // 2-wide path instead.
 
+// Paired single-precision arithmetic of sm_100 (PTX add/sub/mul .rn.f32x2): two
+// independently, correctly rounded IEEE operations per instruction, so the slab
+// products keep the reference's bits at half the instruction count.
+__device__ __forceinline__ unsigned long long pair2(float lo, float hi) {
+	unsigned long long r;
+	asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+	return r;
+}
+__device__ __forceinline__ void unpair2(unsigned long long v, float &lo, float &hi) {
+	asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+	unsigned long long r;
+	asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+	return r;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+	unsigned long long r;
+	asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+	return r;
+}
+
+// The ray's origin and inverse direction duplicated into pairs.
+struct RayPair {
+	unsigned long long ox, oy, oz, ix, iy, iz;
+};
+__device__ __forceinline__ RayPair make_pair_ray(const RayPre &r) {
+	return {pair2(r.ox, r.ox), pair2(r.oy, r.oy), pair2(r.oz, r.oz),
+	        pair2(r.ix, r.ix), pair2(r.iy, r.iy), pair2(r.iz, r.iz)};
+}
+
+// The reference slab test on (lo, hi) pairs; valid for rays whose inverse
+// direction is finite: then no product is NaN, so fminf/fmaxf return the same
+// values as glm's and std::min/max's comparisons (a +0/-0 difference in tenter
+// changes no comparison the traversal makes).
+__device__ __forceinline__ bool slab2(unsigned long long x, unsigned long long y, unsigned long long z,
+                                      const RayPair &r, float &tenter) {
+	float t0x, t1x, t0y, t1y, t0z, t1z;
+	unpair2(mul2(sub2(x, r.ox), r.ix), t0x, t1x);
+	unpair2(mul2(sub2(y, r.oy), r.iy), t0y, t1y);
+	unpair2(mul2(sub2(z, r.oz), r.iz), t0z, t1z);
+	const float te = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
+	const float tx = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
+	tenter = te;
+	return tx >= fmaxf(te, 0.0f);
+}
+
+__device__ __forceinline__ unsigned long long pack_entry(int ref, float tenter) {
+	return (static_cast<unsigned long long>(static_cast<unsigned>(__float_as_int(tenter))) << 32) |
+	       static_cast<unsigned>(ref);
+}
+
 __device__ __forceinline__ bool finite_inverse(const RayPre &r) {
 	return fabsf(r.ix) < __int_as_float(0x7f800000) && fabsf(r.iy) < __int_as_float(0x7f800000) &&
 	       fabsf(r.iz) < __int_as_float(0x7f800000);
 }
 
 __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPre &r, int ignore, int &err) {
+	const RayPair r2 = make_pair_ray(r);
 	HitRec h;
 	h.idx = -1;
 	h.rank = 0x7fffffff;
 	h.t = __int_as_float(0x7f800000);
 	h.u = 0.0f;
 	h.v = 0.0f;
-	int st_ref[kStack];
-	float st_t[kStack];
+	// Stack entry: node or leaf ref in the low word, its entry distance in the high
+	// word, pushed and popped as one 64-bit local-memory access.
+	unsigned long long st[kStack];
 	int sp = 0;
 	float te;
 	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te)) {
-		st_ref[0] = s.root4_ref;
-		st_t[0] = te;
+		st[0] = pack_entry(s.root4_ref, te);
 		sp = 1;
 	}
 	while (sp > 0) {
 		--sp;
-		int ref = st_ref[sp];
-		if (!(st_t[sp] < h.t))
+		const unsigned long long e = st[sp];
+		int ref = static_cast<int>(static_cast<unsigned>(e));
+		if (!(__int_as_float(static_cast<int>(e >> 32)) < h.t))
 			continue;
 		while (ref >= 0) {
 			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ref);
-			const float4 lx = __ldg(nd + 0), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
-			const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5), rf = __ldg(nd + 6);
+			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
+			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
+			const ulonglong2 z01 = __ldg(nq + 4), z23 = __ldg(nq + 5);
+			const float4 rf = __ldg(nd + 6);
 			const int cnt = __float_as_int(__ldg(nd + 7).x);
 			float t0, t1, t2, t3;
-			const bool b0 = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, t0);
-			const bool b1 = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, t1);
-			const bool b2 = cnt > 2 && slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, t2);
-			const bool b3 = cnt > 3 && slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, t3);
+			const bool b0 = slab2(x01.x, y01.x, z01.x, r2, t0);
+			const bool b1 = slab2(x01.y, y01.y, z01.y, r2, t1);
+			const bool b2 = cnt > 2 && slab2(x23.x, y23.x, z23.x, r2, t2);
+			const bool b3 = cnt > 3 && slab2(x23.y, y23.y, z23.y, r2, t3);
 			if (sp + 3 > kStack) {
 				err = 1;
 				return h;
 			}
-			if (b3) {
-				st_ref[sp] = __float_as_int(rf.w);
-				st_t[sp] = t3;
-				++sp;
-			}
-			if (b2) {
-				st_ref[sp] = __float_as_int(rf.z);
-				st_t[sp] = t2;
-				++sp;
-			}
-			if (b1) {
-				st_ref[sp] = __float_as_int(rf.y);
-				st_t[sp] = t1;
-				++sp;
-			}
+			if (b3)
+				st[sp++] = pack_entry(__float_as_int(rf.w), t3);
+			if (b2)
+				st[sp++] = pack_entry(__float_as_int(rf.z), t2);
+			if (b1)
+				st[sp++] = pack_entry(__float_as_int(rf.y), t1);
 			if (b0 && t0 < h.t) {
 				ref = __float_as_int(rf.x);
 			} else {
@@ -432,6 +479,7 @@ __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPr
 }
 
 __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err) {
+	const RayPair r2 = make_pair_ray(r);
 	int st[kStack];
 	int sp = 0;
 	float te;
@@ -444,14 +492,16 @@ __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, 
 		int ref = st[--sp];
 		while (ref >= 0) {
 			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ref);
-			const float4 lx = __ldg(nd + 0), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
-			const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5), rf = __ldg(nd + 6);
+			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
+			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
+			const ulonglong2 z01 = __ldg(nq + 4), z23 = __ldg(nq + 5);
+			const float4 rf = __ldg(nd + 6);
 			const int cnt = __float_as_int(__ldg(nd + 7).x);
 			float t0, t1, t2, t3;
-			const bool b0 = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, t0) && t0 < tmax;
-			const bool b1 = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, t1) && t1 < tmax;
-			const bool b2 = cnt > 2 && slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, t2) && t2 < tmax;
-			const bool b3 = cnt > 3 && slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, t3) && t3 < tmax;
+			const bool b0 = slab2(x01.x, y01.x, z01.x, r2, t0) && t0 < tmax;
+			const bool b1 = slab2(x01.y, y01.y, z01.y, r2, t1) && t1 < tmax;
+			const bool b2 = cnt > 2 && slab2(x23.x, y23.x, z23.x, r2, t2) && t2 < tmax;
+			const bool b3 = cnt > 3 && slab2(x23.y, y23.y, z23.y, r2, t3) && t3 < tmax;
 			if (sp + 3 > kStack) {
 				err = 1;
 				return false;
