@@ -199,6 +199,7 @@ typedef struct {
 	int samples_per_wave;  /* wavefront queue capacity = width*height*samples_per_wave paths */
 	double megakernel_sps; /* samples per second of the megakernel */
 	double wavefront_sps;  /* samples per second of the best wavefront configuration */
+	int dynamic_fetch;     /* wavefront traversal stages hand new rays to lanes whose ray finished */
 } rn_pt_tuning;
 
 /* Time short renders of this scene/camera/settings (a few samples per pixel)

@@ -191,6 +191,7 @@ class Tuning(ctypes.Structure):
         ("samples_per_wave", ctypes.c_int),
         ("megakernel_sps", ctypes.c_double),
         ("wavefront_sps", ctypes.c_double),
+        ("dynamic_fetch", ctypes.c_int),
     ]
 
 

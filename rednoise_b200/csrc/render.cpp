@@ -91,8 +91,8 @@ using namespace rnb;
 namespace {
 
 // Run one integrator over accum (device, 3 floats per pixel). spw <= 0 picks the
-// default samples per wave.
-rn_status run_fixed(rn_scene *s, int integrator, int spw, const PhysScene &ps, const PhysCamera &pc,
+// default samples per wave; dyn selects the wavefront's per-lane ray replacement.
+rn_status run_fixed(rn_scene *s, int integrator, int spw, int dyn, const PhysScene &ps, const PhysCamera &pc,
                     const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
 	if (integrator == RN_PT_WAVEFRONT) {
 		if (pst.max_depth > kWfMaxDepth) {
@@ -109,6 +109,7 @@ rn_status run_fixed(rn_scene *s, int integrator, int spw, const PhysScene &ps, c
 		job.n_pix = pc.width * pc.height;
 		job.spp = pst.spp;
 		s->wf->set_frame_io(nullptr, 0, {});
+		s->wf->set_dynamic(dyn);
 		if (spw <= 0)
 			spw = default_samples_per_wave(job.n_pix, job.spp);
 		rn_status r = s->wf->configure({job}, pst.max_depth, pst.order, spw, cs);
@@ -125,7 +126,9 @@ std::tuple<int, int, int, int> tune_key(const PhysCamera &pc, const PhysSettings
 	return {pc.width, pc.height, pst.max_depth, pst.order};
 }
 
-// Measure the candidates on a few samples per pixel and remember the fastest.
+// Measure the candidates on a few samples per pixel and remember the fastest:
+// the megakernel, and the wavefront at 1x..16x the default queue capacity with
+// and without per-lane ray replacement in its traversal stages.
 rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc, const PhysSettings &pst,
                          rn_pt_tuning &out) {
 	PhysSettings probe = pst;
@@ -139,11 +142,11 @@ rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc,
 	RNB_CUDA(cudaEventCreate(&e0));
 	RNB_CUDA(cudaEventCreate(&e1));
 	const double samples = static_cast<double>(pc.width) * pc.height * probe.spp;
-	auto time_one = [&](int integ, int spw, double &sps) -> rn_status {
+	auto time_one = [&](int integ, int spw, int dyn, double &sps) -> rn_status {
 		for (int rep = 0; rep < 2; rep++) { // the first run warms caches and captures graphs
 			RNB_CUDA(cudaMemsetAsync(acc, 0, bytes, cs));
 			RNB_CUDA(cudaEventRecord(e0, cs));
-			rn_status r = run_fixed(s, integ, spw, ps, pc, probe, acc, cs);
+			rn_status r = run_fixed(s, integ, spw, dyn, ps, pc, probe, acc, cs);
 			if (r != RN_OK)
 				return r;
 			RNB_CUDA(cudaEventRecord(e1, cs));
@@ -154,28 +157,34 @@ rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc,
 		sps = ms > 0.0f ? samples / (ms * 1e-3) : 0.0;
 		return RN_OK;
 	};
-	rn_status r = time_one(RN_PT_MEGAKERNEL, 0, out.megakernel_sps);
+	rn_status r = time_one(RN_PT_MEGAKERNEL, 0, 0, out.megakernel_sps);
 	if (r != RN_OK)
 		return r;
 	out.wavefront_sps = 0.0;
 	out.samples_per_wave = 1;
+	out.dynamic_fetch = 1;
 	const int d = default_samples_per_wave(static_cast<long>(pc.width) * pc.height, probe.spp);
-	for (int spw : {d, 2 * d, 4 * d, 8 * d, 16 * d}) {
-		if (spw > probe.spp)
-			break;
-		double sps = 0.0;
-		r = time_one(RN_PT_WAVEFRONT, spw, sps);
-		if (r != RN_OK)
-			return r;
-		if (sps > out.wavefront_sps) {
-			out.wavefront_sps = sps;
-			out.samples_per_wave = spw;
+	for (int dyn : {1, 0}) {
+		if (dyn && pst.order != kOrderReference)
+			continue;
+		for (int spw : {d, 2 * d, 4 * d, 8 * d, 16 * d}) {
+			if (spw > probe.spp)
+				break;
+			double sps = 0.0;
+			r = time_one(RN_PT_WAVEFRONT, spw, dyn, sps);
+			if (r != RN_OK)
+				return r;
+			if (sps > out.wavefront_sps) {
+				out.wavefront_sps = sps;
+				out.samples_per_wave = spw;
+				out.dynamic_fetch = dyn;
+			}
 		}
 	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	out.integrator = out.wavefront_sps > out.megakernel_sps ? RN_PT_WAVEFRONT : RN_PT_MEGAKERNEL;
-	s->tuned[tune_key(pc, pst)] = {out.integrator, out.samples_per_wave};
+	s->tuned[tune_key(pc, pst)] = {out.integrator, out.samples_per_wave, out.dynamic_fetch};
 	return RN_OK;
 }
 
@@ -183,9 +192,16 @@ rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc,
 // measures) the scene's tuned choice for this image size.
 rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, const PhysScene &ps, const PhysCamera &pc,
                          const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
-	if (st->integrator == RN_PT_MEGAKERNEL || st->integrator == RN_PT_WAVEFRONT)
-		return run_fixed(s, st->integrator, 0, ps, pc, pst, d_accum, cs);
 	auto it = s->tuned.find(tune_key(pc, pst));
+	if (st->integrator == RN_PT_MEGAKERNEL)
+		return run_fixed(s, RN_PT_MEGAKERNEL, 0, 0, ps, pc, pst, d_accum, cs);
+	if (st->integrator == RN_PT_WAVEFRONT) {
+		// An explicit wavefront render keeps the tuned queue capacity when there is one.
+		if (it != s->tuned.end() && std::get<0>(it->second) == RN_PT_WAVEFRONT)
+			return run_fixed(s, RN_PT_WAVEFRONT, std::get<1>(it->second), std::get<2>(it->second), ps, pc, pst,
+			                 d_accum, cs);
+		return run_fixed(s, RN_PT_WAVEFRONT, 0, 1, ps, pc, pst, d_accum, cs);
+	}
 	if (it == s->tuned.end()) {
 		rn_pt_tuning t{};
 		rn_status r = autotune_scene(s, ps, pc, pst, t);
@@ -193,7 +209,8 @@ rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, const PhysScene 
 			return r;
 		it = s->tuned.find(tune_key(pc, pst));
 	}
-	return run_fixed(s, it->second.first, it->second.second, ps, pc, pst, d_accum, cs);
+	const auto [integ, spw, dyn] = it->second;
+	return run_fixed(s, integ, spw, dyn, ps, pc, pst, d_accum, cs);
 }
 
 rn_status finish_sync(rn_scene *s, cudaStream_t cs, const char *what) {

@@ -44,8 +44,9 @@ struct rn_scene {
 	rnb::DevBuf adj; // view table and gradient buffers of device-pointer adjoint calls
 	// Wavefront pools and the captured frame graph of single-scene renders.
 	std::unique_ptr<rnb::WfContext> wf;
-	// Autotuner choices per (width, height, max_depth, order): (integrator, samples per wave).
-	std::map<std::tuple<int, int, int, int>, std::pair<int, int>> tuned;
+	// Autotuner choices per (width, height, max_depth, order):
+	// (integrator, samples per wave, per-lane ray replacement).
+	std::map<std::tuple<int, int, int, int>, std::tuple<int, int, int>> tuned;
 	rnb::DevBuf tune_accum;
 
 	~rn_scene();

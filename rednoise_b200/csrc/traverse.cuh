@@ -366,6 +366,18 @@ __device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigne
 	return r;
 }
 
+// Three-input min / max of sm_100 (PTX min.f32 / max.f32 with three sources).
+__device__ __forceinline__ float max3(float a, float b, float c) {
+	float r;
+	asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+	return r;
+}
+__device__ __forceinline__ float min3(float a, float b, float c) {
+	float r;
+	asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+	return r;
+}
+
 // The ray's origin and inverse direction duplicated into pairs.
 struct RayPair {
 	unsigned long long ox, oy, oz, ix, iy, iz;
@@ -385,8 +397,8 @@ __device__ __forceinline__ bool slab2(unsigned long long x, unsigned long long y
 	unpair2(mul2(sub2(x, r.ox), r.ix), t0x, t1x);
 	unpair2(mul2(sub2(y, r.oy), r.iy), t0y, t1y);
 	unpair2(mul2(sub2(z, r.oz), r.iz), t0z, t1z);
-	const float te = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
-	const float tx = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
+	const float te = max3(fminf(t0x, t1x), fminf(t0y, t1y), fminf(t0z, t1z));
+	const float tx = min3(fmaxf(t0x, t1x), fmaxf(t0y, t1y), fmaxf(t0z, t1z));
 	tenter = te;
 	return tx >= fmaxf(te, 0.0f);
 }
@@ -538,6 +550,118 @@ __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, 
 		}
 	}
 	return false;
+}
+
+// ---- resumable 4-wide traversal for persistent kernels that replace finished rays ----
+// The same visit order and tests as trace_closest4 / trace_any4, cut into steps
+// (one pop, a descent through internal nodes, one leaf) so that a warp can hand
+// a new ray to every lane whose ray has finished between steps.
+constexpr int kPopRef = static_cast<int>(0x80000000u); // no leaf ref can take this value
+
+struct TravState {
+	RayPre r;
+	RayPair r2;
+	HitRec h;
+	float tmax; // any-hit bound (closest hit: unused)
+	int ignore;
+	int cur;    // node (>= 0), leaf (< 0), or kPopRef
+	int sp;
+	bool hit_any;
+	unsigned long long st[kStack];
+};
+
+// Start a ray: root box test as in trace_closest4 / trace_any4.
+template <bool kAny>
+__device__ __forceinline__ void trav_begin(TravState &ts, const SceneView &s, const RayPre &r, float tmax, int ignore) {
+	ts.r = r;
+	ts.r2 = make_pair_ray(r);
+	ts.h.idx = -1;
+	ts.h.rank = 0x7fffffff;
+	ts.h.t = __int_as_float(0x7f800000);
+	ts.h.u = ts.h.v = 0.0f;
+	ts.tmax = tmax;
+	ts.ignore = ignore;
+	ts.hit_any = false;
+	ts.sp = 0;
+	ts.cur = kPopRef;
+	float te;
+	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te) &&
+	    (!kAny || te < tmax)) {
+		ts.st[0] = pack_entry(s.root4_ref, te);
+		ts.sp = 1;
+	}
+}
+
+// One step; returns false once the ray is finished.
+template <bool kAny>
+__device__ __forceinline__ bool trav_step(TravState &ts, const SceneView &s, int &err) {
+	const float bound = kAny ? ts.tmax : ts.h.t;
+	if (ts.cur == kPopRef) {
+		if (ts.sp == 0)
+			return false;
+		const unsigned long long e = ts.st[--ts.sp];
+		if (!kAny && !(__int_as_float(static_cast<int>(e >> 32)) < bound))
+			return true;
+		ts.cur = static_cast<int>(static_cast<unsigned>(e));
+	}
+	while (ts.cur >= 0) {
+		const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ts.cur);
+		const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
+		const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
+		const ulonglong2 z01 = __ldg(nq + 4), z23 = __ldg(nq + 5);
+		const float4 rf = __ldg(nd + 6);
+		const int cnt = __float_as_int(__ldg(nd + 7).x);
+		float t0, t1, t2, t3;
+		const float b = kAny ? ts.tmax : ts.h.t;
+		const bool b0 = slab2(x01.x, y01.x, z01.x, ts.r2, t0) && t0 < b;
+		const bool b1 = slab2(x01.y, y01.y, z01.y, ts.r2, t1) && (!kAny || t1 < b);
+		const bool b2 = cnt > 2 && slab2(x23.x, y23.x, z23.x, ts.r2, t2) && (!kAny || t2 < b);
+		const bool b3 = cnt > 3 && slab2(x23.y, y23.y, z23.y, ts.r2, t3) && (!kAny || t3 < b);
+		if (ts.sp + 3 > kStack) {
+			err = 1;
+			return false;
+		}
+		if (b3)
+			ts.st[ts.sp++] = pack_entry(__float_as_int(rf.w), t3);
+		if (b2)
+			ts.st[ts.sp++] = pack_entry(__float_as_int(rf.z), t2);
+		if (b1)
+			ts.st[ts.sp++] = pack_entry(__float_as_int(rf.y), t1);
+		if (!b0) {
+			ts.cur = kPopRef;
+			return true;
+		}
+		ts.cur = __float_as_int(rf.x);
+	}
+	// Leaf.
+	const int start = leaf_start(ts.cur);
+	const int count = leaf_count(ts.cur);
+	ts.cur = kPopRef;
+	for (int p = start; p < start + count; p++) {
+		const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
+		const float4 a = __ldg(tp + 0);
+		const int ti = __float_as_int(a.w);
+		if (ti == ts.ignore)
+			continue;
+		const float4 bb = __ldg(tp + 1);
+		const float4 c = __ldg(tp + 2);
+		float t, u, v;
+		if (!tri_test(a, bb, c, ts.r, t, u, v))
+			continue;
+		if (kAny) {
+			if (t < ts.tmax) {
+				ts.hit_any = true;
+				return false;
+			}
+		} else if (t < ts.h.t) {
+			ts.h.idx = ti;
+			ts.h.t = t;
+			ts.h.u = u;
+			ts.h.v = v;
+			ts.h.rank = __float_as_int(bb.w);
+		}
+	}
+	return true;
 }
 
 // Closest hit / occlusion with the fastest layout that keeps the reference result.

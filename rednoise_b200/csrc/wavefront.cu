@@ -162,6 +162,96 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 		atomicOr(status, 1);
 }
 
+// Persistent traversal with per-lane ray replacement: a lane whose ray finished
+// takes the next queued ray at the following step, so warps stay full while the
+// queue lasts (closest hits for the extend stage, any hits for shadow records).
+template <bool kAny>
+__global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ jobs, WfPool pool, int k,
+                                                      int *status) {
+	const unsigned n = pool.counters[(kAny ? kCntShadow : kCntRays) + k];
+	unsigned *fetch = pool.counters + (kAny ? kCntFetchSh : kCntFetchExt) + k;
+	const int *__restrict__ q = pool.queue[k & 1];
+	const int lane = threadIdx.x & 31;
+	int err = 0;
+	TravState ts;
+	const WfJob *jb = nullptr;
+	int slot = -1;
+	unsigned rec = 0;
+	bool active = false, exhausted = false;
+	for (;;) {
+		const unsigned idle = __ballot_sync(0xffffffffu, !active);
+		if (idle && !exhausted) {
+			unsigned base = 0;
+			if (lane == 0)
+				base = atomicAdd(fetch, static_cast<unsigned>(__popc(idle)));
+			base = __shfl_sync(0xffffffffu, base, 0);
+			if (base + static_cast<unsigned>(__popc(idle)) >= n)
+				exhausted = true;
+			if (!active) {
+				const unsigned i = base + static_cast<unsigned>(__popc(idle & lanemask_lt()));
+				if (i < n) {
+					RayPre r;
+					float tmax = 0.0f;
+					int ignore;
+					if (kAny) {
+						const float4 so = pool.sh_o[i], sd = pool.sh_d[i];
+						rec = i;
+						slot = __float_as_int(pool.sh_c[i].w);
+						r = make_ray(so.x, so.y, so.z, sd.x, sd.y, sd.z);
+						tmax = so.w;
+						ignore = __float_as_int(sd.w);
+					} else {
+						slot = q[i];
+						const float4 o = pool.o[slot], d = pool.d[slot];
+						r = make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
+						ignore = __float_as_int(o.w);
+					}
+					jb = jobs + __float_as_int(pool.L[slot].w);
+					if (jb->sc.sv.nodes4 && finite_inverse(r)) {
+						trav_begin<kAny>(ts, jb->sc.sv, r, tmax, ignore);
+						active = true;
+					} else if (kAny) { // rays with an infinite 1/d component: 2-wide path at once
+						if (!trace_any(jb->sc.sv, r, tmax, ignore, err)) {
+							const float4 c = pool.sh_c[i];
+							float4 L = pool.L[slot];
+							L.x += c.x;
+							L.y += c.y;
+							L.z += c.z;
+							pool.L[slot] = L;
+						}
+					} else {
+						const HitRec h = trace_closest<kOrderReference>(jb->sc.sv, r, ignore, err);
+						pool.hit_idx[slot] = h.idx;
+						pool.hit_t[slot] = h.t;
+					}
+				}
+			}
+		}
+		if (!__any_sync(0xffffffffu, active) && exhausted)
+			break;
+		if (active && !trav_step<kAny>(ts, jb->sc.sv, err)) {
+			active = false;
+			if (kAny) {
+				if (!ts.hit_any) {
+					const float4 c = pool.sh_c[rec];
+					float4 L = pool.L[slot];
+					L.x += c.x;
+					L.y += c.y;
+					L.z += c.z;
+					pool.L[slot] = L;
+				}
+			} else {
+				pool.hit_idx[slot] = ts.h.idx;
+				pool.hit_t[slot] = ts.h.t;
+			}
+		}
+		if (err) // a corrupt tree: stop this warp's lanes from looping on it
+			active = false;
+	}
+	if (err)
+		atomicOr(status, 1);
+}
+
 // Adds each pixel's samples of this wave to its sum, in sample order.
 __global__ void __launch_bounds__(256) k_wf_accumulate(const WfJob *__restrict__ jobs, WfPool pool, WfWave wave) {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < wave.n_pix; i += gridDim.x * blockDim.x) {
@@ -186,7 +276,8 @@ __global__ void __launch_bounds__(256) k_wf_accumulate(const WfJob *__restrict__
 } // namespace
 
 cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave &wave, int max_depth, int order,
-                           int grid_ext, int grid_shade, int grid_sh, int *status, cudaStream_t st) {
+                           int dyn, int grid_ext, int grid_shade, int grid_sh, int grid_dyn, int *status,
+                           cudaStream_t st) {
 	if (wave.n_slots <= 0)
 		return cudaSuccess;
 	cudaError_t e = cudaMemsetAsync(pool.counters, 0, kCntTotal * sizeof(unsigned), st);
@@ -194,13 +285,19 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 		return e;
 	const int gcam = (wave.n_slots + 255) / 256 < 148 * 8 ? (wave.n_slots + 255) / 256 : 148 * 8;
 	k_wf_camera<<<gcam, 256, 0, st>>>(d_jobs, pool, wave);
+	const bool use_dyn = dyn && order == kOrderReference;
 	for (int k = 0; k < max_depth; k++) {
-		if (order == kOrderNearest)
+		if (use_dyn)
+			k_wf_trace_dyn<false><<<grid_dyn, 128, 0, st>>>(d_jobs, pool, k, status);
+		else if (order == kOrderNearest)
 			k_wf_extend<kOrderNearest><<<grid_ext, 128, 0, st>>>(d_jobs, pool, k, status);
 		else
 			k_wf_extend<kOrderReference><<<grid_ext, 128, 0, st>>>(d_jobs, pool, k, status);
 		k_wf_shade<<<grid_shade, 128, 0, st>>>(d_jobs, pool, k);
-		k_wf_shadow<<<grid_sh, 128, 0, st>>>(d_jobs, pool, k, status);
+		if (use_dyn)
+			k_wf_trace_dyn<true><<<grid_dyn, 128, 0, st>>>(d_jobs, pool, k, status);
+		else
+			k_wf_shadow<<<grid_sh, 128, 0, st>>>(d_jobs, pool, k, status);
 	}
 	const int gacc = (wave.n_pix + 255) / 256 < 148 * 8 ? (wave.n_pix + 255) / 256 : 148 * 8;
 	k_wf_accumulate<<<gacc, 256, 0, st>>>(d_jobs, pool, wave);
@@ -208,17 +305,21 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 }
 
 // Persistent grid sizes (blocks resident on all SMs).
-void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh) {
+void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn) {
 	int dev = 0, sms = 148;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	int a = 0, b = 0, c = 0;
+	int a = 0, b = 0, c = 0, d0 = 0, d1 = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_wf_extend<kOrderNearest>, 128, 0);
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_wf_shade, 128, 0);
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_wf_shadow, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d0, k_wf_trace_dyn<false>, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d1, k_wf_trace_dyn<true>, 128, 0);
 	grid_ext = sms * (a > 0 ? a : 1);
 	grid_shade = sms * (b > 0 ? b : 1);
 	grid_sh = sms * (c > 0 ? c : 1);
+	const int d = d0 < d1 ? d0 : d1;
+	grid_dyn = sms * (d > 0 ? d : 1);
 }
 
 } // namespace rnb

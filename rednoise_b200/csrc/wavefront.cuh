@@ -73,7 +73,9 @@ struct WfWave {
 	int first_sample;   // sample index of k = 0, relative to each job's sample_offset
 };
 
+// dyn = 1: traversal stages use persistent warps that replace finished rays per lane.
 cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave &wave, int max_depth, int order,
-                           int grid_ext, int grid_shade, int grid_sh, int *status, cudaStream_t st);
+                           int dyn, int grid_ext, int grid_shade, int grid_sh, int grid_dyn, int *status,
+                           cudaStream_t st);
 
 } // namespace rnb

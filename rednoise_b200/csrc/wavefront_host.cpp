@@ -118,7 +118,7 @@ rn_status WfContext::configure(const std::vector<WfJob> &jobs, int max_depth, in
 	if (r != RN_OK)
 		return r;
 	if (grid_ext_ == 0)
-		wf_grid_sizes(grid_ext_, grid_shade_, grid_sh_);
+		wf_grid_sizes(grid_ext_, grid_shade_, grid_sh_, grid_dyn_);
 	host_jobs_ = jobs;
 	host_tab_ = tab;
 	RNB_CUDA(d_jobs_.ensure(jobs.size() * sizeof(WfJob)));
@@ -163,8 +163,8 @@ rn_status WfContext::enqueue(int *status, cudaStream_t st) {
 	if (zero_ptr_ && zero_bytes_)
 		RNB_CUDA(cudaMemsetAsync(zero_ptr_, 0, zero_bytes_, st));
 	for (const WfWave &w : waves_)
-		RNB_CUDA(wf_launch_wave(d_jobs_.as<WfJob>(), pool_, w, max_depth_, order_, grid_ext_, grid_shade_, grid_sh_,
-		                        status, st));
+		RNB_CUDA(wf_launch_wave(d_jobs_.as<WfJob>(), pool_, w, max_depth_, order_, dyn_, grid_ext_, grid_shade_,
+		                        grid_sh_, grid_dyn_, status, st));
 	for (const Resolve &r : resolves_)
 		RNB_CUDA(launch_resolve(r.accum, r.mean, r.n_floats, r.inv_spp, st));
 	return RN_OK;

@@ -11,7 +11,7 @@
 
 namespace rnb {
 
-void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh);
+void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn);
 
 // Samples per wave that keep about 2^20 paths in flight (at least 1, at most spp).
 inline int default_samples_per_wave(long n_pix, int spp) {
@@ -44,6 +44,13 @@ public:
 	// Capture the frame into a CUDA graph on first use, then launch it.
 	rn_status launch_graph(int *status, cudaStream_t st);
 	int capacity() const { return capacity_; }
+	// Traversal stages with per-lane ray replacement (1, default) or one ray per lane (0).
+	void set_dynamic(int dyn) {
+		if (dyn != dyn_)
+			release_graph();
+		dyn_ = dyn;
+	}
+	int dynamic() const { return dyn_; }
 
 private:
 	rn_status ensure_pool(int capacity);
@@ -55,7 +62,8 @@ private:
 	int capacity_ = 0;
 	int max_depth_ = 0;
 	int order_ = 0;
-	int grid_ext_ = 0, grid_shade_ = 0, grid_sh_ = 0;
+	int grid_ext_ = 0, grid_shade_ = 0, grid_sh_ = 0, grid_dyn_ = 0;
+	int dyn_ = 1;
 	std::vector<WfWave> waves_;
 	std::vector<WfJob> host_jobs_; // staging copies kept alive for the asynchronous uploads
 	std::vector<int> host_tab_;
