@@ -37,6 +37,7 @@ typedef enum {
 #define RN_PT_DEVICE_POINTERS 1u /* arrays are device pointers; asynchronous on `stream` */
 #define RN_PT_ORDER_NEAREST 2u   /* closest hit: nearest-child-first traversal (default: reference order) */
 #define RN_PT_WIDTH2 4u          /* ray queries: traverse the 2-wide reference tree (default: its 4-wide collapse) */
+#define RN_PT_WAVEFRONT_STATIC 8u /* wavefront: one ray per lane in the traversal stages (default: lanes refetch) */
 
 /* Physical-mode materials. */
 #define RN_PT_LAMBERT 0

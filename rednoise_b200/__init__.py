@@ -334,11 +334,12 @@ class Scene:
         return (canvas, mean) if want_mean else canvas
 
     def render_physical(self, camera: "Camera", settings: "Settings", nearest_first: bool = False,
-                        out: Optional[np.ndarray] = None) -> np.ndarray:
+                        out: Optional[np.ndarray] = None, wavefront_static: bool = False) -> np.ndarray:
         """Physical-mode render: per-pixel mean radiance as (height, width, 3) float32."""
         self._check_open()
         rgb = out if out is not None else np.empty((camera.height, camera.width, 3), np.float32)
-        flags = _native.RN_PT_ORDER_NEAREST if nearest_first else 0
+        flags = (_native.RN_PT_ORDER_NEAREST if nearest_first else 0) | (
+            _native.RN_PT_WAVEFRONT_STATIC if wavefront_static else 0)
         _native.check(_native.load().rn_pt_render(self._handle, ctypes.byref(camera), ctypes.byref(settings), flags,
                                                   None, _ptr(rgb)), "rn_pt_render")
         return rgb

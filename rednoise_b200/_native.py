@@ -16,6 +16,7 @@ RN_OK = 0
 RN_PT_DEVICE_POINTERS = 1
 RN_PT_ORDER_NEAREST = 2
 RN_PT_WIDTH2 = 4
+RN_PT_WAVEFRONT_STATIC = 8
 
 STATUS_NAMES = {
     0: "RN_OK",

@@ -190,17 +190,18 @@ rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc,
 
 // Run the integrator the settings ask for; RN_PT_AUTO uses (and on first use
 // measures) the scene's tuned choice for this image size.
-rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, const PhysScene &ps, const PhysCamera &pc,
-                         const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
+rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, unsigned flags, const PhysScene &ps,
+                         const PhysCamera &pc, const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
 	auto it = s->tuned.find(tune_key(pc, pst));
 	if (st->integrator == RN_PT_MEGAKERNEL)
 		return run_fixed(s, RN_PT_MEGAKERNEL, 0, 0, ps, pc, pst, d_accum, cs);
 	if (st->integrator == RN_PT_WAVEFRONT) {
 		// An explicit wavefront render keeps the tuned queue capacity when there is one.
+		const int dyn = (flags & RN_PT_WAVEFRONT_STATIC) ? 0 : 1;
 		if (it != s->tuned.end() && std::get<0>(it->second) == RN_PT_WAVEFRONT)
-			return run_fixed(s, RN_PT_WAVEFRONT, std::get<1>(it->second), std::get<2>(it->second), ps, pc, pst,
-			                 d_accum, cs);
-		return run_fixed(s, RN_PT_WAVEFRONT, 0, 1, ps, pc, pst, d_accum, cs);
+			return run_fixed(s, RN_PT_WAVEFRONT, std::get<1>(it->second), dyn ? std::get<2>(it->second) : 0, ps, pc,
+			                 pst, d_accum, cs);
+		return run_fixed(s, RN_PT_WAVEFRONT, 0, dyn, ps, pc, pst, d_accum, cs);
 	}
 	if (it == s->tuned.end()) {
 		rn_pt_tuning t{};
@@ -244,12 +245,12 @@ rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, c
 	cudaStream_t cs = pick_stream(scene, stream);
 	const size_t bytes = static_cast<size_t>(camera->width) * camera->height * 3 * sizeof(float);
 	if (flags & RN_PT_DEVICE_POINTERS)
-		return run_integrator(scene, settings, ps, pc, pst, accum, cs);
+		return run_integrator(scene, settings, flags, ps, pc, pst, accum, cs);
 	std::lock_guard<std::mutex> lock(scene->scratch_mu);
 	RNB_CUDA(scene->scratch.ensure(bytes));
 	float *d = scene->scratch.as<float>();
 	RNB_CUDA(cudaMemcpyAsync(d, accum, bytes, cudaMemcpyHostToDevice, cs));
-	r = run_integrator(scene, settings, ps, pc, pst, d, cs);
+	r = run_integrator(scene, settings, flags, ps, pc, pst, d, cs);
 	if (r != RN_OK)
 		return r;
 	RNB_CUDA(cudaMemcpyAsync(accum, d, bytes, cudaMemcpyDeviceToHost, cs));
@@ -322,7 +323,7 @@ rn_status rn_pt_render(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_
 		acc = scene->scratch.as<float>();
 	}
 	RNB_CUDA(cudaMemsetAsync(acc, 0, bytes, cs));
-	r = run_integrator(scene, settings, ps, pc, pst, acc, cs);
+	r = run_integrator(scene, settings, flags, ps, pc, pst, acc, cs);
 	if (r != RN_OK)
 		return r;
 	if (dev) {

@@ -139,6 +139,20 @@ def test_wavefront_equals_megakernel(nearest):
     assert not np.array_equal(a, a2)
 
 
+def test_wavefront_static_and_refetch_agree():
+    """One ray per lane vs lanes refetching rays: same hits, same image."""
+    sc = scenes.icosphere_scene(level=3)
+    s = make_scene(sc)
+    c = cam(64, 48)
+    camera = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], 64, 48)
+    st = rn.Settings.make(spp=8, max_depth=8, rr_depth=3, seed=4, integrator=2)
+    a = s.render_physical(camera, st)
+    b = s.render_physical(camera, st, wavefront_static=True)
+    m = s.render_physical(camera, rn.Settings.make(spp=8, max_depth=8, rr_depth=3, seed=4, integrator=1))
+    crn_agree(a, b, rel_l1=1e-5, pix_frac=1e-3)
+    crn_agree(a, m, rel_l1=1e-5, pix_frac=1e-3)
+
+
 def test_wavefront_matches_oracle_crn(box):
     s = make_scene(box)
     c = cam(48, 36)
