@@ -57,6 +57,24 @@ def dist_env():
         os.environ.get("WORLD_SIZE", "1"))
 
 
+def shard_sample_offset(step: int, rank: int, world: int, spp: int) -> int:
+    """First sample index of this rank's frame at this step: ranks and steps take
+    consecutive, disjoint blocks of spp sample indices, so the ranks' frames sum to
+    one render of world * spp samples (weak scaling, no data-path exchange)."""
+    return (step * world + rank) * spp
+
+
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Element-wise maximum of per-rank timings (the slowest rank sets the job time)."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 # ---- clocks sampled during the timed region ------------------------------------------
 
 class ClockSampler:
@@ -235,7 +253,7 @@ def run_ours(args):
         k = step_counter[0]
         step_counter[0] += 1
         return rn.Settings.make(spp=spp, max_depth=args.depth, rr_depth=args.rr, integrator=integ, seed=1,
-                                sample_offset=(k * world + rank) * spp)
+                                sample_offset=shard_sample_offset(k, rank, world, spp))
 
     def render(st):
         _native.check(lib.rn_pt_render(scene.handle, ctypes.byref(cam), ctypes.byref(st), flags, sptr,
@@ -279,10 +297,7 @@ def run_ours(args):
         clk = clocks.stop()
     total_ms = t_start.elapsed_time(t_end)
     render_ms = [a.elapsed_time(b) for a, b in ev]
-    if dist:
-        t = torch.tensor([total_ms, max(render_ms)], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, max_render = float(t[0]), float(t[1])
+    total_ms = max_over_ranks([total_ms], dist, "cuda")[0]
     ms_per_step = total_ms / args.steps
     samples_per_step = W * H * spp
     value = world * samples_per_step / (ms_per_step / 1e3)
@@ -325,10 +340,7 @@ def run_ours(args):
         _native.check(lib.rn_pt_render(scene.handle, ctypes.byref(cam), ctypes.byref(st), hflags, None,
                                        ctypes.c_void_p(host.data_ptr())), "rn_pt_render (host)")
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t[0])
+    e2e_s = max_over_ranks([e2e_s], dist, "cuda")[0]
     e2e_value = world * samples_per_step / e2e_s
 
     # RMSE of one frame against the FP64 reference on its pixel subset (when available).
