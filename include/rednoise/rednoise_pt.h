@@ -190,6 +190,25 @@ rn_status rn_pt_render(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_
 rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
                                   unsigned flags, void *stream, float *accum);
 
+/* Maximum image size of rn_pt_render_static, in pixels (512 x 512). */
+#define RN_PT_STATIC_MAX_PIXELS 262144
+
+/* rn_pt_render without memory allocation, for callers that may not allocate
+ * while they render (a host that owns a fixed memory budget, a framework whose
+ * allocator must not be bypassed, a real-time loop). No counterpart in the
+ * reference, which renders on the CPU into its own buffers. Runs the megakernel
+ * (settings->integrator is ignored) with its per-pixel sums and work counter in
+ * a fixed array inside the library (RN_PT_STATIC_MAX_PIXELS * 12 + 256 bytes on
+ * each GPU) and writes the mean radiance to rgb, a DEVICE pointer of
+ * width*height*3 floats, asynchronously on stream (NULL: the scene's stream).
+ * The scene must be prepared (rn_pt_scene_prepare) and its device current.
+ * Larger images return RN_ERR_CAPACITY. The first call on a device looks up the
+ * array's address; make it before any stream capture. All calls share the array:
+ * calls whose GPU work overlaps race and must be serialised by the caller. A
+ * traversal error is reported by the scene's next synchronising call. */
+rn_status rn_pt_render_static(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
+                              unsigned flags, void *stream, float *rgb);
+
 /* ---- autotuning ---- */
 
 /* Result of rn_pt_autotune: the chosen integrator and samples per wave (the

@@ -17,6 +17,7 @@ RN_PT_DEVICE_POINTERS = 1
 RN_PT_ORDER_NEAREST = 2
 RN_PT_WIDTH2 = 4
 RN_PT_WAVEFRONT_STATIC = 8
+RN_PT_STATIC_MAX_PIXELS = 512 * 512
 
 STATUS_NAMES = {
     0: "RN_OK",
@@ -225,6 +226,8 @@ SIGNATURES = {
     "rn_pt_render": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint, vp, vp]),
     "rn_pt_render_accumulate": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                                vp, vp]),
+    "rn_pt_render_static": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint, vp,
+                                           vp]),
     "rn_pt_count_traversal": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), vp]),
     "rn_pt_autotune": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                       ctypes.POINTER(Tuning)]),
