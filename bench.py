@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = 1.31M triangles)")
     p.add_argument("--integrator", default="auto", choices=["auto", "megakernel", "wavefront"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-grad", action="store_true", help="skip the gradient-vs-primal timing")
     return p.parse_args()
 
 
@@ -168,6 +169,84 @@ def cpu_baseline(sc, target_s=12.0) -> dict:
             "sample": f"reference renderPathTraced (oracle/_ref, OpenMP, reference semantics: depth 4, default light)"
                       f" on the same 1.31M-triangle geometry and camera, {steps} x {w}x{h} frames at 1 spp"
                       f" ({samples} samples, {total:.1f} s, BVH rebuilt per call as the reference does)"}
+
+
+def cpu_physical_baseline(sc, cam, args, target_s=8.0) -> dict:
+    """The restated FP32 physical integrator (the oracle: same estimator, materials and
+    emitter sampling as the GPU) on all host cores, over a seeded pixel subset."""
+    import oracle
+
+    orc = oracle.OrcPhysScene(sc)
+    rng = np.random.default_rng(7)
+    n_pix = cam["width"] * cam["height"]
+    npx = 2048
+    while True:
+        px = rng.choice(n_pix, npx, replace=False).astype(np.int32)
+        t0 = time.perf_counter()
+        orc.render_sums(cam, 4, args.depth, args.rr, seed=1, pixels=px)
+        dt = time.perf_counter() - t0
+        if dt > target_s / 3 or npx >= n_pix // 4:
+            break
+        npx = min(n_pix // 4, int(npx * max(2.0, target_s / 3 / max(dt, 1e-3))))
+    return {"value": npx * 4 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"oracle FP32 physical integrator (OpenMP), {npx} seeded pixels of the "
+                      f"{cam['width']}x{cam['height']} frame at 4 spp, depth {args.depth}, RR from {args.rr} "
+                      f"({dt:.1f} s)"}
+
+
+def gradient_timing(scene, lib, stream, sptr, l2, size=512, spp=32, depth=6) -> dict:
+    """One albedo/emission gradient by the path-replay adjoint against one primal render:
+    the same 1.31M-triangle scene at 512x512, 32 spp primal + 32 spp adjoint, depth 6,
+    L2 loss against a render with another seed."""
+    import torch
+
+    import rednoise_b200 as rn
+    from rednoise_b200 import _native, scenes
+
+    c = scenes.camera(size, size)
+    cam = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], size, size)
+    flags = _native.RN_PT_DEVICE_POINTERS
+    npx = size * size * 3
+    img = torch.empty(npx, device="cuda")
+    target = torch.empty(npx, device="cuda")
+    n = scene.triangle_count
+    g_alb = torch.empty(n * 3, device="cuda")
+    g_em = torch.empty(n * 3, device="cuda")
+
+    def primal(out, seed):
+        st = rn.Settings.make(spp=spp, max_depth=depth, rr_depth=depth, seed=seed)
+        _native.check(lib.rn_pt_render(scene.handle, ctypes.byref(cam), ctypes.byref(st), flags, sptr,
+                                       ctypes.c_void_p(out.data_ptr())), "rn_pt_render")
+
+    with torch.cuda.stream(stream):
+        primal(target, 99)
+        primal(img, 1)  # first call at this shape: autotune + graph capture
+        d_img = (2.0 / npx) * (img - target)
+        ptrs = (ctypes.c_void_p * 1)(d_img.data_ptr())
+        st = rn.Settings.make(spp=spp, max_depth=depth, rr_depth=depth, seed=1)
+
+        def adjoint():
+            _native.check(lib.rn_pt_backward(scene.handle, 1, ctypes.byref(cam), ctypes.byref(st), ptrs, flags,
+                                             sptr, ctypes.c_void_p(g_alb.data_ptr()),
+                                             ctypes.c_void_p(g_em.data_ptr())), "rn_pt_backward")
+
+        adjoint()
+        torch.cuda.synchronize()
+        tp, ta = [], []
+        for _ in range(3):
+            for fn, acc in ((lambda: primal(img, 1), tp), (adjoint, ta)):
+                l2.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                acc.append(e0.elapsed_time(e1))
+    p_ms, a_ms = float(np.median(tp)), float(np.median(ta))
+    return {"workload": f"{size}x{size}, {spp} spp primal + {spp} spp adjoint, depth {depth}, "
+                        f"d loss / d albedo ({n} x 3) and emission",
+            "primal_ms": p_ms, "adjoint_ms": a_ms, "adjoint_over_primal": a_ms / p_ms,
+            "grad_nonzero": int((g_alb != 0).sum().item())}
 
 
 def run_reference_arm(args):
@@ -307,13 +386,29 @@ def run_ours(args):
 
     # The two integrators side by side on the same frame (same estimator, same samples):
     # the plain megakernel and the wavefront (SoA queues, CUDA-graph frame).
+    ref_path = os.path.join(ROOT, "tests", "golden", "fp64_ref.npz")
+    fp64 = None
+    if os.path.isfile(ref_path) and (W, H, args.depth, args.rr) == (1920, 1080, 8, 3) and args.level == 8:
+        fp64 = np.load(ref_path)
+
+    def rmse_of(flat):
+        if fp64 is None:
+            return None
+        img = np.asarray(flat).reshape(-1, 3)[fp64["c2_pixels"]].astype(np.float64)
+        mref = fp64["c2_mean"]
+        return float(np.sqrt(((img - mref) ** 2).mean()) / max(np.sqrt((mref ** 2).mean()), 1e-30))
+
     compare = {}
+    rmse_by = {}
+    same = settings()  # every integrator renders these same samples
     with torch.cuda.stream(stream):
         for name, code, extra in (("megakernel", 1, 0), ("wavefront", 2, 0),
-                                  ("wavefront_static", 2, _native.RN_PT_WAVEFRONT_STATIC)):
+                                  ("wavefront_static", 2, _native.RN_PT_WAVEFRONT_STATIC),
+                                  ("wavefront_binned", 2, _native.RN_PT_RAY_SORT),
+                                  ("wavefront_unbinned", 2, _native.RN_PT_NO_RAY_SORT)):
             def one():
-                st = settings()
-                st.integrator = code
+                st = rn.Settings.make(spp=spp, max_depth=args.depth, rr_depth=args.rr, integrator=code, seed=1,
+                                      sample_offset=same.sample_offset)
                 _native.check(lib.rn_pt_render(scene.handle, ctypes.byref(cam), ctypes.byref(st), flags | extra,
                                                sptr, ctypes.c_void_p(out.data_ptr())), "rn_pt_render")
             l2.zero_()
@@ -328,10 +423,13 @@ def run_ours(args):
                 torch.cuda.synchronize()
                 ts.append(e0.elapsed_time(e1))
             compare[name] = samples_per_step / (min(ts) / 1e3)
+            if fp64 is not None:
+                rmse_by[name] = rmse_of(out.cpu().numpy())
     compare["wavefront_over_megakernel"] = compare["wavefront"] / compare["megakernel"]
     compare["auto_choice"] = {1: "megakernel", 2: "wavefront"}.get(tuned["integrator"], "?")
     compare["auto_samples_per_wave"] = tuned["samples_per_wave"]
     compare["auto_ray_fetch"] = "per-lane refetch" if tuned["dynamic_fetch"] else "one ray per lane"
+    compare["auto_ray_binning"] = bool(tuned["ray_sort"])
 
     # End to end through the C ABI with host buffers: pinned host output, D2H inside the timed region.
     host = torch.empty(H * W * 3, dtype=torch.float32, pin_memory=True)
@@ -350,14 +448,18 @@ def run_ours(args):
     e2e_value = world * samples_per_step / e2e_s
 
     # RMSE of one frame against the FP64 reference on its pixel subset (when available).
-    rmse = None
-    ref_path = os.path.join(ROOT, "tests", "golden", "fp64_ref.npz")
-    if os.path.isfile(ref_path) and (W, H, args.depth, args.rr) == (1920, 1080, 8, 3) and args.level == 8:
-        ref = np.load(ref_path)
-        px = ref["c2_pixels"]
-        img = host.numpy().reshape(-1, 3)[px].astype(np.float64)
-        mref = ref["c2_mean"]
-        rmse = float(np.sqrt(((img - mref) ** 2).mean()) / max(np.sqrt((mref ** 2).mean()), 1e-30))
+    rmse = rmse_of(host.numpy())
+    at_rmse = None
+    if rmse_by:
+        # Same samples, same estimator: both integrators reach the same RMSE at 64 spp, so
+        # their times to that RMSE are their frame times.
+        at_rmse = {"relative_rmse_64spp": rmse_by, "frame_ms": {k: samples_per_step / compare[k] * 1e3
+                                                                for k in rmse_by},
+                   "wavefront_speedup_at_equal_rmse": compare["wavefront"] / compare["megakernel"]}
+
+    grad = None
+    if not args.no_grad:
+        grad = gradient_timing(scene, lib, stream, sptr, l2)
 
     peak, peak_kind = measured_peaks()
     kernel_ms = float(np.mean(render_ms))
@@ -387,11 +489,15 @@ def run_ours(args):
                               "time (ncu launch list); traffic scaled from a 480x270 capture"},
         "clocks": clk,
         "rmse_vs_fp64_64spp": rmse,
+        "at_equal_rmse": at_rmse,
+        "path_vertices_per_s": value * counts["closest"] / counts["samples"],
+        "gradient": grad,
         "integrators_samples_per_s": compare,
         "scene_build_ms": info["build_ms"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sc)
+        line["cpu_physical_fp32"] = cpu_physical_baseline(sc, c, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -38,6 +38,8 @@ typedef enum {
 #define RN_PT_ORDER_NEAREST 2u   /* closest hit: nearest-child-first traversal (default: reference order) */
 #define RN_PT_WIDTH2 4u          /* ray queries: traverse the 2-wide reference tree (default: its 4-wide collapse) */
 #define RN_PT_WAVEFRONT_STATIC 8u /* wavefront: one ray per lane in the traversal stages (default: lanes refetch) */
+#define RN_PT_RAY_SORT 16u        /* wavefront: bin each bounce's rays by origin cell and direction before tracing */
+#define RN_PT_NO_RAY_SORT 32u     /* wavefront: never bin (default without either flag: the tuned choice) */
 
 /* Physical-mode materials. */
 #define RN_PT_LAMBERT 0
@@ -220,6 +222,7 @@ typedef struct {
 	double megakernel_sps; /* samples per second of the megakernel */
 	double wavefront_sps;  /* samples per second of the best wavefront configuration */
 	int dynamic_fetch;     /* wavefront traversal stages hand new rays to lanes whose ray finished */
+	int ray_sort;          /* wavefront bins each bounce's rays by origin cell and direction */
 } rn_pt_tuning;
 
 /* Time short renders of this scene/camera/settings (a few samples per pixel)

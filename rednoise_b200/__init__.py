@@ -50,6 +50,12 @@ class RenderMode(IntEnum):
         raise TypeError(f"render mode must be RenderMode, int or str, not {type(value).__name__}")
 
 
+def _sort_flag(ray_sort: Optional[bool]) -> int:
+    if ray_sort is None:
+        return 0
+    return _native.RN_PT_RAY_SORT if ray_sort else _native.RN_PT_NO_RAY_SORT
+
+
 def _ptr(a: Optional[np.ndarray]):
     return None if a is None else ctypes.c_void_p(a.ctypes.data)
 
@@ -334,12 +340,14 @@ class Scene:
         return (canvas, mean) if want_mean else canvas
 
     def render_physical(self, camera: "Camera", settings: "Settings", nearest_first: bool = False,
-                        out: Optional[np.ndarray] = None, wavefront_static: bool = False) -> np.ndarray:
-        """Physical-mode render: per-pixel mean radiance as (height, width, 3) float32."""
+                        out: Optional[np.ndarray] = None, wavefront_static: bool = False,
+                        ray_sort: Optional[bool] = None) -> np.ndarray:
+        """Physical-mode render: per-pixel mean radiance as (height, width, 3) float32.
+        ``ray_sort`` forces the wavefront's ray binning on or off (None: the tuned choice)."""
         self._check_open()
         rgb = out if out is not None else np.empty((camera.height, camera.width, 3), np.float32)
         flags = (_native.RN_PT_ORDER_NEAREST if nearest_first else 0) | (
-            _native.RN_PT_WAVEFRONT_STATIC if wavefront_static else 0)
+            _native.RN_PT_WAVEFRONT_STATIC if wavefront_static else 0) | _sort_flag(ray_sort)
         _native.check(_native.load().rn_pt_render(self._handle, ctypes.byref(camera), ctypes.byref(settings), flags,
                                                   None, _ptr(rgb)), "rn_pt_render")
         return rgb
@@ -449,7 +457,8 @@ class Batch:
     frame is captured once as a CUDA graph and replayed on every ``render``.
     """
 
-    def __init__(self, jobs, integrator: int = _native.RN_PT_AUTO, nearest_first: bool = False):
+    def __init__(self, jobs, integrator: int = _native.RN_PT_AUTO, nearest_first: bool = False,
+                 ray_sort: Optional[bool] = None):
         self._scenes = [j[0] for j in jobs]  # keep the scenes alive
         arr = (_native.Job * len(jobs))()
         for i, (scene, camera, settings) in enumerate(jobs):
@@ -458,7 +467,7 @@ class Batch:
             arr[i].settings = settings
         self._shapes = [(c.height, c.width, 3) for _, c, _ in jobs]
         out = ctypes.c_void_p()
-        flags = _native.RN_PT_ORDER_NEAREST if nearest_first else 0
+        flags = (_native.RN_PT_ORDER_NEAREST if nearest_first else 0) | _sort_flag(ray_sort)
         _native.check(_native.load().rn_pt_batch_create(arr, len(jobs), integrator, flags, ctypes.byref(out)),
                       "rn_pt_batch_create")
         self._handle = out.value

@@ -17,6 +17,8 @@ RN_PT_DEVICE_POINTERS = 1
 RN_PT_ORDER_NEAREST = 2
 RN_PT_WIDTH2 = 4
 RN_PT_WAVEFRONT_STATIC = 8
+RN_PT_RAY_SORT = 16
+RN_PT_NO_RAY_SORT = 32
 RN_PT_STATIC_MAX_PIXELS = 512 * 512
 
 STATUS_NAMES = {
@@ -194,6 +196,7 @@ class Tuning(ctypes.Structure):
         ("megakernel_sps", ctypes.c_double),
         ("wavefront_sps", ctypes.c_double),
         ("dynamic_fetch", ctypes.c_int),
+        ("ray_sort", ctypes.c_int),
     ]
 
 

@@ -14,14 +14,15 @@ struct AdjView {
 	PhysSettings st;
 	const float *dimg;
 	int n_pix;
-	int pix_base; // first global pixel index of the view
+	unsigned item_base; // first (pixel, sample) work item of the view: sum of n_pix * spp before it
 };
 
 // Scenes up to this many triangles accumulate their gradients in shared memory.
 constexpr int kAdjointSharedTris = 4096;
 
-cudaError_t launch_adjoint(const PhysScene &sc, const AdjView *d_views, int n_views, int total_pix, float *d_alb,
-                           float *d_em, int n_tris, int *status, cudaStream_t st);
+// counter: one device word, the work counter (zeroed on the stream here).
+cudaError_t launch_adjoint(const PhysScene &sc, const AdjView *d_views, int n_views, unsigned total_items,
+                           float *d_alb, float *d_em, int n_tris, unsigned *counter, int *status, cudaStream_t st);
 
 // Overwrite per-triangle albedo and / or emitted radiance of the shading records.
 cudaError_t launch_set_materials(float4 *shade, int n, const float *albedo, const float *emission, cudaStream_t st);

@@ -19,6 +19,7 @@ struct rn_pt_batch {
 	int order = 0;
 	int max_depth = 1;
 	int spw = 1;
+	int forced_sort = -1; // RN_PT_RAY_SORT / RN_PT_NO_RAY_SORT at creation: 1 / 0; else tuned
 	long total_floats = 0;
 	~rn_pt_batch() {
 		if (stream)
@@ -58,12 +59,18 @@ rn_status batch_enqueue(rn_pt_batch *b, unsigned sample_offset, cudaStream_t cs)
 // Time one frame of each integrator at the batch's own sizes and keep the faster.
 rn_status autotune_batch(rn_pt_batch *b) {
 	float best = 0.0f;
-	int pick = RN_PT_WAVEFRONT;
+	int pick = RN_PT_WAVEFRONT, pick_sort = 0;
 	cudaEvent_t e0, e1;
 	RNB_CUDA(cudaEventCreate(&e0));
 	RNB_CUDA(cudaEventCreate(&e1));
-	for (int integ : {RN_PT_MEGAKERNEL, RN_PT_WAVEFRONT}) {
+	// megakernel per job; wavefront without and with ray binning
+	for (int cand = 0; cand < 3; cand++) {
+		const int integ = cand == 0 ? RN_PT_MEGAKERNEL : RN_PT_WAVEFRONT;
+		const int sort = cand == 2 ? 1 : 0;
+		if (integ == RN_PT_WAVEFRONT && b->forced_sort >= 0 && sort != b->forced_sort)
+			continue;
 		b->integrator = integ;
+		b->wf.set_sort(sort);
 		rn_status r = batch_enqueue(b, 0x40000000u, b->stream); // warm-up (and graph capture)
 		if (r != RN_OK)
 			return r;
@@ -78,11 +85,13 @@ rn_status autotune_batch(rn_pt_batch *b) {
 		if (best == 0.0f || ms < best) {
 			best = ms;
 			pick = integ;
+			pick_sort = sort;
 		}
 	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	b->integrator = pick;
+	b->wf.set_sort(pick_sort);
 	return RN_OK;
 }
 
@@ -105,6 +114,9 @@ rn_status rn_pt_batch_create(const rn_pt_job *jobs, int n, int integrator, unsig
 		return RN_ERR_OUT_OF_MEMORY;
 	b->jobs.assign(jobs, jobs + n);
 	b->order = (flags & RN_PT_ORDER_NEAREST) ? kOrderNearest : kOrderReference;
+	b->forced_sort = (flags & RN_PT_RAY_SORT) ? 1 : ((flags & RN_PT_NO_RAY_SORT) ? 0 : -1);
+	if (b->forced_sort >= 0)
+		b->wf.set_sort(b->forced_sort);
 	long total = 0;
 	int max_spp = 1;
 	long max_pix = 1;

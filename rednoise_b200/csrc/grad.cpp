@@ -51,8 +51,9 @@ rn_status rn_pt_backward(rn_scene *scene, int n_views, const rn_pt_camera *camer
 		return RN_ERR_INVALID_ARGUMENT;
 	}
 	std::vector<AdjView> views(static_cast<size_t>(n_views));
+	std::vector<long> pix_base(static_cast<size_t>(n_views));
 	PhysScene ps{};
-	long total = 0;
+	long total = 0, items = 0;
 	for (int v = 0; v < n_views; v++) {
 		PhysCamera pc;
 		PhysSettings pst;
@@ -66,12 +67,14 @@ rn_status rn_pt_backward(rn_scene *scene, int n_views, const rn_pt_camera *camer
 		views[v].cam = pc;
 		views[v].st = pst;
 		views[v].n_pix = pc.width * pc.height;
-		views[v].pix_base = static_cast<int>(total);
+		views[v].item_base = static_cast<unsigned>(items);
+		pix_base[v] = total;
 		total += views[v].n_pix;
-	}
-	if (total > (1L << 30)) {
-		set_last_error("rn_pt_backward: more than 2^30 pixels");
-		return RN_ERR_CAPACITY;
+		items += static_cast<long>(views[v].n_pix) * (pst.spp > 0 ? pst.spp : 0);
+		if (total > (1L << 30) || items > (1L << 31)) {
+			set_last_error("rn_pt_backward: more than 2^30 pixels or 2^31 (pixel, sample) pairs");
+			return RN_ERR_CAPACITY;
+		}
 	}
 	const int n = static_cast<int>(scene->tris.size());
 	const bool dev = (flags & RN_PT_DEVICE_POINTERS) != 0;
@@ -95,7 +98,7 @@ rn_status rn_pt_backward(rn_scene *scene, int n_views, const rn_pt_camera *camer
 		if (dev) {
 			views[v].dimg = d_images[v];
 		} else {
-			float *dst = imgs + 3 * static_cast<size_t>(views[v].pix_base);
+			float *dst = imgs + 3 * static_cast<size_t>(pix_base[v]);
 			RNB_CUDA(cudaMemcpyAsync(dst, d_images[v], static_cast<size_t>(views[v].n_pix) * 12,
 			                         cudaMemcpyHostToDevice, cs));
 			views[v].dimg = dst;
@@ -104,8 +107,9 @@ rn_status rn_pt_backward(rn_scene *scene, int n_views, const rn_pt_camera *camer
 	RNB_CUDA(cudaMemcpyAsync(d_views, views.data(), views.size() * sizeof(AdjView), cudaMemcpyHostToDevice, cs));
 	RNB_CUDA(cudaMemsetAsync(g_alb, 0, gbytes, cs));
 	RNB_CUDA(cudaMemsetAsync(g_em, 0, gbytes, cs));
-	RNB_CUDA(launch_adjoint(ps, d_views, n_views, static_cast<int>(total), g_alb, g_em, n, scene->d_status.as<int>(),
-	                        cs));
+	RNB_CUDA(scene->d_adj_counter.ensure(256));
+	RNB_CUDA(launch_adjoint(ps, d_views, n_views, static_cast<unsigned>(items), g_alb, g_em, n,
+	                        scene->d_adj_counter.as<unsigned>(), scene->d_status.as<int>(), cs));
 	if (dev)
 		return RN_OK;
 	if (d_albedo)

@@ -91,9 +91,10 @@ using namespace rnb;
 namespace {
 
 // Run one integrator over accum (device, 3 floats per pixel). spw <= 0 picks the
-// default samples per wave; dyn selects the wavefront's per-lane ray replacement.
-rn_status run_fixed(rn_scene *s, int integrator, int spw, int dyn, const PhysScene &ps, const PhysCamera &pc,
-                    const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
+// default samples per wave; dyn selects the wavefront's per-lane ray replacement
+// and sort its binning of each bounce's rays.
+rn_status run_fixed(rn_scene *s, int integrator, int spw, int dyn, int sort, const PhysScene &ps,
+                    const PhysCamera &pc, const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
 	if (integrator == RN_PT_WAVEFRONT) {
 		if (pst.max_depth > kWfMaxDepth) {
 			set_last_error("render: the wavefront integrator supports max_depth <= 64");
@@ -110,6 +111,7 @@ rn_status run_fixed(rn_scene *s, int integrator, int spw, int dyn, const PhysSce
 		job.spp = pst.spp;
 		s->wf->set_frame_io(nullptr, 0, {});
 		s->wf->set_dynamic(dyn);
+		s->wf->set_sort(sort);
 		if (spw <= 0)
 			spw = default_samples_per_wave(job.n_pix, job.spp);
 		rn_status r = s->wf->configure({job}, pst.max_depth, pst.order, spw, cs);
@@ -127,8 +129,9 @@ std::tuple<int, int, int, int> tune_key(const PhysCamera &pc, const PhysSettings
 }
 
 // Measure the candidates on a few samples per pixel and remember the fastest:
-// the megakernel, and the wavefront at 1x..16x the default queue capacity with
-// and without per-lane ray replacement in its traversal stages.
+// the megakernel, and the wavefront at 1x..16x the default queue capacity, with
+// and without per-lane ray replacement in its traversal stages and with and
+// without binning each bounce's rays.
 rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc, const PhysSettings &pst,
                          rn_pt_tuning &out) {
 	PhysSettings probe = pst;
@@ -142,11 +145,11 @@ rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc,
 	RNB_CUDA(cudaEventCreate(&e0));
 	RNB_CUDA(cudaEventCreate(&e1));
 	const double samples = static_cast<double>(pc.width) * pc.height * probe.spp;
-	auto time_one = [&](int integ, int spw, int dyn, double &sps) -> rn_status {
+	auto time_one = [&](int integ, int spw, int dyn, int sort, double &sps) -> rn_status {
 		for (int rep = 0; rep < 2; rep++) { // the first run warms caches and captures graphs
 			RNB_CUDA(cudaMemsetAsync(acc, 0, bytes, cs));
 			RNB_CUDA(cudaEventRecord(e0, cs));
-			rn_status r = run_fixed(s, integ, spw, dyn, ps, pc, probe, acc, cs);
+			rn_status r = run_fixed(s, integ, spw, dyn, sort, ps, pc, probe, acc, cs);
 			if (r != RN_OK)
 				return r;
 			RNB_CUDA(cudaEventRecord(e1, cs));
@@ -157,34 +160,38 @@ rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc,
 		sps = ms > 0.0f ? samples / (ms * 1e-3) : 0.0;
 		return RN_OK;
 	};
-	rn_status r = time_one(RN_PT_MEGAKERNEL, 0, 0, out.megakernel_sps);
+	rn_status r = time_one(RN_PT_MEGAKERNEL, 0, 0, 0, out.megakernel_sps);
 	if (r != RN_OK)
 		return r;
 	out.wavefront_sps = 0.0;
 	out.samples_per_wave = 1;
 	out.dynamic_fetch = 1;
+	out.ray_sort = 0;
 	const int d = default_samples_per_wave(static_cast<long>(pc.width) * pc.height, probe.spp);
-	for (int dyn : {1, 0}) {
-		if (dyn && pst.order != kOrderReference)
-			continue;
-		for (int spw : {d, 2 * d, 4 * d, 8 * d, 16 * d}) {
-			if (spw > probe.spp)
-				break;
-			double sps = 0.0;
-			r = time_one(RN_PT_WAVEFRONT, spw, dyn, sps);
-			if (r != RN_OK)
-				return r;
-			if (sps > out.wavefront_sps) {
-				out.wavefront_sps = sps;
-				out.samples_per_wave = spw;
-				out.dynamic_fetch = dyn;
+	for (int sort : {0, 1}) {
+		for (int dyn : {1, 0}) {
+			if (dyn && pst.order != kOrderReference)
+				continue;
+			for (int spw : {d, 2 * d, 4 * d, 8 * d, 16 * d}) {
+				if (spw > probe.spp)
+					break;
+				double sps = 0.0;
+				r = time_one(RN_PT_WAVEFRONT, spw, dyn, sort, sps);
+				if (r != RN_OK)
+					return r;
+				if (sps > out.wavefront_sps) {
+					out.wavefront_sps = sps;
+					out.samples_per_wave = spw;
+					out.dynamic_fetch = dyn;
+					out.ray_sort = sort;
+				}
 			}
 		}
 	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	out.integrator = out.wavefront_sps > out.megakernel_sps ? RN_PT_WAVEFRONT : RN_PT_MEGAKERNEL;
-	s->tuned[tune_key(pc, pst)] = {out.integrator, out.samples_per_wave, out.dynamic_fetch};
+	s->tuned[tune_key(pc, pst)] = {out.integrator, out.samples_per_wave, out.dynamic_fetch, out.ray_sort};
 	return RN_OK;
 }
 
@@ -193,15 +200,19 @@ rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc,
 rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, unsigned flags, const PhysScene &ps,
                          const PhysCamera &pc, const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
 	auto it = s->tuned.find(tune_key(pc, pst));
+	// Ray binning: forced on or off by the flags, else the tuned choice.
+	auto pick_sort = [flags](int tuned) {
+		return (flags & RN_PT_RAY_SORT) ? 1 : ((flags & RN_PT_NO_RAY_SORT) ? 0 : tuned);
+	};
 	if (st->integrator == RN_PT_MEGAKERNEL)
-		return run_fixed(s, RN_PT_MEGAKERNEL, 0, 0, ps, pc, pst, d_accum, cs);
+		return run_fixed(s, RN_PT_MEGAKERNEL, 0, 0, 0, ps, pc, pst, d_accum, cs);
 	if (st->integrator == RN_PT_WAVEFRONT) {
-		// An explicit wavefront render keeps the tuned queue capacity when there is one.
+		// An explicit wavefront render keeps the tuned wavefront choices when there are some.
 		const int dyn = (flags & RN_PT_WAVEFRONT_STATIC) ? 0 : 1;
 		if (it != s->tuned.end() && std::get<0>(it->second) == RN_PT_WAVEFRONT)
-			return run_fixed(s, RN_PT_WAVEFRONT, std::get<1>(it->second), dyn ? std::get<2>(it->second) : 0, ps, pc,
-			                 pst, d_accum, cs);
-		return run_fixed(s, RN_PT_WAVEFRONT, 0, dyn, ps, pc, pst, d_accum, cs);
+			return run_fixed(s, RN_PT_WAVEFRONT, std::get<1>(it->second), dyn ? std::get<2>(it->second) : 0,
+			                 pick_sort(std::get<3>(it->second)), ps, pc, pst, d_accum, cs);
+		return run_fixed(s, RN_PT_WAVEFRONT, 0, dyn, pick_sort(0), ps, pc, pst, d_accum, cs);
 	}
 	if (it == s->tuned.end()) {
 		rn_pt_tuning t{};
@@ -210,8 +221,8 @@ rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, unsigned flags, 
 			return r;
 		it = s->tuned.find(tune_key(pc, pst));
 	}
-	const auto [integ, spw, dyn] = it->second;
-	return run_fixed(s, integ, spw, dyn, ps, pc, pst, d_accum, cs);
+	const auto [integ, spw, dyn, sort] = it->second;
+	return run_fixed(s, integ, spw, dyn, pick_sort(sort), ps, pc, pst, d_accum, cs);
 }
 
 rn_status finish_sync(rn_scene *s, cudaStream_t cs, const char *what) {

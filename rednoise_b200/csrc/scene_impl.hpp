@@ -42,11 +42,12 @@ struct rn_scene {
 	rnb::DevBuf d_counter;
 	rnb::DevBuf accum;
 	rnb::DevBuf adj; // view table and gradient buffers of device-pointer adjoint calls
+	rnb::DevBuf d_adj_counter; // work counter of the adjoint kernel
 	// Wavefront pools and the captured frame graph of single-scene renders.
 	std::unique_ptr<rnb::WfContext> wf;
 	// Autotuner choices per (width, height, max_depth, order):
 	// (integrator, samples per wave, per-lane ray replacement).
-	std::map<std::tuple<int, int, int, int>, std::tuple<int, int, int>> tuned;
+	std::map<std::tuple<int, int, int, int>, std::tuple<int, int, int, int>> tuned;
 	rnb::DevBuf tune_accum;
 
 	~rn_scene();

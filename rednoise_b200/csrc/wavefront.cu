@@ -60,9 +60,9 @@ __global__ void __launch_bounds__(256) k_wf_camera(const WfJob *__restrict__ job
 }
 
 template <int kOrder>
-__global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ jobs, WfPool pool, int k, int *status) {
+__global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ jobs, WfPool pool, int k,
+                                                   const int *__restrict__ q, int *status) {
 	const unsigned n = pool.counters[kCntRays + k];
-	const int *__restrict__ q = pool.queue[k & 1];
 	const int lane = threadIdx.x & 31;
 	int err = 0;
 	for (;;) {
@@ -88,9 +88,25 @@ __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ job
 		atomicOr(status, 1);
 }
 
-__global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k) {
+// Bin of a ray for the binning sort: its direction octant above a Morton code of
+// the cell (8 x 8 x 8 over the scene's bounding box) that holds its origin.
+__device__ __forceinline__ unsigned spread3(unsigned x) { return (x & 1u) | ((x & 2u) << 2) | ((x & 4u) << 4); }
+__device__ __forceinline__ unsigned cell8(float x, float lo, float hi) {
+	// fmaxf maps the NaN of a flat extent (0 * inf) to cell 0
+	return static_cast<unsigned>(fminf(fmaxf((x - lo) * __fdividef(8.0f, hi - lo), 0.0f), 7.0f));
+}
+__device__ __forceinline__ unsigned ray_bin(const SceneView &sv, const F3 &o, const F3 &d) {
+	const unsigned oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+	const unsigned m = spread3(cell8(o.x, sv.root_lo[0], sv.root_hi[0])) |
+	                   (spread3(cell8(o.y, sv.root_lo[1], sv.root_hi[1])) << 1) |
+	                   (spread3(cell8(o.z, sv.root_lo[2], sv.root_hi[2])) << 2);
+	return (oct << 9) | m;
+}
+static_assert(kBinBits == 12, "ray_bin makes 12-bit keys");
+
+__global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
+                                                  const int *__restrict__ q, int write_keys) {
 	const unsigned n = pool.counters[kCntRays + k];
-	const int *__restrict__ q = pool.queue[k & 1];
 	int *__restrict__ qn = pool.queue[(k + 1) & 1];
 	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
 		const int slot = q[i];
@@ -124,6 +140,8 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 		pool.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, L.w);
 		if (alive) {
 			qn[ni] = slot;
+			if (write_keys)
+				pool.keys[ni] = static_cast<uint16_t>(ray_bin(job.sc.sv, ps.o, ps.d));
 			pool.o[slot] = make_float4(ps.o.x, ps.o.y, ps.o.z, __int_as_float(ps.ignore));
 			pool.d[slot] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.prev_pdf);
 			pool.beta[slot] = make_float4(ps.beta.x, ps.beta.y, ps.beta.z, __int_as_float(ps.bounce));
@@ -167,10 +185,9 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 // queue lasts (closest hits for the extend stage, any hits for shadow records).
 template <bool kAny>
 __global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ jobs, WfPool pool, int k,
-                                                      int *status) {
+                                                      const int *__restrict__ q, int *status) {
 	const unsigned n = pool.counters[(kAny ? kCntShadow : kCntRays) + k];
 	unsigned *fetch = pool.counters + (kAny ? kCntFetchSh : kCntFetchExt) + k;
-	const int *__restrict__ q = pool.queue[k & 1];
 	const int lane = threadIdx.x & 31;
 	int err = 0;
 	TravState ts;
@@ -252,6 +269,85 @@ __global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ 
 		atomicOr(status, 1);
 }
 
+// Binning sort of the closest-hit queue of bounce k (counting sort on the keys
+// the shade stage wrote): histogram, exclusive scan, scatter. Blocks of 1024
+// threads; keys are masked to kBins so every shared-memory index is in range.
+__global__ void __launch_bounds__(1024) k_wf_bin_count(WfPool pool, int k) {
+	__shared__ unsigned h[kBins];
+	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
+		h[b] = 0;
+	__syncthreads();
+	const unsigned n = pool.counters[kCntRays + k];
+	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		atomicAdd(&h[pool.keys[i] & (kBins - 1)], 1u);
+	__syncthreads();
+	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
+		if (h[b])
+			atomicAdd(&pool.bins[b], h[b]);
+}
+
+// One block of kBins / 4 threads: bins[] counts -> exclusive offsets.
+__global__ void __launch_bounds__(kBins / 4) k_wf_bin_scan(WfPool pool) {
+	__shared__ unsigned warp_sum[kBins / 4 / 32];
+	const int t = threadIdx.x;
+	uint4 *b4 = reinterpret_cast<uint4 *>(pool.bins);
+	const uint4 v = b4[t];
+	const unsigned own = v.x + v.y + v.z + v.w;
+	unsigned x = own;
+	for (int o = 1; o < 32; o <<= 1) {
+		const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+		if ((t & 31) >= o)
+			x += y;
+	}
+	if ((t & 31) == 31)
+		warp_sum[t >> 5] = x;
+	__syncthreads();
+	if (t < 32) {
+		const unsigned w = warp_sum[t];
+		unsigned z = w;
+		for (int o = 1; o < 32; o <<= 1) {
+			const unsigned y = __shfl_up_sync(0xffffffffu, z, o);
+			if (t >= o)
+				z += y;
+		}
+		warp_sum[t] = z - w;
+	}
+	__syncthreads();
+	uint4 r;
+	r.x = warp_sum[t >> 5] + x - own;
+	r.y = r.x + v.x;
+	r.z = r.y + v.y;
+	r.w = r.z + v.z;
+	b4[t] = r;
+}
+static_assert(kBins / 4 == 1024, "k_wf_bin_scan runs one block of 1024 threads");
+
+// Each block takes a contiguous chunk of the queue, reserves its share of every
+// bin with one atomic per non-empty bin, then places its rays.
+__global__ void __launch_bounds__(1024) k_wf_bin_scatter(WfPool pool, int k) {
+	__shared__ unsigned h[kBins];
+	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
+		h[b] = 0;
+	__syncthreads();
+	const unsigned n = pool.counters[kCntRays + k];
+	const unsigned per = (n + gridDim.x - 1) / gridDim.x;
+	const unsigned c0 = min(n, blockIdx.x * per);
+	const unsigned c1 = min(n, c0 + per);
+	for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x)
+		atomicAdd(&h[pool.keys[i] & (kBins - 1)], 1u);
+	__syncthreads();
+	for (int b = threadIdx.x; b < kBins; b += blockDim.x) {
+		const unsigned c = h[b];
+		h[b] = c ? atomicAdd(&pool.bins[b], c) : 0u;
+	}
+	__syncthreads();
+	const int *__restrict__ q = pool.queue[k & 1];
+	for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+		const unsigned pos = atomicAdd(&h[pool.keys[i] & (kBins - 1)], 1u);
+		pool.sorted[pos] = q[i];
+	}
+}
+
 // Adds each pixel's samples of this wave to its sum, in sample order.
 __global__ void __launch_bounds__(256) k_wf_accumulate(const WfJob *__restrict__ jobs, WfPool pool, WfWave wave) {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < wave.n_pix; i += gridDim.x * blockDim.x) {
@@ -276,8 +372,7 @@ __global__ void __launch_bounds__(256) k_wf_accumulate(const WfJob *__restrict__
 } // namespace
 
 cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave &wave, int max_depth, int order,
-                           int dyn, int grid_ext, int grid_shade, int grid_sh, int grid_dyn, int *status,
-                           cudaStream_t st) {
+                           const WfLaunch &lc, int *status, cudaStream_t st) {
 	if (wave.n_slots <= 0)
 		return cudaSuccess;
 	cudaError_t e = cudaMemsetAsync(pool.counters, 0, kCntTotal * sizeof(unsigned), st);
@@ -285,19 +380,30 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 		return e;
 	const int gcam = (wave.n_slots + 255) / 256 < 148 * 8 ? (wave.n_slots + 255) / 256 : 148 * 8;
 	k_wf_camera<<<gcam, 256, 0, st>>>(d_jobs, pool, wave);
-	const bool use_dyn = dyn && order == kOrderReference;
+	const bool use_dyn = lc.dyn && order == kOrderReference;
+	const bool sort = lc.sort && pool.keys && pool.sorted && pool.bins;
 	for (int k = 0; k < max_depth; k++) {
+		const int *q = pool.queue[k & 1];
+		if (sort && k > 0) {
+			e = cudaMemsetAsync(pool.bins, 0, kBins * sizeof(unsigned), st);
+			if (e != cudaSuccess)
+				return e;
+			k_wf_bin_count<<<lc.grid_bin, 1024, 0, st>>>(pool, k);
+			k_wf_bin_scan<<<1, kBins / 4, 0, st>>>(pool);
+			k_wf_bin_scatter<<<lc.grid_bin, 1024, 0, st>>>(pool, k);
+			q = pool.sorted;
+		}
 		if (use_dyn)
-			k_wf_trace_dyn<false><<<grid_dyn, 128, 0, st>>>(d_jobs, pool, k, status);
+			k_wf_trace_dyn<false><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, q, status);
 		else if (order == kOrderNearest)
-			k_wf_extend<kOrderNearest><<<grid_ext, 128, 0, st>>>(d_jobs, pool, k, status);
+			k_wf_extend<kOrderNearest><<<lc.grid_ext, 128, 0, st>>>(d_jobs, pool, k, q, status);
 		else
-			k_wf_extend<kOrderReference><<<grid_ext, 128, 0, st>>>(d_jobs, pool, k, status);
-		k_wf_shade<<<grid_shade, 128, 0, st>>>(d_jobs, pool, k);
+			k_wf_extend<kOrderReference><<<lc.grid_ext, 128, 0, st>>>(d_jobs, pool, k, q, status);
+		k_wf_shade<<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, q, sort ? 1 : 0);
 		if (use_dyn)
-			k_wf_trace_dyn<true><<<grid_dyn, 128, 0, st>>>(d_jobs, pool, k, status);
+			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, status);
 		else
-			k_wf_shadow<<<grid_sh, 128, 0, st>>>(d_jobs, pool, k, status);
+			k_wf_shadow<<<lc.grid_sh, 128, 0, st>>>(d_jobs, pool, k, status);
 	}
 	const int gacc = (wave.n_pix + 255) / 256 < 148 * 8 ? (wave.n_pix + 255) / 256 : 148 * 8;
 	k_wf_accumulate<<<gacc, 256, 0, st>>>(d_jobs, pool, wave);
@@ -305,7 +411,7 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 }
 
 // Persistent grid sizes (blocks resident on all SMs).
-void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn) {
+void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn, int &grid_bin) {
 	int dev = 0, sms = 148;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -320,6 +426,7 @@ void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn) 
 	grid_sh = sms * (c > 0 ? c : 1);
 	const int d = d0 < d1 ? d0 : d1;
 	grid_dyn = sms * (d > 0 ? d : 1);
+	grid_bin = sms; // one 1024-thread block per SM keeps the bin atomics few
 }
 
 } // namespace rnb

@@ -49,8 +49,19 @@ struct WfPool {
 	// counters: [0, kWfMaxDepth] ray-queue lengths per bounce, [kWfMaxDepth+1 ...] shadow
 	// lengths per bounce, then per-bounce fetch counters of extend and shadow.
 	unsigned *counters;
+	// Ray binning (optional): the shade stage writes each continuation ray's bin
+	// (direction octant, coarse cell of its origin) to keys; before the next
+	// closest-hit stage a counting sort by bin rewrites the queue into sorted, so
+	// the lanes of a warp trace rays that start close together in similar
+	// directions and visit the same nodes.
+	uint16_t *keys;
+	int *sorted;
+	unsigned *bins; // kBins counters, then offsets
 	int capacity;
 };
+
+constexpr int kBinBits = 12;
+constexpr int kBins = 1 << kBinBits;
 
 constexpr int kCntRays = 0;
 constexpr int kCntShadow = kWfMaxDepth + 1;
@@ -73,9 +84,14 @@ struct WfWave {
 	int first_sample;   // sample index of k = 0, relative to each job's sample_offset
 };
 
-// dyn = 1: traversal stages use persistent warps that replace finished rays per lane.
+// Launch shapes and stage options of a wave.
+struct WfLaunch {
+	int grid_ext, grid_shade, grid_sh, grid_dyn, grid_bin;
+	int dyn;  // traversal stages use persistent warps that replace finished rays per lane
+	int sort; // closest-hit queues after the first bounce are binned by origin and direction
+};
+
 cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave &wave, int max_depth, int order,
-                           int dyn, int grid_ext, int grid_shade, int grid_sh, int grid_dyn, int *status,
-                           cudaStream_t st);
+                           const WfLaunch &lc, int *status, cudaStream_t st);
 
 } // namespace rnb

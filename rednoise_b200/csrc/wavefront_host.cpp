@@ -37,6 +37,9 @@ rn_status WfContext::ensure_pool(int capacity) {
 	RNB_CUDA(sh_d_.ensure(n * 16));
 	RNB_CUDA(sh_c_.ensure(n * 16));
 	RNB_CUDA(counters_.ensure(kCntTotal * sizeof(unsigned)));
+	RNB_CUDA(keys_.ensure(n * sizeof(uint16_t)));
+	RNB_CUDA(sorted_.ensure(n * 4));
+	RNB_CUDA(bins_.ensure(kBins * sizeof(unsigned)));
 	pool_.o = o_.as<float4>();
 	pool_.d = d_.as<float4>();
 	pool_.beta = beta_.as<float4>();
@@ -52,6 +55,9 @@ rn_status WfContext::ensure_pool(int capacity) {
 	pool_.sh_d = sh_d_.as<float4>();
 	pool_.sh_c = sh_c_.as<float4>();
 	pool_.counters = counters_.as<unsigned>();
+	pool_.keys = keys_.as<uint16_t>();
+	pool_.sorted = sorted_.as<int>();
+	pool_.bins = bins_.as<unsigned>();
 	pool_.capacity = capacity;
 	capacity_ = capacity;
 	return RN_OK;
@@ -118,7 +124,7 @@ rn_status WfContext::configure(const std::vector<WfJob> &jobs, int max_depth, in
 	if (r != RN_OK)
 		return r;
 	if (grid_ext_ == 0)
-		wf_grid_sizes(grid_ext_, grid_shade_, grid_sh_, grid_dyn_);
+		wf_grid_sizes(grid_ext_, grid_shade_, grid_sh_, grid_dyn_, grid_bin_);
 	host_jobs_ = jobs;
 	host_tab_ = tab;
 	RNB_CUDA(d_jobs_.ensure(jobs.size() * sizeof(WfJob)));
@@ -162,9 +168,9 @@ void WfContext::set_frame_io(float *zero_ptr, size_t zero_bytes, const std::vect
 rn_status WfContext::enqueue(int *status, cudaStream_t st) {
 	if (zero_ptr_ && zero_bytes_)
 		RNB_CUDA(cudaMemsetAsync(zero_ptr_, 0, zero_bytes_, st));
+	const WfLaunch lc{grid_ext_, grid_shade_, grid_sh_, grid_dyn_, grid_bin_, dyn_, sort_};
 	for (const WfWave &w : waves_)
-		RNB_CUDA(wf_launch_wave(d_jobs_.as<WfJob>(), pool_, w, max_depth_, order_, dyn_, grid_ext_, grid_shade_,
-		                        grid_sh_, grid_dyn_, status, st));
+		RNB_CUDA(wf_launch_wave(d_jobs_.as<WfJob>(), pool_, w, max_depth_, order_, lc, status, st));
 	for (const Resolve &r : resolves_)
 		RNB_CUDA(launch_resolve(r.accum, r.mean, r.n_floats, r.inv_spp, st));
 	return RN_OK;

@@ -11,7 +11,7 @@
 
 namespace rnb {
 
-void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn);
+void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn, int &grid_bin);
 
 // Samples per wave that keep about 2^20 paths in flight (at least 1, at most spp).
 inline int default_samples_per_wave(long n_pix, int spp) {
@@ -51,19 +51,28 @@ public:
 		dyn_ = dyn;
 	}
 	int dynamic() const { return dyn_; }
+	// Binning sort of the closest-hit queues after the first bounce (1) or none (0, default).
+	void set_sort(int sort) {
+		if (sort != sort_)
+			release_graph();
+		sort_ = sort;
+	}
+	int sort() const { return sort_; }
 
 private:
 	rn_status ensure_pool(int capacity);
 	void release_graph();
 
 	DevBuf o_, d_, beta_, L_, pixel_, sample_, hit_idx_, hit_t_, q0_, q1_, sh_o_, sh_d_, sh_c_, counters_;
+	DevBuf keys_, sorted_, bins_;
 	DevBuf d_jobs_, d_wave_tab_;
 	WfPool pool_{};
 	int capacity_ = 0;
 	int max_depth_ = 0;
 	int order_ = 0;
-	int grid_ext_ = 0, grid_shade_ = 0, grid_sh_ = 0, grid_dyn_ = 0;
+	int grid_ext_ = 0, grid_shade_ = 0, grid_sh_ = 0, grid_dyn_ = 0, grid_bin_ = 0;
 	int dyn_ = 1;
+	int sort_ = 0;
 	std::vector<WfWave> waves_;
 	std::vector<WfJob> host_jobs_; // staging copies kept alive for the asynchronous uploads
 	std::vector<int> host_tab_;

@@ -153,6 +153,37 @@ def test_wavefront_static_and_refetch_agree():
     crn_agree(a, m, rel_l1=1e-5, pix_frac=1e-3)
 
 
+@pytest.mark.parametrize("static", [False, True])
+def test_ray_binning_changes_no_path(static):
+    """Binning each bounce's rays only reorders the queue: the image is bit-identical
+    to the unbinned wavefront's and agrees with the megakernel's."""
+    sc = scenes.icosphere_scene(level=3)
+    s = make_scene(sc)
+    c = cam(64, 48)
+    camera = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], 64, 48)
+    st = rn.Settings.make(spp=8, max_depth=8, rr_depth=3, seed=6, integrator=2)
+    plain = s.render_physical(camera, st, wavefront_static=static, ray_sort=False)
+    binned = s.render_physical(camera, st, wavefront_static=static, ray_sort=True)
+    assert np.array_equal(plain.view(np.uint32), binned.view(np.uint32))
+    m = s.render_physical(camera, rn.Settings.make(spp=8, max_depth=8, rr_depth=3, seed=6, integrator=1))
+    crn_agree(binned, m, rel_l1=1e-5, pix_frac=1e-3)
+    # a second binned frame replays the captured graph
+    binned2 = s.render_physical(camera, st, wavefront_static=static, ray_sort=True)
+    assert np.array_equal(binned.view(np.uint32), binned2.view(np.uint32))
+
+
+def test_autotune_reports_ray_binning():
+    sc = scenes.icosphere_scene(level=3)
+    s = make_scene(sc)
+    c = cam(64, 48)
+    camera = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], 64, 48)
+    t = s.autotune(camera, rn.Settings.make(spp=8, max_depth=6, seed=1))
+    assert t["ray_sort"] in (0, 1) and t["integrator"] in (1, 2)
+    a = s.render_physical(camera, rn.Settings.make(spp=8, max_depth=6, seed=1))
+    b = s.render_physical(camera, rn.Settings.make(spp=8, max_depth=6, seed=1, integrator=1))
+    crn_agree(a, b, rel_l1=1e-5, pix_frac=1e-3)
+
+
 def test_wavefront_matches_oracle_crn(box):
     s = make_scene(box)
     c = cam(48, 36)
@@ -176,8 +207,8 @@ def test_batched_wavefront_equals_per_job_megakernel():
         settings = rn.Settings.make(spp=spp, max_depth=6, seed=7, integrator=1)
         jobs.append((s, camera, settings))
         refs.append(s.render_physical(camera, settings))
-    for integ in (2, 1, 0):
-        b = rn.Batch(jobs, integrator=integ)
+    for integ, binning in ((2, None), (2, True), (1, None), (0, None), (0, True)):
+        b = rn.Batch(jobs, integrator=integ, ray_sort=binning)
         assert b.integrator in (1, 2)
         outs = b.render()
         for o, r in zip(outs, refs):
