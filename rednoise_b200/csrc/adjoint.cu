@@ -127,7 +127,7 @@ __device__ __forceinline__ void adjoint_replay_tail(const PhysScene &sc, const P
 }
 
 template <bool kShared>
-__global__ void __launch_bounds__(128) k_adjoint(PhysScene sc, const AdjView *__restrict__ views, int n_views,
+__global__ void __launch_bounds__(128, 8) k_adjoint(PhysScene sc, const AdjView *__restrict__ views, int n_views,
                                                  unsigned total_items, float *__restrict__ d_alb,
                                                  float *__restrict__ d_em, int n_tris, unsigned *counter,
                                                  int *status) {

@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(256) k_wf_camera(const WfJob *__restrict__ job
 
 template <int kOrder>
 __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ jobs, WfPool pool, int k,
-                                                   const int *__restrict__ q, int *status) {
+                                                   const int *__restrict__ q, int only_job, int *status) {
 	const unsigned n = pool.counters[kCntRays + k];
 	const int lane = threadIdx.x & 31;
 	int err = 0;
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ job
 			const int slot = q[i];
 			const float4 o = pool.o[slot];
 			const float4 d = pool.d[slot];
-			const int j = __float_as_int(pool.L[slot].w);
+			const int j = only_job >= 0 ? only_job : __float_as_int(pool.L[slot].w);
 			const RayPre r = make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
 			const HitRec h = trace_closest_best<kOrder>(jobs[j].sc.sv, r, __float_as_int(o.w), err);
 			pool.hit_idx[slot] = h.idx;
@@ -88,21 +88,31 @@ __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ job
 		atomicOr(status, 1);
 }
 
-// Bin of a ray for the binning sort: its direction octant above a Morton code of
-// the cell (8 x 8 x 8 over the scene's bounding box) that holds its origin.
-__device__ __forceinline__ unsigned spread3(unsigned x) { return (x & 1u) | ((x & 2u) << 2) | ((x & 4u) << 4); }
-__device__ __forceinline__ unsigned cell8(float x, float lo, float hi) {
+// Bin of a ray for the binning sort: its direction octant (kBinOctBits) above a
+// Morton code of the cell that holds its origin, kBinCellBits per axis over the
+// scene's bounding box.
+constexpr int kBinOctBits = 3;
+constexpr int kBinCellBits = 3;
+static_assert(kBinOctBits + 3 * kBinCellBits == kBinBits, "bin key width");
+__device__ __forceinline__ unsigned spread_bits(unsigned x) {
+	unsigned r = 0;
+#pragma unroll
+	for (int b = 0; b < kBinCellBits; b++)
+		r |= ((x >> b) & 1u) << (3 * b);
+	return r;
+}
+__device__ __forceinline__ unsigned cell_of(float x, float lo, float hi) {
+	constexpr float kCells = static_cast<float>(1 << kBinCellBits);
 	// fmaxf maps the NaN of a flat extent (0 * inf) to cell 0
-	return static_cast<unsigned>(fminf(fmaxf((x - lo) * __fdividef(8.0f, hi - lo), 0.0f), 7.0f));
+	return static_cast<unsigned>(fminf(fmaxf((x - lo) * __fdividef(kCells, hi - lo), 0.0f), kCells - 1.0f));
 }
 __device__ __forceinline__ unsigned ray_bin(const SceneView &sv, const F3 &o, const F3 &d) {
 	const unsigned oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
-	const unsigned m = spread3(cell8(o.x, sv.root_lo[0], sv.root_hi[0])) |
-	                   (spread3(cell8(o.y, sv.root_lo[1], sv.root_hi[1])) << 1) |
-	                   (spread3(cell8(o.z, sv.root_lo[2], sv.root_hi[2])) << 2);
-	return (oct << 9) | m;
+	const unsigned m = spread_bits(cell_of(o.x, sv.root_lo[0], sv.root_hi[0])) |
+	                   (spread_bits(cell_of(o.y, sv.root_lo[1], sv.root_hi[1])) << 1) |
+	                   (spread_bits(cell_of(o.z, sv.root_lo[2], sv.root_hi[2])) << 2);
+	return ((oct & ((1u << kBinOctBits) - 1u)) << (3 * kBinCellBits)) | m;
 }
-static_assert(kBinBits == 12, "ray_bin makes 12-bit keys");
 
 __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
                                                   const int *__restrict__ q, int write_keys) {
@@ -149,7 +159,8 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 	}
 }
 
-__global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ jobs, WfPool pool, int k, int *status) {
+__global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ jobs, WfPool pool, int k, int only_job,
+                                                   int *status) {
 	const unsigned n = pool.counters[kCntShadow + k];
 	const int lane = threadIdx.x & 31;
 	int err = 0;
@@ -165,7 +176,7 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 			const float4 so = pool.sh_o[i], sd = pool.sh_d[i];
 			const float4 sc = pool.sh_c[i];
 			const int slot = __float_as_int(sc.w);
-			const int j = __float_as_int(pool.L[slot].w);
+			const int j = only_job >= 0 ? only_job : __float_as_int(pool.L[slot].w);
 			const RayPre r = make_ray(so.x, so.y, so.z, sd.x, sd.y, sd.z);
 			if (!trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err)) {
 				float4 L = pool.L[slot];
@@ -185,7 +196,7 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 // queue lasts (closest hits for the extend stage, any hits for shadow records).
 template <bool kAny>
 __global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ jobs, WfPool pool, int k,
-                                                      const int *__restrict__ q, int *status) {
+                                                      const int *__restrict__ q, int only_job, int *status) {
 	const unsigned n = pool.counters[(kAny ? kCntShadow : kCntRays) + k];
 	unsigned *fetch = pool.counters + (kAny ? kCntFetchSh : kCntFetchExt) + k;
 	const int lane = threadIdx.x & 31;
@@ -223,7 +234,7 @@ __global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ 
 						r = make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
 						ignore = __float_as_int(o.w);
 					}
-					jb = jobs + __float_as_int(pool.L[slot].w);
+					jb = jobs + (only_job >= 0 ? only_job : __float_as_int(pool.L[slot].w));
 					if (jb->sc.sv.nodes4 && finite_inverse(r)) {
 						trav_begin<kAny>(ts, jb->sc.sv, r, tmax, ignore);
 						active = true;
@@ -271,9 +282,10 @@ __global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ 
 
 // Binning sort of the closest-hit queue of bounce k (counting sort on the keys
 // the shade stage wrote): histogram, exclusive scan, scatter. Blocks of 1024
-// threads; keys are masked to kBins so every shared-memory index is in range.
+// threads with a kBins-word histogram in dynamic shared memory; keys are masked
+// to kBins so every shared-memory index is in range.
 __global__ void __launch_bounds__(1024) k_wf_bin_count(WfPool pool, int k) {
-	__shared__ unsigned h[kBins];
+	extern __shared__ unsigned h[];
 	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
 		h[b] = 0;
 	__syncthreads();
@@ -286,13 +298,17 @@ __global__ void __launch_bounds__(1024) k_wf_bin_count(WfPool pool, int k) {
 			atomicAdd(&pool.bins[b], h[b]);
 }
 
-// One block of kBins / 4 threads: bins[] counts -> exclusive offsets.
-__global__ void __launch_bounds__(kBins / 4) k_wf_bin_scan(WfPool pool) {
-	__shared__ unsigned warp_sum[kBins / 4 / 32];
+// One block of 1024 threads, kBins / 1024 consecutive bins each: counts -> exclusive offsets.
+constexpr int kScanThreads = 1024;
+constexpr int kBinsPerThread = kBins / kScanThreads;
+static_assert(kBins % kScanThreads == 0, "k_wf_bin_scan splits the bins evenly");
+__global__ void __launch_bounds__(kScanThreads) k_wf_bin_scan(WfPool pool) {
+	__shared__ unsigned warp_sum[kScanThreads / 32];
 	const int t = threadIdx.x;
-	uint4 *b4 = reinterpret_cast<uint4 *>(pool.bins);
-	const uint4 v = b4[t];
-	const unsigned own = v.x + v.y + v.z + v.w;
+	unsigned *mine = pool.bins + t * kBinsPerThread;
+	unsigned own = 0;
+	for (int i = 0; i < kBinsPerThread; i++)
+		own += mine[i];
 	unsigned x = own;
 	for (int o = 1; o < 32; o <<= 1) {
 		const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
@@ -313,19 +329,18 @@ __global__ void __launch_bounds__(kBins / 4) k_wf_bin_scan(WfPool pool) {
 		warp_sum[t] = z - w;
 	}
 	__syncthreads();
-	uint4 r;
-	r.x = warp_sum[t >> 5] + x - own;
-	r.y = r.x + v.x;
-	r.z = r.y + v.y;
-	r.w = r.z + v.z;
-	b4[t] = r;
+	unsigned run = warp_sum[t >> 5] + x - own;
+	for (int i = 0; i < kBinsPerThread; i++) {
+		const unsigned c = mine[i];
+		mine[i] = run;
+		run += c;
+	}
 }
-static_assert(kBins / 4 == 1024, "k_wf_bin_scan runs one block of 1024 threads");
 
 // Each block takes a contiguous chunk of the queue, reserves its share of every
 // bin with one atomic per non-empty bin, then places its rays.
 __global__ void __launch_bounds__(1024) k_wf_bin_scatter(WfPool pool, int k) {
-	__shared__ unsigned h[kBins];
+	extern __shared__ unsigned h[];
 	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
 		h[b] = 0;
 	__syncthreads();
@@ -388,22 +403,23 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			e = cudaMemsetAsync(pool.bins, 0, kBins * sizeof(unsigned), st);
 			if (e != cudaSuccess)
 				return e;
-			k_wf_bin_count<<<lc.grid_bin, 1024, 0, st>>>(pool, k);
-			k_wf_bin_scan<<<1, kBins / 4, 0, st>>>(pool);
-			k_wf_bin_scatter<<<lc.grid_bin, 1024, 0, st>>>(pool, k);
+			k_wf_bin_count<<<lc.grid_bin, 1024, kBins * sizeof(unsigned), st>>>(pool, k);
+			k_wf_bin_scan<<<1, kScanThreads, 0, st>>>(pool);
+			k_wf_bin_scatter<<<lc.grid_bin, 1024, kBins * sizeof(unsigned), st>>>(pool, k);
 			q = pool.sorted;
 		}
+		const int oj = wave.only_job;
 		if (use_dyn)
-			k_wf_trace_dyn<false><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, q, status);
+			k_wf_trace_dyn<false><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, q, oj, status);
 		else if (order == kOrderNearest)
-			k_wf_extend<kOrderNearest><<<lc.grid_ext, 128, 0, st>>>(d_jobs, pool, k, q, status);
+			k_wf_extend<kOrderNearest><<<lc.grid_ext, 128, 0, st>>>(d_jobs, pool, k, q, oj, status);
 		else
-			k_wf_extend<kOrderReference><<<lc.grid_ext, 128, 0, st>>>(d_jobs, pool, k, q, status);
+			k_wf_extend<kOrderReference><<<lc.grid_ext, 128, 0, st>>>(d_jobs, pool, k, q, oj, status);
 		k_wf_shade<<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, q, sort ? 1 : 0);
 		if (use_dyn)
-			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, status);
+			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, oj, status);
 		else
-			k_wf_shadow<<<lc.grid_sh, 128, 0, st>>>(d_jobs, pool, k, status);
+			k_wf_shadow<<<lc.grid_sh, 128, 0, st>>>(d_jobs, pool, k, oj, status);
 	}
 	const int gacc = (wave.n_pix + 255) / 256 < 148 * 8 ? (wave.n_pix + 255) / 256 : 148 * 8;
 	k_wf_accumulate<<<gacc, 256, 0, st>>>(d_jobs, pool, wave);
@@ -427,6 +443,11 @@ void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn, 
 	const int d = d0 < d1 ? d0 : d1;
 	grid_dyn = sms * (d > 0 ? d : 1);
 	grid_bin = sms; // one 1024-thread block per SM keeps the bin atomics few
+	constexpr int kHist = kBins * static_cast<int>(sizeof(unsigned));
+	if (kHist > 48 * 1024) {
+		cudaFuncSetAttribute(k_wf_bin_count, cudaFuncAttributeMaxDynamicSharedMemorySize, kHist);
+		cudaFuncSetAttribute(k_wf_bin_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, kHist);
+	}
 }
 
 } // namespace rnb

@@ -82,6 +82,7 @@ struct WfWave {
 	int n_slots;        // paths in the wave
 	int n_pix;          // pixels in the wave (sum of active jobs' pixels)
 	int first_sample;   // sample index of k = 0, relative to each job's sample_offset
+	int only_job;       // the job id when the wave holds one job, else -1
 };
 
 // Launch shapes and stage options of a wave.

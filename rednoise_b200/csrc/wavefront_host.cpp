@@ -94,6 +94,7 @@ rn_status WfContext::configure(const std::vector<WfJob> &jobs, int max_depth, in
 		size_t off;
 		int n_jobs;
 		long n_slots, n_pix;
+		int only_job;
 	};
 	std::vector<Span> spans;
 	long capacity = 1;
@@ -115,7 +116,7 @@ rn_status WfContext::configure(const std::vector<WfJob> &jobs, int max_depth, in
 				return RN_ERR_CAPACITY;
 			}
 		}
-		spans.push_back({tab.size(), static_cast<int>(ids.size()), base, pbase});
+		spans.push_back({tab.size(), static_cast<int>(ids.size()), base, pbase, ids.size() == 1 ? ids[0] : -1});
 		for (const auto *v : {&ids, &bases, &pbases, &nsamp})
 			tab.insert(tab.end(), v->begin(), v->end());
 		capacity = std::max(capacity, base);
@@ -146,6 +147,7 @@ rn_status WfContext::configure(const std::vector<WfJob> &jobs, int max_depth, in
 		wv.n_slots = static_cast<int>(sp.n_slots);
 		wv.n_pix = static_cast<int>(sp.n_pix);
 		wv.first_sample = w * spw;
+		wv.only_job = sp.only_job;
 		waves_.push_back(wv);
 	}
 	max_depth_ = max_depth;
