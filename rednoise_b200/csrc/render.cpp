@@ -1,4 +1,5 @@
 // Physical-mode rendering entry points (rn_pt_render / rn_pt_render_accumulate).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -128,68 +129,98 @@ std::tuple<int, int, int, int> tune_key(const PhysCamera &pc, const PhysSettings
 	return {pc.width, pc.height, pst.max_depth, pst.order};
 }
 
-// Measure the candidates on a few samples per pixel and remember the fastest:
-// the megakernel, and the wavefront at 1x..16x the default queue capacity, with
-// and without per-lane ray replacement in its traversal stages and with and
-// without binning each bounce's rays.
+// Device bytes per wavefront path slot: origin, direction, throughput, radiance,
+// pixel, sample, hit record, two queues and the sorted queue, bin key, shadow record.
+constexpr size_t kWfBytesPerPath = 4 * 16 + 4 * 4 + 3 * 4 + 2 + 3 * 16;
+
+// Measure the candidates on up to 64 samples per pixel and remember the fastest:
+// the megakernel, and the wavefront with and without binning each bounce's rays
+// and with and without per-lane ray replacement in its traversal stages (at the
+// largest queue capacity), then the queue capacity itself, from the default up to
+// a whole frame's paths in one wave, within a memory budget.
 rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc, const PhysSettings &pst,
                          rn_pt_tuning &out) {
 	PhysSettings probe = pst;
-	probe.spp = pst.spp < 16 ? (pst.spp > 0 ? pst.spp : 1) : 16;
+	probe.spp = std::clamp(pst.spp, 1, 64);
 	probe.sample_offset = 0x40000000u;
-	const size_t bytes = static_cast<size_t>(pc.width) * pc.height * 3 * sizeof(float);
+	const long n_pix = static_cast<long>(pc.width) * pc.height;
+	const size_t bytes = static_cast<size_t>(n_pix) * 3 * sizeof(float);
 	RNB_CUDA(s->tune_accum.ensure(bytes));
 	float *acc = s->tune_accum.as<float>();
 	cudaStream_t cs = s->stream;
-	cudaEvent_t e0, e1;
-	RNB_CUDA(cudaEventCreate(&e0));
-	RNB_CUDA(cudaEventCreate(&e1));
-	const double samples = static_cast<double>(pc.width) * pc.height * probe.spp;
+	struct Events {
+		cudaEvent_t a = nullptr, b = nullptr;
+		~Events() {
+			if (a)
+				cudaEventDestroy(a);
+			if (b)
+				cudaEventDestroy(b);
+		}
+	} ev;
+	RNB_CUDA(cudaEventCreate(&ev.a));
+	RNB_CUDA(cudaEventCreate(&ev.b));
+	const double samples = static_cast<double>(n_pix) * probe.spp;
 	auto time_one = [&](int integ, int spw, int dyn, int sort, double &sps) -> rn_status {
 		for (int rep = 0; rep < 2; rep++) { // the first run warms caches and captures graphs
 			RNB_CUDA(cudaMemsetAsync(acc, 0, bytes, cs));
-			RNB_CUDA(cudaEventRecord(e0, cs));
+			RNB_CUDA(cudaEventRecord(ev.a, cs));
 			rn_status r = run_fixed(s, integ, spw, dyn, sort, ps, pc, probe, acc, cs);
 			if (r != RN_OK)
 				return r;
-			RNB_CUDA(cudaEventRecord(e1, cs));
+			RNB_CUDA(cudaEventRecord(ev.b, cs));
 		}
-		RNB_CUDA(cudaEventSynchronize(e1));
+		RNB_CUDA(cudaEventSynchronize(ev.b));
 		float ms = 0.0f;
-		RNB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+		RNB_CUDA(cudaEventElapsedTime(&ms, ev.a, ev.b));
 		sps = ms > 0.0f ? samples / (ms * 1e-3) : 0.0;
 		return RN_OK;
 	};
 	rn_status r = time_one(RN_PT_MEGAKERNEL, 0, 0, 0, out.megakernel_sps);
 	if (r != RN_OK)
 		return r;
+	// Queue capacities: d, 2d, 4d, ... samples per wave, at most the probe's spp, with
+	// the path pool within half the free memory and 32 GiB.
+	size_t free_b = 0, total_b = 0;
+	RNB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+	const size_t budget = std::min<size_t>(free_b / 2, static_cast<size_t>(32) << 30);
+	std::vector<int> spws;
+	for (int k = default_samples_per_wave(n_pix, probe.spp); k <= probe.spp; k *= 2) {
+		if (!spws.empty() && static_cast<size_t>(n_pix) * k * kWfBytesPerPath > budget)
+			break;
+		spws.push_back(k);
+	}
+	const int widest = spws.back();
 	out.wavefront_sps = 0.0;
-	out.samples_per_wave = 1;
-	out.dynamic_fetch = 1;
+	out.samples_per_wave = widest;
+	out.dynamic_fetch = 0;
 	out.ray_sort = 0;
-	const int d = default_samples_per_wave(static_cast<long>(pc.width) * pc.height, probe.spp);
 	for (int sort : {0, 1}) {
-		for (int dyn : {1, 0}) {
+		for (int dyn : {0, 1}) {
 			if (dyn && pst.order != kOrderReference)
 				continue;
-			for (int spw : {d, 2 * d, 4 * d, 8 * d, 16 * d}) {
-				if (spw > probe.spp)
-					break;
-				double sps = 0.0;
-				r = time_one(RN_PT_WAVEFRONT, spw, dyn, sort, sps);
-				if (r != RN_OK)
-					return r;
-				if (sps > out.wavefront_sps) {
-					out.wavefront_sps = sps;
-					out.samples_per_wave = spw;
-					out.dynamic_fetch = dyn;
-					out.ray_sort = sort;
-				}
+			double sps = 0.0;
+			r = time_one(RN_PT_WAVEFRONT, widest, dyn, sort, sps);
+			if (r != RN_OK)
+				return r;
+			if (sps > out.wavefront_sps) {
+				out.wavefront_sps = sps;
+				out.dynamic_fetch = dyn;
+				out.ray_sort = sort;
 			}
 		}
 	}
-	cudaEventDestroy(e0);
-	cudaEventDestroy(e1);
+	for (int spw : spws) {
+		if (spw == widest)
+			continue;
+		double sps = 0.0;
+		r = time_one(RN_PT_WAVEFRONT, spw, out.dynamic_fetch, out.ray_sort, sps);
+		if (r != RN_OK)
+			return r;
+		if (sps > out.wavefront_sps) {
+			out.wavefront_sps = sps;
+			out.samples_per_wave = spw;
+		}
+	}
 	out.integrator = out.wavefront_sps > out.megakernel_sps ? RN_PT_WAVEFRONT : RN_PT_MEGAKERNEL;
 	s->tuned[tune_key(pc, pst)] = {out.integrator, out.samples_per_wave, out.dynamic_fetch, out.ray_sort};
 	return RN_OK;

@@ -88,12 +88,12 @@ __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ job
 		atomicOr(status, 1);
 }
 
-// Bin of a ray for the binning sort: its direction octant (kBinOctBits) above a
-// Morton code of the cell that holds its origin, kBinCellBits per axis over the
-// scene's bounding box.
-constexpr int kBinOctBits = 3;
+// Bin of a ray for the binning sort: an octahedral cell of its direction
+// (8 x 8 over the unit octahedron unfolded onto a square) above a Morton code of
+// the cell that holds its origin (8 x 8 x 8 over the scene's bounding box).
+constexpr int kBinDirBits = 6;
 constexpr int kBinCellBits = 3;
-static_assert(kBinOctBits + 3 * kBinCellBits == kBinBits, "bin key width");
+static_assert(kBinDirBits + 3 * kBinCellBits == kBinBits, "bin key width");
 __device__ __forceinline__ unsigned spread_bits(unsigned x) {
 	unsigned r = 0;
 #pragma unroll
@@ -101,17 +101,30 @@ __device__ __forceinline__ unsigned spread_bits(unsigned x) {
 		r |= ((x >> b) & 1u) << (3 * b);
 	return r;
 }
+// fmaxf maps a NaN (a flat extent: 0 * inf) to cell 0
+__device__ __forceinline__ unsigned quantize(float x, float cells) {
+	return static_cast<unsigned>(fminf(fmaxf(x * cells, 0.0f), cells - 1.0f));
+}
 __device__ __forceinline__ unsigned cell_of(float x, float lo, float hi) {
 	constexpr float kCells = static_cast<float>(1 << kBinCellBits);
-	// fmaxf maps the NaN of a flat extent (0 * inf) to cell 0
-	return static_cast<unsigned>(fminf(fmaxf((x - lo) * __fdividef(kCells, hi - lo), 0.0f), kCells - 1.0f));
+	return quantize((x - lo) * __fdividef(1.0f, hi - lo), kCells);
 }
 __device__ __forceinline__ unsigned ray_bin(const SceneView &sv, const F3 &o, const F3 &d) {
-	const unsigned oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+	const float inv_l1 = __fdividef(1.0f, fabsf(d.x) + fabsf(d.y) + fabsf(d.z));
+	float px = d.x * inv_l1, py = d.y * inv_l1;
+	if (d.z < 0.0f) { // fold the lower hemisphere onto the corners
+		const float qx = (1.0f - fabsf(py)) * (px >= 0.0f ? 1.0f : -1.0f);
+		const float qy = (1.0f - fabsf(px)) * (py >= 0.0f ? 1.0f : -1.0f);
+		px = qx;
+		py = qy;
+	}
+	constexpr float kDirCells = static_cast<float>(1 << (kBinDirBits / 2));
+	const unsigned dir = (quantize(0.5f * (py + 1.0f), kDirCells) << (kBinDirBits / 2)) |
+	                     quantize(0.5f * (px + 1.0f), kDirCells);
 	const unsigned m = spread_bits(cell_of(o.x, sv.root_lo[0], sv.root_hi[0])) |
 	                   (spread_bits(cell_of(o.y, sv.root_lo[1], sv.root_hi[1])) << 1) |
 	                   (spread_bits(cell_of(o.z, sv.root_lo[2], sv.root_hi[2])) << 2);
-	return ((oct & ((1u << kBinOctBits) - 1u)) << (3 * kBinCellBits)) | m;
+	return (dir << (3 * kBinCellBits)) | m;
 }
 
 __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,

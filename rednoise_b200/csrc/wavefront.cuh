@@ -50,7 +50,7 @@ struct WfPool {
 	// lengths per bounce, then per-bounce fetch counters of extend and shadow.
 	unsigned *counters;
 	// Ray binning (optional): the shade stage writes each continuation ray's bin
-	// (direction octant, coarse cell of its origin) to keys; before the next
+	// (coarse cell of its direction, coarse cell of its origin) to keys; before the next
 	// closest-hit stage a counting sort by bin rewrites the queue into sorted, so
 	// the lanes of a warp trace rays that start close together in similar
 	// directions and visit the same nodes.
@@ -60,7 +60,7 @@ struct WfPool {
 	int capacity;
 };
 
-constexpr int kBinBits = 12;
+constexpr int kBinBits = 15;
 constexpr int kBins = 1 << kBinBits;
 
 constexpr int kCntRays = 0;
