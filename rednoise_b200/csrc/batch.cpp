@@ -56,42 +56,81 @@ rn_status batch_enqueue(rn_pt_batch *b, unsigned sample_offset, cudaStream_t cs)
 	return RN_OK;
 }
 
-// Time one frame of each integrator at the batch's own sizes and keep the faster.
-rn_status autotune_batch(rn_pt_batch *b) {
-	float best = 0.0f;
-	int pick = RN_PT_WAVEFRONT, pick_sort = 0;
-	cudaEvent_t e0, e1;
-	RNB_CUDA(cudaEventCreate(&e0));
-	RNB_CUDA(cudaEventCreate(&e1));
-	// megakernel per job; wavefront without and with ray binning
-	for (int cand = 0; cand < 3; cand++) {
-		const int integ = cand == 0 ? RN_PT_MEGAKERNEL : RN_PT_WAVEFRONT;
-		const int sort = cand == 2 ? 1 : 0;
-		if (integ == RN_PT_WAVEFRONT && b->forced_sort >= 0 && sort != b->forced_sort)
-			continue;
+// Time one frame of each candidate at the batch's own sizes and keep the fastest:
+// one megakernel per job; the wavefront without and with ray binning at the default
+// queue capacity; then the better of those at 2x, 4x, ... the capacity, up to the
+// largest job's spp, within a memory budget.
+rn_status autotune_batch(rn_pt_batch *b, int max_spp, long total_pix) {
+	struct Events {
+		cudaEvent_t a = nullptr, b = nullptr;
+		~Events() {
+			if (a)
+				cudaEventDestroy(a);
+			if (b)
+				cudaEventDestroy(b);
+		}
+	} ev;
+	RNB_CUDA(cudaEventCreate(&ev.a));
+	RNB_CUDA(cudaEventCreate(&ev.b));
+	auto time_one = [&](int integ, int sort, int spw, float &ms) -> rn_status {
 		b->integrator = integ;
 		b->wf.set_sort(sort);
+		b->spw = spw;
 		rn_status r = batch_enqueue(b, 0x40000000u, b->stream); // warm-up (and graph capture)
 		if (r != RN_OK)
 			return r;
-		RNB_CUDA(cudaEventRecord(e0, b->stream));
+		RNB_CUDA(cudaEventRecord(ev.a, b->stream));
 		r = batch_enqueue(b, 0x40000000u, b->stream);
 		if (r != RN_OK)
 			return r;
-		RNB_CUDA(cudaEventRecord(e1, b->stream));
-		RNB_CUDA(cudaEventSynchronize(e1));
+		RNB_CUDA(cudaEventRecord(ev.b, b->stream));
+		RNB_CUDA(cudaEventSynchronize(ev.b));
+		RNB_CUDA(cudaEventElapsedTime(&ms, ev.a, ev.b));
+		return RN_OK;
+	};
+	const int spw0 = b->spw;
+	float best = 0.0f;
+	int pick = RN_PT_MEGAKERNEL, pick_sort = 0, pick_spw = spw0;
+	rn_status r = time_one(RN_PT_MEGAKERNEL, 0, spw0, best);
+	if (r != RN_OK)
+		return r;
+	float best_wf = 0.0f;
+	int wf_sort = 0;
+	for (int sort : {0, 1}) {
+		if (b->forced_sort >= 0 && sort != b->forced_sort)
+			continue;
 		float ms = 0.0f;
-		RNB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-		if (best == 0.0f || ms < best) {
-			best = ms;
-			pick = integ;
-			pick_sort = sort;
+		r = time_one(RN_PT_WAVEFRONT, sort, spw0, ms);
+		if (r != RN_OK)
+			return r;
+		if (best_wf == 0.0f || ms < best_wf) {
+			best_wf = ms;
+			wf_sort = sort;
 		}
 	}
-	cudaEventDestroy(e0);
-	cudaEventDestroy(e1);
+	int wf_spw = spw0;
+	size_t budget = 0;
+	RNB_CUDA(wf_pool_budget(budget));
+	for (int spw = 2 * spw0; spw <= max_spp; spw *= 2) {
+		if (static_cast<size_t>(total_pix) * spw * kWfBytesPerPath > budget)
+			break;
+		float ms = 0.0f;
+		r = time_one(RN_PT_WAVEFRONT, wf_sort, spw, ms);
+		if (r != RN_OK)
+			return r;
+		if (ms < best_wf) {
+			best_wf = ms;
+			wf_spw = spw;
+		}
+	}
+	if (best_wf < best) {
+		pick = RN_PT_WAVEFRONT;
+		pick_sort = wf_sort;
+		pick_spw = wf_spw;
+	}
 	b->integrator = pick;
 	b->wf.set_sort(pick_sort);
+	b->spw = pick_spw;
 	return RN_OK;
 }
 
@@ -162,7 +201,7 @@ rn_status rn_pt_batch_create(const rn_pt_job *jobs, int n, int integrator, unsig
 		               b->wf_jobs[i].spp > 0 ? 1.0f / static_cast<float>(b->wf_jobs[i].spp) : 0.0f});
 	b->wf.set_frame_io(b->accum.as<float>(), static_cast<size_t>(total) * sizeof(float), res);
 	if (integrator == RN_PT_AUTO) {
-		rn_status r = autotune_batch(b.get());
+		rn_status r = autotune_batch(b.get(), max_spp, total / 3);
 		if (r != RN_OK)
 			return r;
 	} else {

@@ -60,7 +60,6 @@ __device__ __forceinline__ V3 refract(V3 I, V3 N, float eta) {
 // glm mix(x, y, a) = x * (1 - a) + y * a
 __device__ __forceinline__ V3 mix(V3 x, V3 y, float a) { return x * (1.0f - a) + y * a; }
 __device__ __forceinline__ float gmin(float x, float y) { return (y < x) ? y : x; }
-__device__ __forceinline__ float gmax(float x, float y) { return (x < y) ? y : x; }
 __device__ __forceinline__ V3 vmin(V3 a, V3 b) { return {gmin(a.x, b.x), gmin(a.y, b.y), gmin(a.z, b.z)}; }
 // std::max(a, b) = (a < b) ? b : a
 __device__ __forceinline__ float smax(float a, float b) { return (a < b) ? b : a; }

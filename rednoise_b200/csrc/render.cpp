@@ -129,10 +129,6 @@ std::tuple<int, int, int, int> tune_key(const PhysCamera &pc, const PhysSettings
 	return {pc.width, pc.height, pst.max_depth, pst.order};
 }
 
-// Device bytes per wavefront path slot: origin, direction, throughput, radiance,
-// pixel, sample, hit record, two queues and the sorted queue, bin key, shadow record.
-constexpr size_t kWfBytesPerPath = 4 * 16 + 4 * 4 + 3 * 4 + 2 + 3 * 16;
-
 // Measure the candidates on up to 64 samples per pixel and remember the fastest:
 // the megakernel, and the wavefront with and without binning each bounce's rays
 // and with and without per-lane ray replacement in its traversal stages (at the
@@ -180,9 +176,8 @@ rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc,
 		return r;
 	// Queue capacities: d, 2d, 4d, ... samples per wave, at most the probe's spp, with
 	// the path pool within half the free memory and 32 GiB.
-	size_t free_b = 0, total_b = 0;
-	RNB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-	const size_t budget = std::min<size_t>(free_b / 2, static_cast<size_t>(32) << 30);
+	size_t budget = 0;
+	RNB_CUDA(wf_pool_budget(budget));
 	std::vector<int> spws;
 	for (int k = default_samples_per_wave(n_pix, probe.spp); k <= probe.spp; k *= 2) {
 		if (!spws.empty() && static_cast<size_t>(n_pix) * k * kWfBytesPerPath > budget)

@@ -18,7 +18,9 @@ struct U4 {
 
 __host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
 	const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#ifdef __CUDACC__
 #pragma unroll
+#endif
 	for (int r = 0; r < 10; r++) {
 #ifdef __CUDA_ARCH__
 		const uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;

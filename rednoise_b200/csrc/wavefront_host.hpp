@@ -23,6 +23,18 @@ inline int default_samples_per_wave(long n_pix, int spp) {
 	return static_cast<int>(k < 1 ? 1 : k);
 }
 
+// Device bytes per wavefront path slot: origin, direction, throughput, radiance,
+// pixel, sample, hit record, two queues and the sorted queue, bin key, shadow record.
+constexpr size_t kWfBytesPerPath = 4 * 16 + 4 * 4 + 3 * 4 + 2 + 3 * 16;
+
+// Memory the autotuners let a path pool take: half the free device memory, at most 32 GiB.
+inline cudaError_t wf_pool_budget(size_t &budget) {
+	size_t free_b = 0, total_b = 0;
+	const cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+	budget = free_b / 2 < (static_cast<size_t>(32) << 30) ? free_b / 2 : (static_cast<size_t>(32) << 30);
+	return e;
+}
+
 class WfContext {
 public:
 	~WfContext();

@@ -13,6 +13,8 @@ material assignment), so any process reproduces the same triangles bit for bit.
   hash: 60 % Lambert (albedo U[0.2, 0.8]^3), 25 % GGX (roughness U[0.05, 0.5]),
   15 % dielectric (IOR 1.5).
 * ``soup_scene()`` -- the room plus a seeded random triangle soup.
+* ``batch_jobs()`` -- the 64-job batched workload (soup sizes, resolutions, spp).
+* ``views()`` -- seeded camera views for multi-view inverse rendering.
 
 The pinhole camera looks down -z through the open front of the room with a
 40 degree vertical field of view.
@@ -255,6 +257,40 @@ def soup_scene(count: int, seed: int) -> Dict:
     mat = np.zeros(v.shape[0], np.int32)
     par = np.full(v.shape[0], 0.2, np.float32)
     return _finish(v, alb, em, mat, par)
+
+
+def batch_jobs(count: int = 64, seed: int = 0x5EED0003):
+    """The batched workload's job list: per job the room plus a seeded triangle soup
+    whose size is log-uniform in [1e3, 5e5] triangles, a resolution drawn from
+    {256x256, 512x384, 1024x768}, log-uniform spp in [4, 64] and depth 6. Returns
+    dicts with the soup's seed and size (build the scene with ``soup_scene``)."""
+    idx = np.arange(count, dtype=np.uint64)
+    u_n, u_r, u_s = (uniform(seed, k, idx) for k in range(3))
+    sizes = ((256, 256), (512, 384), (1024, 768))
+    jobs = []
+    for i in range(count):
+        n = int(round(math.exp(math.log(1e3) + float(u_n[i]) * math.log(5e5 / 1e3))))
+        w, h = sizes[min(2, int(float(u_r[i]) * 3))]
+        spp = int(round(math.exp(math.log(4.0) + float(u_s[i]) * math.log(64.0 / 4.0))))
+        jobs.append({"soup_seed": seed + 1 + i, "triangles": n, "width": w, "height": h, "spp": spp,
+                     "max_depth": 6})
+    return jobs
+
+
+def views(count: int = 16, size: int = 384, seed: int = 0x5EED0005):
+    """Seeded camera views of the room for multi-view inverse rendering: each camera
+    stands just inside the open front (x, y in [-1.5, 1.5] m, z in [2.0, 2.6] m) and
+    looks at a point near the back wall (x, y in [-1, 1] m, z in [-2, -1] m) with a
+    50 degree vertical field of view."""
+    idx = np.arange(count, dtype=np.uint64)
+    u = [uniform(seed, k, idx) for k in range(6)]
+    out = []
+    for i in range(count):
+        pos = (-1.5 + 3.0 * float(u[0][i]), -1.5 + 3.0 * float(u[1][i]), 2.0 + 0.6 * float(u[2][i]))
+        tgt = (-1.0 + 2.0 * float(u[3][i]), -1.0 + 2.0 * float(u[4][i]), -2.0 + float(u[5][i]))
+        out.append({"position": pos, "target": tgt, "up": (0.0, 1.0, 0.0), "vfov_deg": 50.0, "width": size,
+                    "height": size})
+    return out
 
 
 def glm_normalize(v: np.ndarray) -> np.ndarray:

@@ -160,3 +160,19 @@ def test_icosphere_generator_shape():
     box = scenes.cornell_box()
     assert box["vertices"].shape == (36, 9)
     assert (box["emission"].max(axis=1) > 0).sum() == 2
+
+
+def test_workload_generators_are_seeded_and_in_range():
+    from rednoise_b200 import scenes
+
+    a, b = scenes.batch_jobs(), scenes.batch_jobs()
+    assert a == b and len(a) == 64
+    for j in a:
+        assert 1000 <= j["triangles"] <= 500000
+        assert (j["width"], j["height"]) in ((256, 256), (512, 384), (1024, 768))
+        assert 4 <= j["spp"] <= 64 and j["max_depth"] == 6
+    v = scenes.views()
+    assert v == scenes.views() and len(v) == 16
+    for c in v:
+        assert -1.5 <= c["position"][0] <= 1.5 and 2.0 <= c["position"][2] <= 2.6
+        assert -2.0 <= c["target"][2] <= -1.0 and c["width"] == c["height"] == 384
