@@ -31,10 +31,16 @@ using namespace rnb;
 
 namespace {
 
-rn_status batch_enqueue(rn_pt_batch *b, unsigned sample_offset, cudaStream_t cs) {
+// spp_div > 1 (autotuning probes only): every job renders ceil(spp / spp_div) samples.
+rn_status batch_enqueue(rn_pt_batch *b, unsigned sample_offset, cudaStream_t cs, int spp_div = 1) {
 	std::vector<WfJob> jobs = b->wf_jobs;
-	for (size_t i = 0; i < jobs.size(); i++)
+	for (size_t i = 0; i < jobs.size(); i++) {
 		jobs[i].st.sample_offset = b->jobs[i].settings.sample_offset + sample_offset;
+		if (spp_div > 1) {
+			jobs[i].spp = (jobs[i].spp + spp_div - 1) / spp_div;
+			jobs[i].st.spp = jobs[i].spp;
+		}
+	}
 	int *status = b->status.as<int>();
 	if (b->integrator == RN_PT_WAVEFRONT) {
 		rn_status r = b->wf.configure(jobs, b->max_depth, b->order, b->spw, cs);
@@ -56,11 +62,14 @@ rn_status batch_enqueue(rn_pt_batch *b, unsigned sample_offset, cudaStream_t cs)
 	return RN_OK;
 }
 
-// Time one frame of each candidate at the batch's own sizes and keep the fastest:
+// Time one frame of each candidate at the batch's own image sizes (with a quarter
+// of every job's samples once the largest job has 16 or more) and keep the fastest:
 // one megakernel per job; the wavefront without and with ray binning at the default
-// queue capacity; then the better of those at 2x, 4x, ... the capacity, up to the
-// largest job's spp, within a memory budget.
+// queue capacity; then the better of those at 2x, 4x, ... the capacity while that
+// keeps helping, up to the probe's largest spp, within a memory budget.
 rn_status autotune_batch(rn_pt_batch *b, int max_spp, long total_pix) {
+	const int div = max_spp >= 16 ? 4 : 1;
+	const int probe_spp = (max_spp + div - 1) / div;
 	struct Events {
 		cudaEvent_t a = nullptr, b = nullptr;
 		~Events() {
@@ -76,11 +85,11 @@ rn_status autotune_batch(rn_pt_batch *b, int max_spp, long total_pix) {
 		b->integrator = integ;
 		b->wf.set_sort(sort);
 		b->spw = spw;
-		rn_status r = batch_enqueue(b, 0x40000000u, b->stream); // warm-up (and graph capture)
+		rn_status r = batch_enqueue(b, 0x40000000u, b->stream, div); // warm-up (and graph capture)
 		if (r != RN_OK)
 			return r;
 		RNB_CUDA(cudaEventRecord(ev.a, b->stream));
-		r = batch_enqueue(b, 0x40000000u, b->stream);
+		r = batch_enqueue(b, 0x40000000u, b->stream, div);
 		if (r != RN_OK)
 			return r;
 		RNB_CUDA(cudaEventRecord(ev.b, b->stream));
@@ -111,17 +120,17 @@ rn_status autotune_batch(rn_pt_batch *b, int max_spp, long total_pix) {
 	int wf_spw = spw0;
 	size_t budget = 0;
 	RNB_CUDA(wf_pool_budget(budget));
-	for (int spw = 2 * spw0; spw <= max_spp; spw *= 2) {
+	for (int spw = 2 * spw0; spw <= probe_spp; spw *= 2) {
 		if (static_cast<size_t>(total_pix) * spw * kWfBytesPerPath > budget)
 			break;
 		float ms = 0.0f;
 		r = time_one(RN_PT_WAVEFRONT, wf_sort, spw, ms);
 		if (r != RN_OK)
 			return r;
-		if (ms < best_wf) {
-			best_wf = ms;
-			wf_spw = spw;
-		}
+		if (ms >= best_wf)
+			break;
+		best_wf = ms;
+		wf_spw = spw;
 	}
 	if (best_wf < best) {
 		pick = RN_PT_WAVEFRONT;
