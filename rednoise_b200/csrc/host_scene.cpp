@@ -7,6 +7,7 @@
 #include <fstream>
 #include <map>
 #include <sstream>
+#include <thread>
 
 namespace rnb {
 
@@ -18,19 +19,52 @@ namespace {
 inline float gmin(float x, float y) { return (y < x) ? y : x; }
 inline float gmax(float x, float y) { return (x < y) ? y : x; }
 
+// The tree's shape depends only on the triangle count: a range of c > 4 triangles
+// splits into c/2 and c - c/2. So every subtree's node count (and depth) is known
+// before it is built, each node's pre-order slot can be computed up front, and
+// disjoint subtrees can be built on separate threads with the same result.
+struct Shape {
+	std::map<int, int> nodes, depth;
+	int node_count(int c) {
+		if (c <= 4)
+			return 1;
+		auto it = nodes.find(c);
+		if (it != nodes.end())
+			return it->second;
+		const int v = 1 + node_count(c / 2) + node_count(c - c / 2);
+		nodes[c] = v;
+		return v;
+	}
+	int depth_of(int c) {
+		if (c <= 4)
+			return 1;
+		auto it = depth.find(c);
+		if (it != depth.end())
+			return it->second;
+		const int v = 1 + std::max(depth_of(c / 2), depth_of(c - c / 2));
+		depth[c] = v;
+		return v;
+	}
+};
+
 struct Builder {
 	const float *v;
 	std::vector<Vec3> centroids;
 	Bvh2 *out;
+	Shape shape;
 
 	const float *tri(int i) const { return v + 9 * static_cast<size_t>(i); }
 
 	// src/BVH.cpp:18-63, restated: box over the triangles of order[start, start+count),
 	// leaf when count <= 4, else nth_element at the median centroid of the widest
-	// centroid axis; the node slot is reserved before the children (pre-order).
-	int build(int start, int count, int depth) {
-		if (depth > out->depth)
-			out->depth = depth;
+	// centroid axis; the node takes pre-order slot `self`, its left subtree the slots
+	// after it, its right subtree the slots after those. The top `par_levels` levels
+	// build their left subtree on a new thread.
+	// Node count of a subtree of c triangles; shape.node_count(n) has filled the
+	// table for every size below n before the threads start, so this only reads it.
+	int subtree_nodes(int c) const { return c <= 4 ? 1 : shape.nodes.at(c); }
+
+	void build(int self, int start, int count, int par_levels) {
 		BvhNode node;
 		float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
 		for (int i = start; i < start + count; i++) {
@@ -46,8 +80,8 @@ struct Builder {
 		if (count <= 4) {
 			node.start = start;
 			node.count = count;
-			out->nodes.push_back(node);
-			return static_cast<int>(out->nodes.size()) - 1;
+			out->nodes[static_cast<size_t>(self)] = node;
+			return;
 		}
 		float cmin[3] = {1e30f, 1e30f, 1e30f}, cmax[3] = {-1e30f, -1e30f, -1e30f};
 		for (int i = start; i < start + count; i++) {
@@ -65,20 +99,21 @@ struct Builder {
 		auto key = [cen, axis](int a) { return axis == 0 ? cen[a].x : (axis == 1 ? cen[a].y : cen[a].z); };
 		std::nth_element(out->order.begin() + start, out->order.begin() + mid, out->order.begin() + start + count,
 		                 [&key](int a, int b) { return key(a) < key(b); });
-		if (mid == start || mid == start + count) {
-			node.start = start;
-			node.count = count;
-			out->nodes.push_back(node);
-			return static_cast<int>(out->nodes.size()) - 1;
-		}
+		const int nl = mid - start, nr = start + count - mid;
+		const int l = self + 1;
+		const int r = self + 1 + subtree_nodes(nl);
 		node.count = 0;
-		const int self = static_cast<int>(out->nodes.size());
-		out->nodes.push_back(node);
-		const int l = build(start, mid - start, depth + 1);
-		const int r = build(mid, start + count - mid, depth + 1);
-		out->nodes[self].left = l;
-		out->nodes[self].right = r;
-		return self;
+		node.left = l;
+		node.right = r;
+		out->nodes[static_cast<size_t>(self)] = node;
+		if (par_levels > 0) {
+			std::thread left([this, l, start, nl, par_levels] { build(l, start, nl, par_levels - 1); });
+			build(r, mid, nr, par_levels - 1);
+			left.join();
+		} else {
+			build(l, start, nl, 0);
+			build(r, mid, nr, 0);
+		}
 	}
 };
 
@@ -100,10 +135,15 @@ void build_reference_bvh(const float *v9, int n, Bvh2 &out) {
 		b.centroids[i] = {((t[0] + t[3]) + t[6]) / 3.0f, ((t[1] + t[4]) + t[7]) / 3.0f, ((t[2] + t[5]) + t[8]) / 3.0f};
 	}
 	if (n > 0) {
-		// The tree is built in pre-order, so the node count of a subtree depends only
-		// on its triangle count; reserve once to avoid reallocations on big meshes.
-		out.nodes.reserve(static_cast<size_t>(n) / 2 + 8);
-		out.root = b.build(0, n, 1);
+		out.nodes.resize(static_cast<size_t>(b.shape.node_count(n)));
+		out.depth = b.shape.depth_of(n);
+		// Threads only where subtrees are large enough to repay them.
+		const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+		int par = 0;
+		while ((1u << par) < 2 * hw && (n >> par) > 65536)
+			par++;
+		b.build(0, 0, n, par);
+		out.root = 0;
 	}
 }
 

@@ -135,9 +135,10 @@ def _tree_equal(scene_arrays_v9):
         assert np.array_equal(got["links"], r["links"])
 
 
-@pytest.mark.parametrize("kind", ["cornell", "sphere", "box", "soup", "tiny", "dups"])
+@pytest.mark.parametrize("kind", ["cornell", "sphere", "box", "soup", "tiny", "dups", "threaded"])
 def test_host_bvh_equals_reference_tree(kind):
-    """The product's host build yields the reference's exact tree (src/BVH.cpp:6-63)."""
+    """The product's host build yields the reference's exact tree (src/BVH.cpp:6-63);
+    "threaded" is large enough for the build to split subtrees across threads."""
     a = _assets()
     if kind in ("cornell", "sphere"):
         v9 = a[f"{kind}_v"]
@@ -145,6 +146,8 @@ def test_host_bvh_equals_reference_tree(kind):
         v9 = scenes.cornell_box()["vertices"]
     elif kind == "soup":
         v9 = scenes.soup_scene(5000, seed=3)["vertices"]
+    elif kind == "threaded":
+        v9 = scenes.soup_scene(300000, seed=4)["vertices"]
     elif kind == "tiny":
         v9 = a["cornell_v"][:3]
     else:
