@@ -60,6 +60,8 @@ typedef struct {
 	const float *emission;       /* 3 floats per triangle, radiance Le (default 0) */
 	const int *material;         /* RN_PT_LAMBERT / RN_PT_GGX / RN_PT_DIELECTRIC (default Lambert) */
 	const float *material_param; /* GGX alpha, or dielectric IOR (default 0.2 / 1.5) */
+	const float *ref_vertex_normals; /* 9 floats per triangle, ModelTriangle::vertexNormals for the
+	                                    ray-traced renderer's Phong/Gouraud shading (default: the face normal) */
 } rn_pt_scene_desc;
 
 /* Create a scene from arrays. The scene is freed with rn_scene_free. */
@@ -148,6 +150,28 @@ void rn_pt_ref_params_init(rn_pt_ref_params *p, int width, int height, float cam
  * floats of the per-pixel sample mean before the 8-bit clamp. */
 rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *params, unsigned flags, void *stream,
                                  uint32_t *argb, float *mean_rgb);
+
+/* Shading models of the ray-traced renderer, in the reference's ShadingModel order. */
+#define RN_PT_SHADING_FLAT 0
+#define RN_PT_SHADING_GOURAUD 1
+#define RN_PT_SHADING_PHONG 2
+
+/* Whitted ray tracing with reference semantics (renderRaytraced,
+ * src/Renderer.cpp:909-948, with traceRay / glassTrace / shadeDiffuse /
+ * shadeSurface, src/Renderer.cpp:500-773): mirrors, glass (Fresnel-weighted
+ * reflection and refraction), dispersive glass, tinted metal reflection, emissive
+ * surfaces, and multi-light diffuse + specular shading with soft-shadow visibility
+ * on an ambient floor. The camera, lights and max_depth (recursion levels, 0..8;
+ * the reference uses 4) come from params; samples and the depth-of-field fields
+ * are not used. fog_density > 0 blends towards fog_colour (NULL: the reference's
+ * default (200, 210, 230)) by 1 - exp(-density * distance). argb: width*height
+ * pixels 0xAARRGGBB. rn_render(RN_RAYTRACED) is this call with Phong shading. */
+rn_status rn_pt_render_raytraced(rn_scene *scene, const rn_pt_ref_params *params, int shading, float fog_density,
+                                 const float *fog_colour, unsigned flags, void *stream, uint32_t *argb);
+
+/* Copy the scene's per-corner vertex normals out (9 floats per triangle), as the
+ * reference OBJ loader smooths them (src/ObjLoader.cpp:178-204). */
+rn_status rn_pt_scene_get_vertex_normals(const rn_scene *scene, float *vertex_normals);
 
 /* ---- physical-mode rendering (the additive path-tracing estimator) ---- */
 

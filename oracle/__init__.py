@@ -58,6 +58,8 @@ def ref() -> ctypes.CDLL:
             "refsh_brute_intersect": (None, [vp, ci, vp, vp, vp, vp]),
             "refsh_intersect_triangle": (ci, [vp, vp, vp, vp, vp, vp]),
             "refsh_render_pathtraced": (None, [vp, ci, ci, cf, vp, vp, ci, ci, vp, cf, cf, vp, ci, vp]),
+            "refsh_render_raytraced": (None, [vp, ci, ci, cf, vp, vp, ci, ci, vp, cf, vp, vp]),
+            "refsh_model_set_vertex_normals": (None, [vp, vp]),
             "rn_scene_load_obj": (vp, [ctypes.c_char_p, cf]),
             "rn_scene_free": (None, [vp]),
             "rn_render": (ci, [vp, ci, ci, ci, cf, ci, vp]),
@@ -137,6 +139,29 @@ class RefModel:
         rough = np.zeros(n, np.float32)
         ref().refsh_model_get(self.h, P(v), P(rgb), P(mat), P(nrm), P(rough), None)
         return {"v": v, "rgb": rgb, "material": mat, "normal": nrm, "roughness": rough}
+
+    def vertex_normals(self) -> np.ndarray:
+        """ModelTriangle::vertexNormals of every triangle, (n, 9) float32."""
+        vn = np.zeros((self.count, 9), np.float32)
+        ref().refsh_model_get(self.h, None, None, None, None, None, P(vn))
+        return vn
+
+    def set_vertex_normals(self, vn9) -> None:
+        vn = np.ascontiguousarray(vn9, np.float32).reshape(-1, 9)
+        assert vn.shape[0] == self.count
+        ref().refsh_model_set_vertex_normals(self.h, P(vn))
+
+    def render_raytraced(self, w, h, focal=2.0, pos=(0, 0, 4), target=(0, 0, 0), shading=2, lights=None,
+                         fog_density=0.0, fog_colour=None) -> np.ndarray:
+        """The reference renderRaytraced (src/Renderer.cpp:909-948): 0xAARRGGBB canvas."""
+        pos = np.asarray(pos, np.float32)
+        target = np.asarray(target, np.float32)
+        lt = None if lights is None or len(lights) == 0 else np.ascontiguousarray(lights, np.float32).reshape(-1, 24)
+        fog = None if fog_colour is None else np.asarray(fog_colour, np.float32)
+        out = np.zeros((h, w), np.uint32)
+        ref().refsh_render_raytraced(self.h, w, h, focal, P(pos), P(target), int(shading),
+                                     0 if lt is None else lt.shape[0], P(lt), float(fog_density), P(fog), P(out))
+        return out
 
     def bvh(self):
         if self._bvh is None:

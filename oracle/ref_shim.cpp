@@ -7,6 +7,7 @@
 //   * BVH::BVH / BVH::intersect / BVH::occluded      (src/BVH.cpp:6-139)
 //   * getClosestIntersection / intersectTriangle     (src/Geometry.cpp:11-63)
 //   * renderPathTraced                               (src/Renderer.cpp:1119-1170)
+//   * renderRaytraced                                (src/Renderer.cpp:909-948)
 //   * loadOBJ                                        (src/ObjLoader.cpp:102-214)
 // BVH's node array and triangle order are private in the reference; this shim
 // exposes them (for dumping the tree it built) by compiling BVH.h with
@@ -109,6 +110,15 @@ void refsh_model_get(const void *h, float *v9, int *rgb, int *material, float *n
 		if (roughness)
 			roughness[i] = t.roughness;
 	}
+}
+
+// vn9: n*9 floats, the three vertex normals of each triangle (ModelTriangle::vertexNormals).
+void refsh_model_set_vertex_normals(void *h, const float *vn9) {
+	Model *m = static_cast<Model *>(h);
+	for (size_t i = 0; i < m->tris.size(); i++)
+		for (int k = 0; k < 3; k++)
+			m->tris[i].vertexNormals[k] =
+			    glm::vec3(vn9[9 * i + 3 * k], vn9[9 * i + 3 * k + 1], vn9[9 * i + 3 * k + 2]);
 }
 
 void refsh_model_free(void *h) {
@@ -239,6 +249,21 @@ void refsh_render_pathtraced(const void *model, int w, int h, float focal, const
 	glm::vec3 motion = motion3 ? glm::vec3(motion3[0], motion3[1], motion3[2]) : glm::vec3(0.0f);
 	renderPathTraced(m->tris, cam, canvas, samples, unpackLights(n_lights, lights), aperture, focus, motion, {},
 	                 blades);
+	std::memcpy(out, canvas.pixels.data(), sizeof(uint32_t) * static_cast<size_t>(w) * static_cast<size_t>(h));
+}
+
+// renderRaytraced with the camera built as renderPathTraced's above; shading is the
+// ShadingModel value (0 flat, 1 Gouraud, 2 Phong); fog3 may be null (the default colour).
+void refsh_render_raytraced(const void *model, int w, int h, float focal, const float *pos3, const float *target3,
+                            int shading, int n_lights, const float *lights, float fog_density, const float *fog3,
+                            uint32_t *out) {
+	const Model *m = static_cast<const Model *>(model);
+	Camera cam(w, h, focal, glm::vec3(pos3[0], pos3[1], pos3[2]));
+	cam.lookAt(glm::vec3(target3[0], target3[1], target3[2]));
+	Canvas canvas(static_cast<size_t>(w), static_cast<size_t>(h));
+	const glm::vec3 fog = fog3 ? glm::vec3(fog3[0], fog3[1], fog3[2]) : glm::vec3(200.0f, 210.0f, 230.0f);
+	renderRaytraced(m->tris, cam, canvas, static_cast<ShadingModel>(shading), unpackLights(n_lights, lights), {},
+	                fog_density, fog);
 	std::memcpy(out, canvas.pixels.data(), sizeof(uint32_t) * static_cast<size_t>(w) * static_cast<size_t>(h));
 }
 

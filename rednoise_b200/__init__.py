@@ -153,6 +153,7 @@ class Scene:
         emission=None,
         material=None,
         material_param=None,
+        ref_vertex_normals=None,
     ) -> "Scene":
         """Create a scene from arrays (``vertices``: (n, 9) or (n, 3, 3) floats)."""
         v = _f32(vertices, 9).reshape(-1, 9)
@@ -179,6 +180,7 @@ class Scene:
         opt(emission, _f32, 3, "emission")
         opt(material, _i32, 1, "material")
         opt(material_param, _f32, 1, "material_param")
+        opt(ref_vertex_normals, _f32, 9, "ref_vertex_normals")
         out = ctypes.c_void_p()
         _native.check(_native.load().rn_pt_scene_create(ctypes.byref(desc), ctypes.byref(out)), "rn_pt_scene_create")
         return cls(out.value)
@@ -199,8 +201,8 @@ class Scene:
     ) -> Image:
         """Render through ``rn_render`` and return an :class:`Image`.
 
-        Only ``"pathtraced"`` is served; it runs on the GPU with the reference's
-        camera, default light, depth 4 and 8-bit output.
+        ``"pathtraced"`` and ``"raytraced"`` are served; both run on the GPU with
+        the reference's camera, default light, depth 4 and 8-bit output.
         """
         self._check_open()
         render_mode = RenderMode.coerce(mode)
@@ -338,6 +340,54 @@ class Scene:
         _native.check(_native.load().rn_pt_render_reference(self._handle, ctypes.byref(p), 0, None, _ptr(canvas),
                                                             _ptr(mean)), "render_reference")
         return (canvas, mean) if want_mean else canvas
+
+    def render_raytraced(
+        self,
+        width: int,
+        height: int,
+        *,
+        position: Sequence[float] = (0.0, 0.0, 4.0),
+        target: Sequence[float] = (0.0, 0.0, 0.0),
+        focal_length: float = 2.0,
+        scale: float = 150.0,
+        lights: Optional[Sequence[Light]] = None,
+        max_depth: int = 4,
+        shading: int = _native.RN_PT_SHADING_PHONG,
+        fog_density: float = 0.0,
+        fog_colour: Optional[Sequence[float]] = None,
+        orthographic: bool = False,
+        ortho_scale: float = 1.0,
+    ) -> np.ndarray:
+        """renderRaytraced semantics (Whitted ray tracing): the Canvas as
+        (height, width) uint32 0xAARRGGBB."""
+        self._check_open()
+        p = _native.RefParams()
+        _native.load().rn_pt_ref_params_init(ctypes.byref(p), int(width), int(height), ctypes.c_float(4.0), 1)
+        p.position[:] = tuple(float(x) for x in position)
+        p.target[:] = tuple(float(x) for x in target)
+        p.focal_length = focal_length
+        p.scale = scale
+        p.max_depth = max_depth
+        p.orthographic = 1 if orthographic else 0
+        p.ortho_scale = ortho_scale
+        arr = None
+        if lights:
+            arr = (Light * len(lights))(*lights)
+            p.num_lights = len(lights)
+            p.lights = ctypes.cast(arr, ctypes.POINTER(Light))
+        fog = None if fog_colour is None else np.asarray(fog_colour, np.float32)
+        canvas = np.empty((height, width), np.uint32)
+        _native.check(_native.load().rn_pt_render_raytraced(self._handle, ctypes.byref(p), int(shading),
+                                                            ctypes.c_float(fog_density), _ptr(fog), 0, None,
+                                                            _ptr(canvas)), "render_raytraced")
+        return canvas
+
+    def vertex_normals(self) -> np.ndarray:
+        """Per-corner vertex normals, (n, 9) float32 (the OBJ loader's smoothing)."""
+        self._check_open()
+        out = np.zeros((self.triangle_count, 9), np.float32)
+        _native.check(_native.load().rn_pt_scene_get_vertex_normals(self._handle, _ptr(out)), "vertex_normals")
+        return out
 
     def render_physical(self, camera: "Camera", settings: "Settings", nearest_first: bool = False,
                         out: Optional[np.ndarray] = None, wavefront_static: bool = False,

@@ -19,6 +19,7 @@ RN_PT_WIDTH2 = 4
 RN_PT_WAVEFRONT_STATIC = 8
 RN_PT_RAY_SORT = 16
 RN_PT_NO_RAY_SORT = 32
+RN_PT_SHADING_FLAT, RN_PT_SHADING_GOURAUD, RN_PT_SHADING_PHONG = 0, 1, 2
 RN_PT_STATIC_MAX_PIXELS = 512 * 512
 
 STATUS_NAMES = {
@@ -57,6 +58,7 @@ class SceneDesc(ctypes.Structure):
         ("emission", vp),
         ("material", vp),
         ("material_param", vp),
+        ("ref_vertex_normals", vp),
     ]
 
 
@@ -226,6 +228,9 @@ SIGNATURES = {
     "rn_pt_ref_params_init": (None, [ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                      ctypes.c_int]),
     "rn_pt_render_reference": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_uint, vp, vp, vp]),
+    "rn_pt_render_raytraced": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_float, vp,
+                                              ctypes.c_uint, vp, vp]),
+    "rn_pt_scene_get_vertex_normals": (ctypes.c_int, [vp, vp]),
     "rn_pt_render": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint, vp, vp]),
     "rn_pt_render_accumulate": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                                vp, vp]),

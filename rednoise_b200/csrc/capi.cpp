@@ -203,12 +203,104 @@ rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *prm, u
 	return RN_OK;
 }
 
+rn_status rn_pt_render_raytraced(rn_scene *scene, const rn_pt_ref_params *prm, int shading, float fog_density,
+                                 const float *fog_colour, unsigned flags, void *stream, uint32_t *argb) {
+	if (!scene || !prm || prm->width <= 0 || prm->height <= 0 || !argb) {
+		set_last_error("rn_pt_render_raytraced: invalid argument");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (shading < 0 || shading > 2) {
+		set_last_error("rn_pt_render_raytraced: shading must be RN_PT_SHADING_FLAT, _GOURAUD or _PHONG");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (prm->num_lights < 0 || prm->num_lights > kMaxRefLights || (prm->num_lights > 0 && !prm->lights)) {
+		set_last_error("rn_pt_render_raytraced: num_lights must be in [0, 16] with a lights array");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (prm->max_depth < 0 || prm->max_depth > kMaxWhittedDepth) {
+		set_last_error("rn_pt_render_raytraced: max_depth must be in [0, 8]");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	const long npix = static_cast<long>(prm->width) * prm->height;
+	if (npix > (1L << 28)) {
+		set_last_error("rn_pt_render_raytraced: image too large");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	rn_status st = rn_pt_scene_prepare(scene);
+	if (st != RN_OK)
+		return st;
+	cudaStream_t cs = pick_stream(scene, stream);
+	{
+		// Vertices and vertex normals in the caller's triangle order, 6 float4 each.
+		std::lock_guard<std::mutex> lock(scene->mu);
+		if (!scene->ref_geom_ready) {
+			const TriangleSet &ts = scene->tris;
+			const size_t n = ts.size();
+			std::vector<float4> g(6 * n);
+			for (size_t i = 0; i < n; i++)
+				for (int k = 0; k < 3; k++) {
+					g[6 * i + k] = make_float4(ts.v[9 * i + 3 * k], ts.v[9 * i + 3 * k + 1], ts.v[9 * i + 3 * k + 2], 0.0f);
+					g[6 * i + 3 + k] = make_float4(ts.vnormal[9 * i + 3 * k], ts.vnormal[9 * i + 3 * k + 1],
+					                               ts.vnormal[9 * i + 3 * k + 2], 0.0f);
+				}
+			RNB_CUDA(scene->d_ref_geom.ensure(g.size() * sizeof(float4)));
+			RNB_CUDA(cudaMemcpy(scene->d_ref_geom.p, g.data(), g.size() * sizeof(float4), cudaMemcpyHostToDevice));
+			scene->ref_geom_ready = true;
+		}
+	}
+	RefParams p{};
+	p.width = prm->width;
+	p.height = prm->height;
+	std::memcpy(p.position, prm->position, 12);
+	look_at(prm->position, prm->target, p.orient);
+	p.f = prm->focal_length * prm->scale;
+	p.orthographic = prm->orthographic;
+	p.ortho_scale = prm->ortho_scale;
+	p.max_depth = prm->max_depth;
+	if (prm->num_lights == 0) {
+		p.num_lights = 1;
+		p.lights[0] = default_light();
+	} else {
+		p.num_lights = prm->num_lights;
+		for (int i = 0; i < prm->num_lights; i++)
+			p.lights[i] = to_ref_light(prm->lights[i]);
+	}
+	p.shading = shading;
+	p.fog_density = fog_density;
+	const float fog_default[3] = {200.0f, 210.0f, 230.0f};
+	std::memcpy(p.fog_colour, fog_colour ? fog_colour : fog_default, 12);
+
+	std::lock_guard<std::mutex> lock(scene->scratch_mu);
+	const size_t pb = (sizeof(RefParams) + 255) & ~size_t(255);
+	RNB_CUDA(scene->scratch.ensure(256 + pb + static_cast<size_t>(npix) * 4 + 256));
+	char *base = scene->scratch.as<char>();
+	int *d_err = reinterpret_cast<int *>(base);
+	RefParams *d_p = reinterpret_cast<RefParams *>(base + 256);
+	uint32_t *d_argb = reinterpret_cast<uint32_t *>(base + 256 + pb);
+	const bool dev = (flags & RN_PT_DEVICE_POINTERS) != 0;
+	RNB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), cs));
+	RNB_CUDA(cudaMemcpyAsync(d_p, &p, sizeof(p), cudaMemcpyHostToDevice, cs));
+	RNB_CUDA(launch_render_raytraced(scene->view, scene->d_ref_shade.as<float4>(), scene->d_ref_geom.as<float4>(), d_p,
+	                                 p.width, p.height, dev ? argb : d_argb, d_err, cs));
+	if (!dev)
+		RNB_CUDA(cudaMemcpyAsync(argb, d_argb, static_cast<size_t>(npix) * 4, cudaMemcpyDeviceToHost, cs));
+	// The parameter block lives in scratch: finish before releasing the lock.
+	int h = 0;
+	RNB_CUDA(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, cs));
+	RNB_CUDA(cudaStreamSynchronize(cs));
+	if (h) {
+		set_last_error("rn_pt_render_raytraced: traversal stack bound exceeded (corrupt scene)");
+		return RN_ERR_INTERNAL;
+	}
+	return RN_OK;
+}
+
 int rn_render(const rn_scene *scene, rn_render_mode mode, int width, int height, float cam_z, int samples,
               unsigned char *rgba) {
 	if (!scene || !rgba || width <= 0 || height <= 0)
 		return 0;
-	if (mode != RN_PATHTRACED) {
-		set_last_error("rn_render: only RN_PATHTRACED is served by rednoise-b200");
+	if (mode != RN_PATHTRACED && mode != RN_RAYTRACED) {
+		set_last_error("rn_render: RN_PATHTRACED and RN_RAYTRACED are served by rednoise-b200");
 		return 0;
 	}
 	try {
@@ -216,7 +308,12 @@ int rn_render(const rn_scene *scene, rn_render_mode mode, int width, int height,
 		rn_pt_ref_params_init(&p, width, height, cam_z, samples);
 		std::vector<uint32_t> canvas(static_cast<size_t>(width) * height);
 		// The C ABI takes a const scene; preparation only fills lazily built caches.
-		rn_status st = rn_pt_render_reference(const_cast<rn_scene *>(scene), &p, 0, nullptr, canvas.data(), nullptr);
+		// renderRaytraced's defaults: Phong shading, depth 4, no fog (src/Renderer.h:43-46).
+		rn_status st = mode == RN_RAYTRACED
+		                   ? rn_pt_render_raytraced(const_cast<rn_scene *>(scene), &p, RN_PT_SHADING_PHONG, 0.0f,
+		                                            nullptr, 0, nullptr, canvas.data())
+		                   : rn_pt_render_reference(const_cast<rn_scene *>(scene), &p, 0, nullptr, canvas.data(),
+		                                            nullptr);
 		if (st != RN_OK)
 			return 0;
 		// Canvas 0xAARRGGBB -> RGBA8 (src/capi.cpp:70-78).

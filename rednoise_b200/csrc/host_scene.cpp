@@ -345,6 +345,43 @@ bool load_obj(const std::string &path, float scale, TriangleSet &ts, std::string
 		err = "no faces in " + path;
 		return false;
 	}
+	// Vertex normals (src/ObjLoader.cpp:178-204): per face corner, the normalised sum
+	// of the normals of the faces sharing that OBJ vertex whose normal is within
+	// about 60 degrees (dot > 0.5) of this face's, in face order; the face normal
+	// when the sum vanishes.
+	std::vector<std::vector<int>> vertex_faces(static_cast<size_t>(nv));
+	for (size_t i = 0; i < n; i++)
+		for (int idx : {faces[i].a, faces[i].b, faces[i].c})
+			vertex_faces[static_cast<size_t>(idx)].push_back(static_cast<int>(i));
+	auto fn = [&ts](int i) -> Vec3 {
+		return {ts.normal[3 * static_cast<size_t>(i)], ts.normal[3 * static_cast<size_t>(i) + 1],
+		        ts.normal[3 * static_cast<size_t>(i) + 2]};
+	};
+	auto dot3 = [](Vec3 a, Vec3 b) {
+		const float x = a.x * b.x, y = a.y * b.y, z = a.z * b.z;
+		return (x + y) + z;
+	};
+	ts.vnormal.resize(9 * n);
+	for (size_t i = 0; i < n; i++) {
+		const Vec3 own = fn(static_cast<int>(i));
+		const int corner[3] = {faces[i].a, faces[i].b, faces[i].c};
+		for (int k = 0; k < 3; k++) {
+			Vec3 sum{0.0f, 0.0f, 0.0f};
+			for (int g : vertex_faces[static_cast<size_t>(corner[k])]) {
+				const Vec3 o = fn(g);
+				if (dot3(o, own) > 0.5f)
+					sum = {sum.x + o.x, sum.y + o.y, sum.z + o.z};
+			}
+			Vec3 out = own;
+			if (std::sqrt(dot3(sum, sum)) > 0.0f) {
+				const float inv = 1.0f / std::sqrt(dot3(sum, sum));
+				out = {sum.x * inv, sum.y * inv, sum.z * inv};
+			}
+			ts.vnormal[9 * i + 3 * k] = out.x;
+			ts.vnormal[9 * i + 3 * k + 1] = out.y;
+			ts.vnormal[9 * i + 3 * k + 2] = out.z;
+		}
+	}
 	return true;
 }
 

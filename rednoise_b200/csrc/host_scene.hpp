@@ -40,6 +40,7 @@ struct TriangleSet {
 	std::vector<int> ref_material;  // reference Material code
 	std::vector<float> roughness;   // reference Metal roughness (default 0.2)
 	std::vector<float> normal;      // 3 per triangle, face normal as the loader computes it
+	std::vector<float> vnormal;     // 9 per triangle, vertex normals (ModelTriangle::vertexNormals)
 	std::vector<float> albedo;      // 3 per triangle (physical mode)
 	std::vector<float> emission;    // 3 per triangle (physical mode, Le)
 	std::vector<int> phys_material; // PhysMaterial

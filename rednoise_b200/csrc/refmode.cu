@@ -584,7 +584,286 @@ __global__ void __launch_bounds__(128) k_render_reference(SceneView sv, const fl
 		atomicOr(status, 1);
 }
 
+// ---- Whitted ray tracing (renderRaytraced, src/Renderer.cpp:500-773 and 909-948) ----
+
+struct WHit {
+	bool hit;
+	int idx;
+	float t, u, v;
+	V3 point;
+};
+__device__ __forceinline__ WHit intersect_uv(Ctx &c, V3 o, V3 d) {
+	const RayPre r = make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
+	const HitRec h = trace_closest_best<kOrderReference>(c.sv, r, -1, c.err);
+	WHit out;
+	out.hit = h.idx >= 0;
+	out.idx = h.idx;
+	out.t = h.t;
+	out.u = h.u;
+	out.v = h.v;
+	out.point = o + h.t * d;
+	return out;
+}
+
+// shadeSurface (src/Renderer.cpp:503-535): per light, proximity/incidence diffuse and
+// a power-64 specular lobe, both times soft-shadow visibility, on an ambient floor.
+__device__ V3 shade_surface(Ctx &c, V3 point, V3 normal, V3 view_dir, int ignore, V3 base) {
+	const float ambient = 0.2f;
+	V3 diffuse = mk(0.0f, 0.0f, 0.0f);
+	float spec = 0.0f;
+	for (int li = 0; li < c.p->num_lights; li++) {
+		const RefLight &L = c.p->lights[li];
+		V3 ld;
+		float atten;
+		light_dir(L, point, ld, atten);
+		float cone = 1.0f;
+		if (L.type == kLightSpot)
+			cone = (dot(-ld, normalize(l3(L.direction))) > L.cone_cos) ? 1.0f : 0.0f;
+		const float vis = visibility(c, L, point, ignore);
+		const float incidence = smax(0.0f, dot(normal, ld));
+		const float brightness = vis * cone * atten * incidence;
+		diffuse = diffuse + l3(L.colour) * brightness;
+		if (brightness > 0.0f) {
+			const V3 rd = (2.0f * dot(normal, ld)) * normal - ld;
+			spec += vis * cone * lm_pow(smax(0.0f, dot(rd, view_dir)), 64.0f);
+		}
+	}
+	const V3 lit = vmin(mk(1.0f, 1.0f, 1.0f), diffuse + mk(ambient, ambient, ambient));
+	return base * lit + mk(255.0f, 255.0f, 255.0f) * smin(1.0f, spec);
+}
+
+// bumpNormal (src/Renderer.cpp:574-581): the normal tilted by a Perlin gradient.
+__device__ V3 bump_normal(V3 normal, V3 p) {
+	const V3 q = p * 6.0f;
+	const float e = 0.15f;
+	const V3 g = mk(perlin(q.x + e, q.y, q.z) - perlin(q.x - e, q.y, q.z),
+	                perlin(q.x, q.y + e, q.z) - perlin(q.x, q.y - e, q.z),
+	                perlin(q.x, q.y, q.z + e) - perlin(q.x, q.y, q.z - e));
+	return normalize(normal + 2.0f * g);
+}
+
+// shadeDiffuse (src/Renderer.cpp:663-700), untextured: flat, Gouraud or Phong.
+__device__ V3 shade_diffuse(Ctx &c, const float4 *__restrict__ geom, const WHit &hit, V3 dir) {
+	const float4 s0 = c.ref_shade[2 * hit.idx], s1 = c.ref_shade[2 * hit.idx + 1];
+	const int mat = __float_as_int(s0.w);
+	const V3 point = hit.point;
+	const V3 view = -dir;
+	const float w0 = 1.0f - hit.u - hit.v, w1 = hit.u, w2 = hit.v;
+	const V3 base = base_colour(mat, mk(s1.x, s1.y, s1.z), point);
+	const float4 *g = geom + 6 * static_cast<size_t>(hit.idx);
+	if (c.p->shading == 1) { // Gouraud: shade the corners, interpolate the colours
+		V3 col[3];
+		for (int k = 0; k < 3; k++) {
+			const float4 vk = g[k], nk = g[3 + k];
+			col[k] = shade_surface(c, mk(vk.x, vk.y, vk.z), face_viewer(mk(nk.x, nk.y, nk.z), dir), view, hit.idx,
+			                       base);
+		}
+		return w0 * col[0] + w1 * col[1] + w2 * col[2];
+	}
+	V3 normal;
+	if (c.p->shading == 2) {
+		const float4 n0 = g[3], n1 = g[4], n2 = g[5];
+		normal = normalize(w0 * mk(n0.x, n0.y, n0.z) + w1 * mk(n1.x, n1.y, n1.z) + w2 * mk(n2.x, n2.y, n2.z));
+	} else {
+		normal = mk(s0.x, s0.y, s0.z);
+	}
+	normal = face_viewer(normal, dir);
+	if (mat == kRefBump)
+		normal = bump_normal(normal, point);
+	return shade_surface(c, point, normal, view, hit.idx, base);
+}
+
+// traceRay's recursion (src/Renderer.cpp:704-773) on an explicit stack. A frame is a
+// traceRay call whose value combines the values of its child rays: one reflection
+// for mirrors and metal, and per glassTrace (one for glass, three indices of
+// refraction for dispersive glass) a reflection and, unless totally reflected, a
+// refraction. Each value is formed from its children exactly as the reference
+// forms it, so the result is the recursion's, bit for bit.
+constexpr int kWMirror = 0, kWMetal = 1, kWGlass = 2;
+struct WFrame {
+	V3 co[6], cd[6], res[6];
+	V3 tint;
+	float fres[3];
+	int n, next, kind, ng, tir, depth;
+};
+
+// glassTrace's rays and Fresnel weight (src/Renderer.cpp:711-731) for child pair g.
+__device__ void glass_setup(V3 point, V3 direction, V3 tri_n, float ior, WFrame &f, int g) {
+	V3 n = tri_n;
+	float cosi = dot(direction, n);
+	float etai = 1.0f, etat = ior;
+	if (cosi < 0.0f) {
+		cosi = -cosi;
+	} else {
+		const float tmp = etai;
+		etai = etat;
+		etat = tmp;
+		n = -n;
+	}
+	const V3 refl = reflect(direction, n);
+	f.co[2 * g] = point + 1e-4f * refl;
+	f.cd[2 * g] = refl;
+	const V3 refr = refract(direction, n, etai / etat);
+	f.fres[g] = 0.0f;
+	if (length(refr) < 1e-6f) {
+		f.tir |= 1 << g;
+		return;
+	}
+	float r0 = (etai - etat) / (etai + etat);
+	r0 *= r0;
+	f.fres[g] = r0 + (1.0f - r0) * lm_pow(1.0f - cosi, 5.0f);
+	f.co[2 * g + 1] = point + 1e-4f * refr;
+	f.cd[2 * g + 1] = refr;
+}
+
+// One traceRay(o, d, depth): its value (true), or the frame of its child rays (false).
+__device__ bool whitted_expand(Ctx &c, const float4 *__restrict__ geom, V3 o, V3 d, int depth, V3 &value,
+                               WFrame &f) {
+	const WHit hit = intersect_uv(c, o, d);
+	if (!hit.hit) {
+		value = environment(d);
+		return true;
+	}
+	const float4 s0 = c.ref_shade[2 * hit.idx], s1 = c.ref_shade[2 * hit.idx + 1];
+	const int mat = __float_as_int(s0.w);
+	const V3 tri_n = mk(s0.x, s0.y, s0.z), rgb = mk(s1.x, s1.y, s1.z);
+	if (mat == kRefEmissive) {
+		value = rgb * 1.3f;
+		return true;
+	}
+	if (depth > 0 && (mat == kRefMirror || mat == kRefMetal)) {
+		const V3 n = face_viewer(tri_n, d);
+		const V3 r = reflect(d, n);
+		f.co[0] = hit.point + 1e-4f * r;
+		f.cd[0] = r;
+		f.n = 1;
+		f.next = 0;
+		f.kind = mat == kRefMirror ? kWMirror : kWMetal;
+		f.tint = rgb / 255.0f;
+		f.ng = 0;
+		f.tir = 0;
+		f.depth = depth;
+		return false;
+	}
+	if (depth > 0 && (mat == kRefGlass || mat == kRefDispersive)) {
+		f.kind = kWGlass;
+		f.ng = mat == kRefGlass ? 1 : 3;
+		f.n = 2 * f.ng;
+		f.next = 0;
+		f.tir = 0;
+		f.depth = depth;
+		if (f.ng == 1) {
+			glass_setup(hit.point, d, tri_n, 1.5f, f, 0);
+		} else {
+			glass_setup(hit.point, d, tri_n, 1.50f, f, 0);
+			glass_setup(hit.point, d, tri_n, 1.53f, f, 1);
+			glass_setup(hit.point, d, tri_n, 1.56f, f, 2);
+		}
+		return false;
+	}
+	value = shade_diffuse(c, geom, hit, d);
+	return true;
+}
+
+__device__ V3 whitted_combine(const WFrame &f) {
+	if (f.kind == kWMirror)
+		return f.res[0];
+	if (f.kind == kWMetal)
+		return f.tint * f.res[0];
+	V3 g[3];
+	for (int k = 0; k < f.ng; k++)
+		g[k] = ((f.tir >> k) & 1) ? f.res[2 * k] : f.fres[k] * f.res[2 * k] + (1.0f - f.fres[k]) * f.res[2 * k + 1];
+	if (f.ng == 1)
+		return g[0];
+	return mk(g[0].x, g[1].y, g[2].z);
+}
+
+__device__ V3 trace_whitted(Ctx &c, const float4 *__restrict__ geom, V3 o, V3 d, int max_depth) {
+	// Frames have depth >= 1 and a child's depth is one less, so at most max_depth
+	// frames are open at once.
+	WFrame st[kMaxWhittedDepth + 1];
+	V3 v;
+	if (whitted_expand(c, geom, o, d, max_depth, v, st[0]))
+		return v;
+	int sp = 1;
+	for (;;) {
+		WFrame &f = st[sp - 1];
+		while (f.next < f.n && f.kind == kWGlass && (f.next & 1) && ((f.tir >> (f.next >> 1)) & 1))
+			f.next++; // no refraction ray after total internal reflection
+		if (f.next < f.n) {
+			const int i = f.next;
+			if (whitted_expand(c, geom, f.co[i], f.cd[i], f.depth - 1, v, st[sp])) {
+				f.res[i] = v;
+				f.next++;
+			} else {
+				sp++;
+			}
+			continue;
+		}
+		v = whitted_combine(f);
+		if (--sp == 0)
+			return v;
+		WFrame &parent = st[sp - 1];
+		parent.res[parent.next] = v;
+		parent.next++;
+	}
+}
+
+__global__ void __launch_bounds__(128) k_render_raytraced(SceneView sv, const float4 *__restrict__ ref_shade,
+                                                          const float4 *__restrict__ geom,
+                                                          const RefParams *__restrict__ params,
+                                                          uint32_t *__restrict__ argb, int *status) {
+	const RefParams &p = *params;
+	const long pix = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (pix >= static_cast<long>(p.width) * p.height)
+		return;
+	const int x = static_cast<int>(pix % p.width), y = static_cast<int>(pix / p.width);
+	Ctx c{sv, ref_shade, &p, 0};
+	const V3 right = mk(p.orient[0], p.orient[1], p.orient[2]);
+	const V3 upv = mk(p.orient[3], p.orient[4], p.orient[5]);
+	const V3 fwd = mk(p.orient[6], p.orient[7], p.orient[8]);
+	const V3 pos = l3(p.position);
+	const float f = p.f;
+	// Camera::primaryRay(x - W/2, -(y - H/2), f) (src/Camera.cpp:69-79)
+	const float sx = static_cast<float>(x) - static_cast<float>(p.width) / 2.0f;
+	const float sy = -(static_cast<float>(y) - static_cast<float>(p.height) / 2.0f);
+	V3 ro, dir;
+	if (p.orthographic) {
+		const V3 v = mk(sx / f * p.ortho_scale, sy / f * p.ortho_scale, 0.0f);
+		ro = pos + (right * v.x + upv * v.y + fwd * v.z);
+		dir = normalize(right * 0.0f + upv * 0.0f + fwd * -1.0f);
+	} else {
+		const V3 v = mk(sx / f, sy / f, -1.0f);
+		ro = pos;
+		dir = normalize(right * v.x + upv * v.y + fwd * v.z);
+	}
+	V3 colour = trace_whitted(c, geom, ro, dir, p.max_depth);
+	if (p.fog_density > 0.0f) {
+		const WHit h = intersect_uv(c, ro, dir);
+		const float dist = h.hit ? h.t : 30.0f;
+		colour = mix(colour, l3(p.fog_colour), 1.0f - lm_exp(-p.fog_density * dist));
+	}
+	const int r = min(255, cvt_trunc(colour.x));
+	const int g = min(255, cvt_trunc(colour.y));
+	const int b = min(255, cvt_trunc(colour.z));
+	argb[pix] = (255u << 24) | ((static_cast<uint32_t>(r) & 0xFFu) << 16) | ((static_cast<uint32_t>(g) & 0xFFu) << 8) |
+	            (static_cast<uint32_t>(b) & 0xFFu);
+	if (c.err)
+		atomicOr(status, 1);
+}
+
 } // namespace
+
+cudaError_t launch_render_raytraced(const SceneView &sv, const float4 *ref_shade, const float4 *ref_geom,
+                                    const RefParams *d_params, int width, int height, uint32_t *argb, int *status,
+                                    cudaStream_t st) {
+	const long n = static_cast<long>(width) * height;
+	if (n <= 0)
+		return cudaSuccess;
+	const int bs = 128;
+	k_render_raytraced<<<ceil_div(n, bs), bs, 0, st>>>(sv, ref_shade, ref_geom, d_params, argb, status);
+	return cudaGetLastError();
+}
 
 cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade, const RefParams *d_params, int width,
                                     int height, uint32_t *argb, float *mean_rgb, int *status, cudaStream_t st) {

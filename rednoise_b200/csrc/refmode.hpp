@@ -50,7 +50,19 @@ struct RefParams {
 	float camera_motion[3];
 	int aperture_blades;
 	int aperture_args_right_to_left;
+	// ray-traced renderer only
+	int shading; // 0 flat, 1 Gouraud, 2 Phong
+	float fog_density;
+	float fog_colour[3];
 };
+
+constexpr int kMaxWhittedDepth = 8;
+
+// Whitted ray tracing (renderRaytraced). ref_geom: 6 float4 per triangle in the
+// caller's triangle order: v0, v1, v2, then the three vertex normals.
+cudaError_t launch_render_raytraced(const SceneView &sv, const float4 *ref_shade, const float4 *ref_geom,
+                                    const RefParams *d_params, int width, int height, uint32_t *argb, int *status,
+                                    cudaStream_t st);
 
 cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade, const RefParams *d_params, int width,
                                     int height, uint32_t *argb, float *mean_rgb, int *status, cudaStream_t st);

@@ -173,6 +173,13 @@ bool finish_triangle_set(TriangleSet &ts, std::string &err) {
 			ts.normal[3 * i + 2] = nn.z;
 		}
 	}
+	if (ts.vnormal.size() != 9 * n) { // every corner takes the face normal
+		ts.vnormal.resize(9 * n);
+		for (size_t i = 0; i < n; i++)
+			for (int k = 0; k < 3; k++)
+				for (int a = 0; a < 3; a++)
+					ts.vnormal[9 * i + 3 * k + a] = ts.normal[3 * i + a];
+	}
 	if (ts.albedo.size() != 3 * n)
 		ts.albedo.assign(3 * n, 0.8f);
 	if (ts.emission.size() != 3 * n)
@@ -275,6 +282,8 @@ rn_status rn_pt_scene_create(const rn_pt_scene_desc *desc, rn_scene **out) {
 			ts.roughness.assign(desc->ref_roughness, desc->ref_roughness + n);
 		if (desc->ref_normal)
 			ts.normal.assign(desc->ref_normal, desc->ref_normal + 3 * n);
+		if (desc->ref_vertex_normals)
+			ts.vnormal.assign(desc->ref_vertex_normals, desc->ref_vertex_normals + 9 * n);
 		if (desc->albedo)
 			ts.albedo.assign(desc->albedo, desc->albedo + 3 * n);
 		if (desc->emission)
@@ -348,6 +357,16 @@ rn_status rn_pt_scene_get_triangles(const rn_scene *scene, float *vertices, int 
 		std::memcpy(ref_material, ts.ref_material.data(), ts.ref_material.size() * sizeof(int));
 	if (ref_normal)
 		std::memcpy(ref_normal, ts.normal.data(), ts.normal.size() * sizeof(float));
+	return RN_OK;
+}
+
+rn_status rn_pt_scene_get_vertex_normals(const rn_scene *scene, float *vertex_normals) {
+	if (!scene || !vertex_normals) {
+		set_last_error("rn_pt_scene_get_vertex_normals: NULL argument");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	const TriangleSet &ts = scene->tris;
+	std::memcpy(vertex_normals, ts.vnormal.data(), ts.vnormal.size() * sizeof(float));
 	return RN_OK;
 }
 

@@ -29,6 +29,8 @@ struct rn_scene {
 	int device = -1;
 	cudaStream_t stream = nullptr;
 	rnb::DevBuf d_nodes, d_nodes4, d_tris, d_ref_shade, d_phys_shade, d_emitters;
+	rnb::DevBuf d_ref_geom; // ray-traced renderer: vertices and vertex normals, uploaded on first use
+	bool ref_geom_ready = false;
 	rnb::DevBuf d_status; // error word for asynchronous (device-pointer) calls
 	rnb::SceneView view{};
 	int n_emitters = 0;

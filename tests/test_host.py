@@ -179,3 +179,30 @@ def test_workload_generators_are_seeded_and_in_range():
     for c in v:
         assert -1.5 <= c["position"][0] <= 1.5 and 2.0 <= c["position"][2] <= 2.6
         assert -2.0 <= c["target"][2] <= -1.0 and c["width"] == c["height"] == 384
+
+
+@pytest.mark.parametrize("name", ["sphere", "cornell", "icosphere", "box"])
+def test_loader_vertex_normals_match_reference_loader(name, tmp_path):
+    """Per-corner smoothed normals (src/ObjLoader.cpp:178-204) equal the reference
+    loader's bit for bit on OBJ files whose faces share vertices."""
+    if not oracle.ref_available():
+        pytest.skip("reference library not built")
+    a = _assets()
+    if name in ("sphere", "cornell"):
+        v9, rgb, mat = a[f"{name}_v"], a[f"{name}_rgb"], a[f"{name}_material"]
+    elif name == "icosphere":
+        v9 = scenes.icosphere(2).reshape(-1, 9).astype(np.float32)
+        rgb, mat = np.full((v9.shape[0], 3), 200, np.int32), np.zeros(v9.shape[0], np.int32)
+    else:
+        sc = scenes.cornell_box()
+        v9, rgb, mat = sc["vertices"], sc["ref_rgb"], sc["ref_material"]
+    path = objio.write_obj(str(tmp_path), name, v9, rgb, mat, share_vertices=True)
+    got = rn.Scene.load_obj(path, 1.0).vertex_normals()
+    m = oracle.RefModel.from_obj(path, 1.0)
+    want = m.vertex_normals()
+    m.close()
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    if name in ("sphere", "icosphere"):  # smoothing happened somewhere
+        face = np.repeat(rn.Scene.load_obj(path, 1.0).triangles()["normal"], 3, axis=0).reshape(-1, 9)
+        assert not np.array_equal(got, face)
