@@ -153,5 +153,7 @@ def test_rn_render_zero_samples_and_other_modes(assets, tmp_path):
     assert lib.rn_render(sc, 3, 8, 6, 4.0, 0, buf) == 1
     px = np.frombuffer(buf.raw, np.uint8).reshape(6, 8, 4)
     assert (px[..., :3] == 0).all() and (px[..., 3] == 255).all()  # reference: 0/0 -> black, alpha 255
-    assert lib.rn_render(sc, 2, 8, 6, 4.0, 1, buf) == 0
+    assert lib.rn_render(sc, 2, 8, 6, 4.0, 1, buf) == 1  # RN_RAYTRACED is served too
+    assert lib.rn_render(sc, 1, 8, 6, 4.0, 1, buf) == 0  # the rasteriser is not
+    assert lib.rn_render(sc, 0, 8, 6, 4.0, 1, buf) == 0
     lib.rn_scene_free(sc)
