@@ -50,9 +50,9 @@ def parse():
     p.add_argument("--integrator", default="auto", choices=["auto", "megakernel", "wavefront"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-grad", action="store_true", help="skip the gradient-vs-primal timing")
-    p.add_argument("--workload", default="frame", choices=["frame", "batch64", "inverse"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batch64", "inverse", "raytraced"],
                    help="frame: the 1.31M-triangle 1080p frame (the bench line); batch64: 64 scenes per "
-                        "launch; inverse: 16-view albedo recovery")
+                        "launch; inverse: 16-view albedo recovery; raytraced: Whitted ray tracing")
     p.add_argument("--inverse-steps", type=int, default=200)
     return p.parse_args()
 
@@ -659,6 +659,48 @@ def run_inverse(args):
     print(json.dumps(line), flush=True)
 
 
+def run_raytraced(args):
+    """Whitted ray tracing (rn_render(RN_RAYTRACED) semantics: Phong, default disk
+    light, depth 4) of the 1.31M-triangle scene at the bench resolution, through
+    the C ABI with a host output canvas, against the reference renderRaytraced on
+    the host cores (a bounded 1/16-area frame of the same camera)."""
+    import torch
+
+    import rednoise_b200 as rn
+    from rednoise_b200 import scenes
+
+    torch.cuda.set_device(0)
+    sc = scenes.icosphere_scene(level=args.level)
+    s = rn.Scene.from_arrays(sc["vertices"], ref_rgb=sc["ref_rgb"], ref_material=sc["ref_material"],
+                             ref_roughness=sc["ref_roughness"])
+    s.prepare()
+    W, H = args.width, args.height
+    pos = (0.0, 0.0, scenes.CAMERA_Z)
+    focal = reference_focal(H)
+    for _ in range(args.warmup):
+        s.render_raytraced(W, H, focal_length=focal, position=pos)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.render_raytraced(W, H, focal_length=focal, position=pos)
+    gpu_s = (time.perf_counter() - t0) / args.steps
+    model = reference_model(sc)
+    w, h = W // 4, H // 4
+    t0 = time.perf_counter()
+    model.render_raytraced(w, h, focal=reference_focal(h), pos=pos)
+    cpu_s = time.perf_counter() - t0
+    build = reference_bvh_build_s(model)
+    cpu_rate = w * h / max(cpu_s - build, 1e-9)
+    line = {"metric": "pixels/s (Whitted ray tracing, end to end through the C ABI)", "value": W * H / gpu_s,
+            "unit": "pixels/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": gpu_s * 1e3,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"icosphere-cornell-1.31M-tris {W}x{H} renderRaytraced (Phong, default light, "
+                                   "depth 4)", "output": "host canvas, copy included"},
+            "cpu_baseline": {"value": cpu_rate, "unit": "pixels/s", "cores": os.cpu_count(), "kind": "reference",
+                             "sample": f"reference renderRaytraced, one {w}x{h} frame of the same camera "
+                                       f"({cpu_s:.1f} s, its BVH rebuild of {build:.2f} s excluded)"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -667,6 +709,8 @@ def main():
         run_batch64(args)
     elif args.workload == "inverse":
         run_inverse(args)
+    elif args.workload == "raytraced":
+        run_raytraced(args)
     else:
         run_ours(args)
 
