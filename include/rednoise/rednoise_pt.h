@@ -169,6 +169,19 @@ rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *params
 rn_status rn_pt_render_raytraced(rn_scene *scene, const rn_pt_ref_params *params, int shading, float fog_density,
                                  const float *fog_colour, unsigned flags, void *stream, uint32_t *argb);
 
+/* Photon mapping with reference semantics (renderPhotonMapped,
+ * src/Renderer.cpp:1177-1349, PhotonMap, src/Photon.cpp): num_photons photons
+ * (the reference's default is 200000) from the first light, traced through
+ * mirrors, metal and glass and stored at diffuse hits with Russian roulette, all
+ * drawn from one std::mt19937(777) stream in the reference's order; then per pixel
+ * direct light plus the irradiance gathered within 0.25 units (gather_rays > 0: a
+ * final gather of that many cosine rays, each image row drawing from
+ * std::mt19937(1000 + y)). The camera and lights come from params (samples,
+ * max_depth and depth-of-field fields are not used). argb: width*height pixels
+ * 0xAARRGGBB; num_stored (may be NULL) receives the number of stored photons. */
+rn_status rn_pt_render_photon_mapped(rn_scene *scene, const rn_pt_ref_params *params, int num_photons, int gather_rays,
+                                     unsigned flags, void *stream, uint32_t *argb, unsigned *num_stored);
+
 /* Copy the scene's per-corner vertex normals out (9 floats per triangle), as the
  * reference OBJ loader smooths them (src/ObjLoader.cpp:178-204). */
 rn_status rn_pt_scene_get_vertex_normals(const rn_scene *scene, float *vertex_normals);

@@ -60,6 +60,7 @@ def ref() -> ctypes.CDLL:
             "refsh_render_pathtraced": (None, [vp, ci, ci, cf, vp, vp, ci, ci, vp, cf, cf, vp, ci, vp]),
             "refsh_render_raytraced": (None, [vp, ci, ci, cf, vp, vp, ci, ci, vp, cf, vp, vp]),
             "refsh_model_set_vertex_normals": (None, [vp, vp]),
+            "refsh_render_photon_mapped": (None, [vp, ci, ci, cf, vp, vp, ci, ci, ci, vp, vp]),
             "rn_scene_load_obj": (vp, [ctypes.c_char_p, cf]),
             "rn_scene_free": (None, [vp]),
             "rn_render": (ci, [vp, ci, ci, ci, cf, ci, vp]),
@@ -161,6 +162,17 @@ class RefModel:
         out = np.zeros((h, w), np.uint32)
         ref().refsh_render_raytraced(self.h, w, h, focal, P(pos), P(target), int(shading),
                                      0 if lt is None else lt.shape[0], P(lt), float(fog_density), P(fog), P(out))
+        return out
+
+    def render_photon_mapped(self, w, h, num_photons=200000, gather_rays=0, focal=2.0, pos=(0, 0, 4),
+                             target=(0, 0, 0), lights=None) -> np.ndarray:
+        """The reference renderPhotonMapped (src/Renderer.cpp:1300-1349): 0xAARRGGBB canvas."""
+        pos = np.asarray(pos, np.float32)
+        target = np.asarray(target, np.float32)
+        lt = None if lights is None or len(lights) == 0 else np.ascontiguousarray(lights, np.float32).reshape(-1, 24)
+        out = np.zeros((h, w), np.uint32)
+        ref().refsh_render_photon_mapped(self.h, w, h, focal, P(pos), P(target), int(num_photons), int(gather_rays),
+                                         0 if lt is None else lt.shape[0], P(lt), P(out))
         return out
 
     def bvh(self):

@@ -8,6 +8,7 @@
 //   * getClosestIntersection / intersectTriangle     (src/Geometry.cpp:11-63)
 //   * renderPathTraced                               (src/Renderer.cpp:1119-1170)
 //   * renderRaytraced                                (src/Renderer.cpp:909-948)
+//   * renderPhotonMapped                             (src/Renderer.cpp:1300-1349)
 //   * loadOBJ                                        (src/ObjLoader.cpp:102-214)
 // BVH's node array and triangle order are private in the reference; this shim
 // exposes them (for dumping the tree it built) by compiling BVH.h with
@@ -264,6 +265,17 @@ void refsh_render_raytraced(const void *model, int w, int h, float focal, const 
 	const glm::vec3 fog = fog3 ? glm::vec3(fog3[0], fog3[1], fog3[2]) : glm::vec3(200.0f, 210.0f, 230.0f);
 	renderRaytraced(m->tris, cam, canvas, static_cast<ShadingModel>(shading), unpackLights(n_lights, lights), {},
 	                fog_density, fog);
+	std::memcpy(out, canvas.pixels.data(), sizeof(uint32_t) * static_cast<size_t>(w) * static_cast<size_t>(h));
+}
+
+// renderPhotonMapped with the camera built as above (src/Renderer.cpp:1300-1349).
+void refsh_render_photon_mapped(const void *model, int w, int h, float focal, const float *pos3, const float *target3,
+                                int num_photons, int gather_rays, int n_lights, const float *lights, uint32_t *out) {
+	const Model *m = static_cast<const Model *>(model);
+	Camera cam(w, h, focal, glm::vec3(pos3[0], pos3[1], pos3[2]));
+	cam.lookAt(glm::vec3(target3[0], target3[1], target3[2]));
+	Canvas canvas(static_cast<size_t>(w), static_cast<size_t>(h));
+	renderPhotonMapped(m->tris, cam, canvas, num_photons, unpackLights(n_lights, lights), {}, gather_rays);
 	std::memcpy(out, canvas.pixels.data(), sizeof(uint32_t) * static_cast<size_t>(w) * static_cast<size_t>(h));
 }
 

@@ -382,6 +382,41 @@ class Scene:
                                                             _ptr(canvas)), "render_raytraced")
         return canvas
 
+    def render_photon_mapped(
+        self,
+        width: int,
+        height: int,
+        num_photons: int = 200000,
+        *,
+        gather_rays: int = 0,
+        position: Sequence[float] = (0.0, 0.0, 4.0),
+        target: Sequence[float] = (0.0, 0.0, 0.0),
+        focal_length: float = 2.0,
+        scale: float = 150.0,
+        lights: Optional[Sequence[Light]] = None,
+        return_count: bool = False,
+    ):
+        """renderPhotonMapped semantics: the Canvas as (height, width) uint32
+        0xAARRGGBB (and the number of stored photons with ``return_count``)."""
+        self._check_open()
+        p = _native.RefParams()
+        _native.load().rn_pt_ref_params_init(ctypes.byref(p), int(width), int(height), ctypes.c_float(4.0), 1)
+        p.position[:] = tuple(float(x) for x in position)
+        p.target[:] = tuple(float(x) for x in target)
+        p.focal_length = focal_length
+        p.scale = scale
+        arr = None
+        if lights:
+            arr = (Light * len(lights))(*lights)
+            p.num_lights = len(lights)
+            p.lights = ctypes.cast(arr, ctypes.POINTER(Light))
+        canvas = np.empty((height, width), np.uint32)
+        count = ctypes.c_uint(0)
+        _native.check(_native.load().rn_pt_render_photon_mapped(self._handle, ctypes.byref(p), int(num_photons),
+                                                                int(gather_rays), 0, None, _ptr(canvas),
+                                                                ctypes.byref(count)), "render_photon_mapped")
+        return (canvas, int(count.value)) if return_count else canvas
+
     def vertex_normals(self) -> np.ndarray:
         """Per-corner vertex normals, (n, 9) float32 (the OBJ loader's smoothing)."""
         self._check_open()

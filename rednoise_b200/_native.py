@@ -231,6 +231,8 @@ SIGNATURES = {
     "rn_pt_render_raytraced": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_float, vp,
                                               ctypes.c_uint, vp, vp]),
     "rn_pt_scene_get_vertex_normals": (ctypes.c_int, [vp, vp]),
+    "rn_pt_render_photon_mapped": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_uint, vp, vp, vp]),
     "rn_pt_render": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint, vp, vp]),
     "rn_pt_render_accumulate": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                                vp, vp]),

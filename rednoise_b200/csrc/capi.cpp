@@ -4,6 +4,7 @@
 #include <cstring>
 #include <vector>
 
+#include "photon.hpp"
 #include "refmode.hpp"
 #include "scene_impl.hpp"
 
@@ -290,6 +291,74 @@ rn_status rn_pt_render_raytraced(rn_scene *scene, const rn_pt_ref_params *prm, i
 	RNB_CUDA(cudaStreamSynchronize(cs));
 	if (h) {
 		set_last_error("rn_pt_render_raytraced: traversal stack bound exceeded (corrupt scene)");
+		return RN_ERR_INTERNAL;
+	}
+	return RN_OK;
+}
+
+rn_status rn_pt_render_photon_mapped(rn_scene *scene, const rn_pt_ref_params *prm, int num_photons, int gather_rays,
+                                     unsigned flags, void *stream, uint32_t *argb, unsigned *num_stored) {
+	if (!scene || !prm || prm->width <= 0 || prm->height <= 0 || !argb) {
+		set_last_error("rn_pt_render_photon_mapped: invalid argument");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (num_photons < 1 || num_photons > kMaxPhotons || gather_rays < 0 || gather_rays > 4096) {
+		set_last_error("rn_pt_render_photon_mapped: need 1 <= num_photons <= 4194304 and 0 <= gather_rays <= 4096");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (prm->num_lights < 0 || prm->num_lights > kMaxRefLights || (prm->num_lights > 0 && !prm->lights)) {
+		set_last_error("rn_pt_render_photon_mapped: num_lights must be in [0, 16] with a lights array");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	const long npix = static_cast<long>(prm->width) * prm->height;
+	if (npix > (1L << 28)) {
+		set_last_error("rn_pt_render_photon_mapped: image too large");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	rn_status st = rn_pt_scene_prepare(scene);
+	if (st != RN_OK)
+		return st;
+	RefParams p{};
+	p.width = prm->width;
+	p.height = prm->height;
+	std::memcpy(p.position, prm->position, 12);
+	look_at(prm->position, prm->target, p.orient);
+	p.f = prm->focal_length * prm->scale;
+	if (prm->num_lights == 0) {
+		p.num_lights = 1;
+		p.lights[0] = default_light();
+	} else {
+		p.num_lights = prm->num_lights;
+		for (int i = 0; i < prm->num_lights; i++)
+			p.lights[i] = to_ref_light(prm->lights[i]);
+	}
+	size_t map_bytes = 0;
+	RNB_CUDA(photon_scratch_bytes(num_photons, map_bytes));
+	cudaStream_t cs = pick_stream(scene, stream);
+	std::lock_guard<std::mutex> lock(scene->scratch_mu);
+	const size_t pb = (sizeof(RefParams) + 255) & ~size_t(255);
+	const size_t img = (static_cast<size_t>(npix) * 4 + 255) & ~size_t(255);
+	RNB_CUDA(scene->scratch.ensure(256 + pb + img + map_bytes));
+	char *base = scene->scratch.as<char>();
+	int *d_err = reinterpret_cast<int *>(base);
+	RefParams *d_p = reinterpret_cast<RefParams *>(base + 256);
+	uint32_t *d_argb = reinterpret_cast<uint32_t *>(base + 256 + pb);
+	void *d_map = base + 256 + pb + img;
+	const bool dev = (flags & RN_PT_DEVICE_POINTERS) != 0;
+	RNB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), cs));
+	RNB_CUDA(cudaMemcpyAsync(d_p, &p, sizeof(p), cudaMemcpyHostToDevice, cs));
+	unsigned stored = 0;
+	RNB_CUDA(launch_photon_mapped(scene->view, scene->d_ref_shade.as<float4>(), p, d_p, num_photons, gather_rays, d_map,
+	                              map_bytes, dev ? argb : d_argb, d_err, cs, &stored));
+	if (num_stored)
+		*num_stored = stored;
+	if (!dev)
+		RNB_CUDA(cudaMemcpyAsync(argb, d_argb, static_cast<size_t>(npix) * 4, cudaMemcpyDeviceToHost, cs));
+	int h = 0;
+	RNB_CUDA(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, cs));
+	RNB_CUDA(cudaStreamSynchronize(cs));
+	if (h) {
+		set_last_error("rn_pt_render_photon_mapped: traversal stack bound exceeded (corrupt scene)");
 		return RN_ERR_INTERNAL;
 	}
 	return RN_OK;
