@@ -50,9 +50,10 @@ def parse():
     p.add_argument("--integrator", default="auto", choices=["auto", "megakernel", "wavefront"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-grad", action="store_true", help="skip the gradient-vs-primal timing")
-    p.add_argument("--workload", default="frame", choices=["frame", "batch64", "inverse", "raytraced"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batch64", "inverse", "raytraced", "photon"],
                    help="frame: the 1.31M-triangle 1080p frame (the bench line); batch64: 64 scenes per "
-                        "launch; inverse: 16-view albedo recovery; raytraced: Whitted ray tracing")
+                        "launch; inverse: 16-view albedo recovery; raytraced: Whitted ray tracing; "
+                        "photon: photon mapping")
     p.add_argument("--inverse-steps", type=int, default=200)
     return p.parse_args()
 
@@ -663,7 +664,7 @@ def run_raytraced(args):
     """Whitted ray tracing (rn_render(RN_RAYTRACED) semantics: Phong, default disk
     light, depth 4) of the 1.31M-triangle scene at the bench resolution, through
     the C ABI with a host output canvas, against the reference renderRaytraced on
-    the host cores (a bounded 1/16-area frame of the same camera)."""
+    the host cores (one frame of the same camera)."""
     import torch
 
     import rednoise_b200 as rn
@@ -684,7 +685,7 @@ def run_raytraced(args):
         s.render_raytraced(W, H, focal_length=focal, position=pos)
     gpu_s = (time.perf_counter() - t0) / args.steps
     model = reference_model(sc)
-    w, h = W // 4, H // 4
+    w, h = W, H
     t0 = time.perf_counter()
     model.render_raytraced(w, h, focal=reference_focal(h), pos=pos)
     cpu_s = time.perf_counter() - t0
@@ -701,6 +702,50 @@ def run_raytraced(args):
     print(json.dumps(line), flush=True)
 
 
+def run_photon(args):
+    """Photon mapping (renderPhotonMapped: 200 000 photons from the default light,
+    gather radius 0.25, no final gather) of the 1.31M-triangle scene at the bench
+    resolution, through the C ABI with a host output canvas, against the reference
+    on the host cores (one frame)."""
+    import torch
+
+    import rednoise_b200 as rn
+    from rednoise_b200 import scenes
+
+    torch.cuda.set_device(0)
+    sc = scenes.icosphere_scene(level=args.level)
+    s = rn.Scene.from_arrays(sc["vertices"], ref_rgb=sc["ref_rgb"], ref_material=sc["ref_material"],
+                             ref_roughness=sc["ref_roughness"])
+    s.prepare()
+    W, H = args.width, args.height
+    pos = (0.0, 0.0, scenes.CAMERA_Z)
+    focal = reference_focal(H)
+    photons = 200000
+    for _ in range(args.warmup):
+        s.render_photon_mapped(W, H, photons, focal_length=focal, position=pos)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        img, stored = s.render_photon_mapped(W, H, photons, focal_length=focal, position=pos, return_count=True)
+    gpu_s = (time.perf_counter() - t0) / args.steps
+    model = reference_model(sc)
+    t0 = time.perf_counter()
+    want = model.render_photon_mapped(W, H, photons, focal=focal, pos=pos)
+    cpu_s = time.perf_counter() - t0
+    build = reference_bvh_build_s(model)
+    same = float((img == want).mean())
+    line = {"metric": "frames/s (photon mapping, end to end through the C ABI)", "value": 1.0 / gpu_s,
+            "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": gpu_s * 1e3,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"icosphere-cornell-1.31M-tris {W}x{H} renderPhotonMapped, {photons} photons",
+                       "stored_photons": stored, "output": "host canvas, copy included"},
+            "identical_pixels_vs_reference": same,
+            "cpu_baseline": {"value": 1.0 / max(cpu_s - build, 1e-9), "unit": "frames/s", "cores": os.cpu_count(),
+                             "kind": "reference",
+                             "sample": f"reference renderPhotonMapped, one frame ({cpu_s:.1f} s, its BVH rebuild of "
+                                       f"{build:.2f} s excluded)"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -711,6 +756,8 @@ def main():
         run_inverse(args)
     elif args.workload == "raytraced":
         run_raytraced(args)
+    elif args.workload == "photon":
+        run_photon(args)
     else:
         run_ours(args)
 
