@@ -182,6 +182,26 @@ rn_status rn_pt_render_raytraced(rn_scene *scene, const rn_pt_ref_params *params
 rn_status rn_pt_render_photon_mapped(rn_scene *scene, const rn_pt_ref_params *params, int num_photons, int gather_rays,
                                      unsigned flags, void *stream, uint32_t *argb, unsigned *num_stored);
 
+/* ---- canvas post-processing (src/Renderer.cpp:1353-1470), reference semantics ----
+ * Canvases are width*height pixels 0xAARRGGBB, processed in place; host arrays
+ * unless flags has RN_PT_DEVICE_POINTERS. */
+
+/* toneMap: Reinhard on exposure-scaled colour, then gamma. */
+rn_status rn_pt_tonemap(uint32_t *argb, int width, int height, float exposure, float gamma, unsigned flags,
+                        void *stream);
+/* applyBloom: pixels brighter than threshold (luma in 0..1), blurred by three
+ * separable 13-tap box passes, added back times intensity. */
+rn_status rn_pt_bloom(uint32_t *argb, int width, int height, float threshold, float intensity, unsigned flags,
+                      void *stream);
+/* applyFXAA: interior pixels on luma edges (contrast >= 0.12) blended towards
+ * their 4-neighbour average. */
+rn_status rn_pt_fxaa(uint32_t *argb, int width, int height, unsigned flags, void *stream);
+/* AccumBuffer::add / resolve: sum (3 floats per pixel, read and written) += the
+ * canvas colour; resolve writes sum / count as a canvas. */
+rn_status rn_pt_accum_add(float *sum, const uint32_t *argb, int width, int height, unsigned flags, void *stream);
+rn_status rn_pt_accum_resolve(const float *sum, int count, uint32_t *argb, int width, int height, unsigned flags,
+                              void *stream);
+
 /* Copy the scene's per-corner vertex normals out (9 floats per triangle), as the
  * reference OBJ loader smooths them (src/ObjLoader.cpp:178-204). */
 rn_status rn_pt_scene_get_vertex_normals(const rn_scene *scene, float *vertex_normals);

@@ -61,6 +61,10 @@ def ref() -> ctypes.CDLL:
             "refsh_render_raytraced": (None, [vp, ci, ci, cf, vp, vp, ci, ci, vp, cf, vp, vp]),
             "refsh_model_set_vertex_normals": (None, [vp, vp]),
             "refsh_render_photon_mapped": (None, [vp, ci, ci, cf, vp, vp, ci, ci, ci, vp, vp]),
+            "refsh_tonemap": (None, [vp, ci, ci, cf, cf]),
+            "refsh_bloom": (None, [vp, ci, ci, cf, cf]),
+            "refsh_fxaa": (None, [vp, ci, ci]),
+            "refsh_accum": (None, [ci, vp, ci, ci, vp]),
             "rn_scene_load_obj": (vp, [ctypes.c_char_p, cf]),
             "rn_scene_free": (None, [vp]),
             "rn_render": (ci, [vp, ci, ci, ci, cf, ci, vp]),
@@ -101,6 +105,24 @@ def orc() -> ctypes.CDLL:
 
 
 # ---- convenience wrappers ---------------------------------------------------------
+
+def ref_postfx(kind: str, canvas, *args) -> np.ndarray:
+    """The reference's toneMap / applyBloom / applyFXAA on a copy of canvas ((h, w) uint32)."""
+    c = np.ascontiguousarray(canvas, np.uint32).copy()
+    h, w = c.shape
+    fn = {"tonemap": ref().refsh_tonemap, "bloom": ref().refsh_bloom, "fxaa": ref().refsh_fxaa}[kind]
+    fn(P(c), w, h, *args)
+    return c
+
+
+def ref_accum(frames) -> np.ndarray:
+    """The reference AccumBuffer: add every frame ((k, h, w) uint32), then resolve."""
+    f = np.ascontiguousarray(frames, np.uint32)
+    k, h, w = f.shape
+    out = np.zeros((h, w), np.uint32)
+    ref().refsh_accum(k, P(f), w, h, P(out))
+    return out
+
 
 class RefModel:
     """A reference triangle list (vector<ModelTriangle>) and, lazily, its BVH."""

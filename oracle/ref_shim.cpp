@@ -279,4 +279,39 @@ void refsh_render_photon_mapped(const void *model, int w, int h, float focal, co
 	std::memcpy(out, canvas.pixels.data(), sizeof(uint32_t) * static_cast<size_t>(w) * static_cast<size_t>(h));
 }
 
+// ---- canvas post-processing (src/Renderer.cpp:1353-1470), in place on px ----
+static Canvas to_canvas(const uint32_t *px, int w, int h) {
+	Canvas c(static_cast<size_t>(w), static_cast<size_t>(h));
+	std::memcpy(c.pixels.data(), px, sizeof(uint32_t) * static_cast<size_t>(w) * static_cast<size_t>(h));
+	return c;
+}
+static void from_canvas(const Canvas &c, uint32_t *px) {
+	std::memcpy(px, c.pixels.data(), sizeof(uint32_t) * c.pixels.size());
+}
+void refsh_tonemap(uint32_t *px, int w, int h, float exposure, float gamma) {
+	Canvas c = to_canvas(px, w, h);
+	toneMap(c, exposure, gamma);
+	from_canvas(c, px);
+}
+void refsh_bloom(uint32_t *px, int w, int h, float threshold, float intensity) {
+	Canvas c = to_canvas(px, w, h);
+	applyBloom(c, threshold, intensity);
+	from_canvas(c, px);
+}
+void refsh_fxaa(uint32_t *px, int w, int h) {
+	Canvas c = to_canvas(px, w, h);
+	applyFXAA(c);
+	from_canvas(c, px);
+}
+// AccumBuffer over n_frames canvases stored one after another; the resolve into out.
+void refsh_accum(int n_frames, const uint32_t *frames, int w, int h, uint32_t *out) {
+	AccumBuffer acc(w, h);
+	const size_t n = static_cast<size_t>(w) * static_cast<size_t>(h);
+	for (int f = 0; f < n_frames; f++)
+		acc.add(to_canvas(frames + n * static_cast<size_t>(f), w, h));
+	Canvas c(static_cast<size_t>(w), static_cast<size_t>(h));
+	acc.resolve(c);
+	from_canvas(c, out);
+}
+
 } // extern "C"

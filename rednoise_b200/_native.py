@@ -231,6 +231,13 @@ SIGNATURES = {
     "rn_pt_render_raytraced": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_float, vp,
                                               ctypes.c_uint, vp, vp]),
     "rn_pt_scene_get_vertex_normals": (ctypes.c_int, [vp, vp]),
+    "rn_pt_tonemap": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_uint,
+                                     vp]),
+    "rn_pt_bloom": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_uint,
+                                   vp]),
+    "rn_pt_fxaa": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, vp]),
+    "rn_pt_accum_add": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, vp]),
+    "rn_pt_accum_resolve": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, vp]),
     "rn_pt_render_photon_mapped": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_uint, vp, vp, vp]),
     "rn_pt_render": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint, vp, vp]),
