@@ -326,28 +326,6 @@ def profiled_traffic():
         return json.load(f)
 
 
-def l2_roofline(achieved_gbs: float) -> dict:
-    """The traversal's algorithmic bytes are served mostly by L2 and L1, not DRAM: the
-    same achieved rate against an L2-resident read bandwidth measured here (a 64 MB
-    float32 reduction, repeated, well inside the 126 MB L2)."""
-    import torch
-
-    x = torch.ones(16 << 20, dtype=torch.float32, device="cuda")
-    for _ in range(3):
-        x.sum()
-    torch.cuda.synchronize()
-    reps = 50
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
-        x.sum()
-    e1.record()
-    torch.cuda.synchronize()
-    gbs = reps * x.numel() * 4 / (e0.elapsed_time(e1) / 1e3) / 1e9
-    return {"achieved": achieved_gbs, "peak": gbs, "unit": "GB/s", "frac": achieved_gbs / gbs,
-            "peak_kind": "measured here: L2-resident 64 MB read (torch.sum)"}
-
-
 def run_ours(args):
     import torch
 
@@ -537,8 +515,7 @@ def run_ours(args):
                                     "traversal, counted on the GPU for 1 spp of the same frame",
                      "kernel_ms": kernel_ms,
                      "scope": "whole frame: the closest-hit and shadow traversal kernels are 81 % of its device "
-                              "time (ncu launch list); traffic scaled from a 480x270 capture",
-                     "l2": l2_roofline(achieved)},
+                              "time (ncu launch list); traffic scaled from a 480x270 capture"},
         "clocks": clk,
         "rmse_vs_fp64_64spp": rmse,
         "at_equal_rmse": at_rmse,
