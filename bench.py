@@ -326,6 +326,29 @@ def profiled_traffic():
         return json.load(f)
 
 
+def reference_semantics_rate(sc, W, H, args, spp=2) -> dict:
+    """The drop-in renderer (rn_render's renderPathTraced semantics: depth 4, the
+    default disk light with its 9 shadow rays per vertex, per-pixel mt19937, 8-bit
+    output) on the same geometry and camera as the CPU baseline, through the C ABI
+    with a host canvas: the like-for-like counterpart of cpu_baseline."""
+    import rednoise_b200 as rn
+    from rednoise_b200 import scenes
+
+    s = rn.Scene.from_arrays(sc["vertices"], ref_rgb=sc["ref_rgb"], ref_material=sc["ref_material"],
+                             ref_roughness=sc["ref_roughness"])
+    s.prepare()
+    kw = dict(position=(0.0, 0.0, scenes.CAMERA_Z), focal_length=reference_focal(H))
+    s.render_reference(W, H, spp, **kw)
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        s.render_reference(W, H, spp, **kw)
+    dt = (time.perf_counter() - t0) / reps
+    s.close()
+    return {"value": W * H * spp / dt, "unit": UNIT, "ms_per_frame": dt * 1e3,
+            "workload": f"{W}x{H} at {spp} spp, reference semantics (rn_pt_render_reference, host canvas)"}
+
+
 def run_ours(args):
     import torch
 
@@ -489,6 +512,7 @@ def run_ours(args):
     grad = None
     if not args.no_grad:
         grad = gradient_timing(scene, lib, stream, sptr, l2)
+    like_for_like = reference_semantics_rate(sc, W, H, args)
 
     peak, peak_kind = measured_peaks()
     kernel_ms = float(np.mean(render_ms))
@@ -521,6 +545,7 @@ def run_ours(args):
         "at_equal_rmse": at_rmse,
         "path_vertices_per_s": value * counts["closest"] / counts["samples"],
         "gradient": grad,
+        "reference_semantics_gpu": like_for_like,
         "integrators_samples_per_s": compare,
         "scene_build_ms": info["build_ms"],
     }
