@@ -181,7 +181,7 @@ __device__ void sample_aperture(int blades, float u1, float u2, float &lx, float
 	ly = v0y * s + v1y * t;
 }
 
-__global__ void __launch_bounds__(128) k_render_reference(SceneView sv, const float4 *__restrict__ ref_shade,
+__global__ void __launch_bounds__(128, 10) k_render_reference(SceneView sv, const float4 *__restrict__ ref_shade,
                                                           const RefParams *__restrict__ params,
                                                           uint32_t *__restrict__ argb, float *__restrict__ mean_rgb,
                                                           int *status) {
