@@ -413,7 +413,33 @@ __device__ __forceinline__ bool finite_inverse(const RayPre &r) {
 	       fabsf(r.iz) < __int_as_float(0x7f800000);
 }
 
-__device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPre &r, int ignore, int &err) {
+// Traversal stack storage. LocalStack keeps the whole stack in the thread's
+// local memory. SharedShortStack keeps the top kN entries in this thread's column
+// of a shared-memory array (entry i of thread t at base[i * stride + t]) and
+// deeper entries in local memory: the frequent shallow pushes and pops then cost
+// one shared-memory access instead of a scattered local-memory access.
+template <typename T> struct LocalStack {
+	T st[kStack];
+	__device__ __forceinline__ void put(int i, T v) { st[i] = v; }
+	__device__ __forceinline__ T get(int i) const { return st[i]; }
+};
+template <typename T, int kN> struct SharedShortStack {
+	T *col;
+	int stride;
+	T spill[kStack - kN];
+	__device__ __forceinline__ SharedShortStack(T *column, int stride_) : col(column), stride(stride_) {}
+	__device__ __forceinline__ void put(int i, T v) {
+		if (i < kN)
+			col[i * stride] = v;
+		else
+			spill[i - kN] = v;
+	}
+	__device__ __forceinline__ T get(int i) const { return i < kN ? col[i * stride] : spill[i - kN]; }
+};
+
+template <class Stack>
+__device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPre &r, int ignore, int &err,
+                                                 Stack &st) {
 	const RayPair r2 = make_pair_ray(r);
 	HitRec h;
 	h.idx = -1;
@@ -423,16 +449,15 @@ __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPr
 	h.v = 0.0f;
 	// Stack entry: node or leaf ref in the low word, its entry distance in the high
 	// word, pushed and popped as one 64-bit local-memory access.
-	unsigned long long st[kStack];
 	int sp = 0;
 	float te;
 	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te)) {
-		st[0] = pack_entry(s.root4_ref, te);
+		st.put(0, pack_entry(s.root4_ref, te));
 		sp = 1;
 	}
 	while (sp > 0) {
 		--sp;
-		const unsigned long long e = st[sp];
+		const unsigned long long e = st.get(sp);
 		int ref = static_cast<int>(static_cast<unsigned>(e));
 		if (!(__int_as_float(static_cast<int>(e >> 32)) < h.t))
 			continue;
@@ -453,11 +478,11 @@ __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPr
 				return h;
 			}
 			if (b3)
-				st[sp++] = pack_entry(__float_as_int(rf.w), t3);
+				st.put(sp++, pack_entry(__float_as_int(rf.w), t3));
 			if (b2)
-				st[sp++] = pack_entry(__float_as_int(rf.z), t2);
+				st.put(sp++, pack_entry(__float_as_int(rf.z), t2));
 			if (b1)
-				st[sp++] = pack_entry(__float_as_int(rf.y), t1);
+				st.put(sp++, pack_entry(__float_as_int(rf.y), t1));
 			if (b0 && t0 < h.t) {
 				ref = __float_as_int(rf.x);
 			} else {
@@ -490,18 +515,24 @@ __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPr
 	return h;
 }
 
-__device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err) {
+__device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPre &r, int ignore, int &err) {
+	LocalStack<unsigned long long> st;
+	return trace_closest4(s, r, ignore, err, st);
+}
+
+template <class Stack>
+__device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err,
+                                           Stack &st) {
 	const RayPair r2 = make_pair_ray(r);
-	int st[kStack];
 	int sp = 0;
 	float te;
 	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te) &&
 	    te < tmax) {
-		st[0] = s.root4_ref;
+		st.put(0, s.root4_ref);
 		sp = 1;
 	}
 	while (sp > 0) {
-		int ref = st[--sp];
+		int ref = st.get(--sp);
 		while (ref >= 0) {
 			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ref);
 			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
@@ -519,15 +550,15 @@ __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, 
 				return false;
 			}
 			if (b3)
-				st[sp++] = __float_as_int(rf.w);
+				st.put(sp++, __float_as_int(rf.w));
 			if (b2)
-				st[sp++] = __float_as_int(rf.z);
+				st.put(sp++, __float_as_int(rf.z));
 			if (b1)
-				st[sp++] = __float_as_int(rf.y);
+				st.put(sp++, __float_as_int(rf.y));
 			if (b0) {
 				ref = __float_as_int(rf.x);
 			} else if (sp > 0) {
-				ref = st[--sp];
+				ref = st.get(--sp);
 			} else {
 				ref = 0x7fffffff;
 				break;
@@ -550,6 +581,11 @@ __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, 
 		}
 	}
 	return false;
+}
+
+__device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err) {
+	LocalStack<int> st;
+	return trace_any4(s, r, tmax, ignore, err, st);
 }
 
 // ---- resumable 4-wide traversal for persistent kernels that replace finished rays ----
@@ -675,6 +711,22 @@ __device__ __forceinline__ HitRec trace_closest_best(const SceneView &s, const R
 __device__ __forceinline__ bool trace_any_best(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err) {
 	if (s.nodes4 && finite_inverse(r))
 		return trace_any4(s, r, tmax, ignore, err);
+	return trace_any(s, r, tmax, ignore, err);
+}
+
+// The same with caller-provided stack storage for the 4-wide traversals.
+template <int kOrder, class Stack>
+__device__ __forceinline__ HitRec trace_closest_best(const SceneView &s, const RayPre &r, int ignore, int &err,
+                                                     Stack &st) {
+	if (kOrder == kOrderReference && s.nodes4 && finite_inverse(r))
+		return trace_closest4(s, r, ignore, err, st);
+	return trace_closest<kOrder>(s, r, ignore, err);
+}
+template <class Stack>
+__device__ __forceinline__ bool trace_any_best(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err,
+                                               Stack &st) {
+	if (s.nodes4 && finite_inverse(r))
+		return trace_any4(s, r, tmax, ignore, err, st);
 	return trace_any(s, r, tmax, ignore, err);
 }
 

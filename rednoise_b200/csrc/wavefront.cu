@@ -59,6 +59,14 @@ __global__ void __launch_bounds__(256) k_wf_camera(const WfJob *__restrict__ job
 		pool.counters[kCntRays] = static_cast<unsigned>(wave.n_slots);
 }
 
+// Top entries of the traversal stack that the one-ray-per-lane traversal stages
+// keep in shared memory, the rest in local memory (0: all in local memory). On
+// the 1.31M-triangle frame 8 and 16 entries measure the same frame rate as the
+// all-local stack: the L1-cached local stack is not what bounds these stages.
+constexpr int kWfShortStack = 8;
+constexpr size_t kWfExtendSmem = static_cast<size_t>(kWfShortStack) * 128 * sizeof(unsigned long long);
+constexpr size_t kWfShadowSmem = static_cast<size_t>(kWfShortStack) * 128 * sizeof(int);
+
 template <int kOrder>
 __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ jobs, WfPool pool, int k,
                                                    const int *__restrict__ q, int only_job, int *status) {
@@ -79,7 +87,14 @@ __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ job
 			const float4 d = pool.d[slot];
 			const int j = only_job >= 0 ? only_job : __float_as_int(pool.L[slot].w);
 			const RayPre r = make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
-			const HitRec h = trace_closest_best<kOrder>(jobs[j].sc.sv, r, __float_as_int(o.w), err);
+			HitRec h;
+			if constexpr (kWfShortStack > 0) {
+				extern __shared__ unsigned long long wf_ext_stack[];
+				SharedShortStack<unsigned long long, kWfShortStack> st(wf_ext_stack + threadIdx.x, blockDim.x);
+				h = trace_closest_best<kOrder>(jobs[j].sc.sv, r, __float_as_int(o.w), err, st);
+			} else {
+				h = trace_closest_best<kOrder>(jobs[j].sc.sv, r, __float_as_int(o.w), err);
+			}
 			pool.hit_idx[slot] = h.idx;
 			pool.hit_t[slot] = h.t;
 		}
@@ -191,7 +206,15 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 			const int slot = __float_as_int(sc.w);
 			const int j = only_job >= 0 ? only_job : __float_as_int(pool.L[slot].w);
 			const RayPre r = make_ray(so.x, so.y, so.z, sd.x, sd.y, sd.z);
-			if (!trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err)) {
+			bool occluded;
+			if constexpr (kWfShortStack > 0) {
+				extern __shared__ int wf_sh_stack[];
+				SharedShortStack<int, kWfShortStack> st(wf_sh_stack + threadIdx.x, blockDim.x);
+				occluded = trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err, st);
+			} else {
+				occluded = trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err);
+			}
+			if (!occluded) {
 				float4 L = pool.L[slot];
 				L.x += sc.x;
 				L.y += sc.y;
@@ -425,14 +448,14 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 		if (use_dyn)
 			k_wf_trace_dyn<false><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, q, oj, status);
 		else if (order == kOrderNearest)
-			k_wf_extend<kOrderNearest><<<lc.grid_ext, 128, 0, st>>>(d_jobs, pool, k, q, oj, status);
+			k_wf_extend<kOrderNearest><<<lc.grid_ext, 128, kWfExtendSmem, st>>>(d_jobs, pool, k, q, oj, status);
 		else
-			k_wf_extend<kOrderReference><<<lc.grid_ext, 128, 0, st>>>(d_jobs, pool, k, q, oj, status);
+			k_wf_extend<kOrderReference><<<lc.grid_ext, 128, kWfExtendSmem, st>>>(d_jobs, pool, k, q, oj, status);
 		k_wf_shade<<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, q, sort ? 1 : 0);
 		if (use_dyn)
 			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, oj, status);
 		else
-			k_wf_shadow<<<lc.grid_sh, 128, 0, st>>>(d_jobs, pool, k, oj, status);
+			k_wf_shadow<<<lc.grid_sh, 128, kWfShadowSmem, st>>>(d_jobs, pool, k, oj, status);
 	}
 	const int gacc = (wave.n_pix + 255) / 256 < 148 * 8 ? (wave.n_pix + 255) / 256 : 148 * 8;
 	k_wf_accumulate<<<gacc, 256, 0, st>>>(d_jobs, pool, wave);
@@ -445,9 +468,9 @@ void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn, 
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	int a = 0, b = 0, c = 0, d0 = 0, d1 = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_wf_extend<kOrderNearest>, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_wf_extend<kOrderReference>, 128, kWfExtendSmem);
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_wf_shade, 128, 0);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_wf_shadow, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_wf_shadow, 128, kWfShadowSmem);
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d0, k_wf_trace_dyn<false>, 128, 0);
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d1, k_wf_trace_dyn<true>, 128, 0);
 	grid_ext = sms * (a > 0 ? a : 1);
