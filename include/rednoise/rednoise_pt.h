@@ -40,6 +40,8 @@ typedef enum {
 #define RN_PT_WAVEFRONT_STATIC 8u /* wavefront: one ray per lane in the traversal stages (default: lanes refetch) */
 #define RN_PT_RAY_SORT 16u        /* wavefront: bin each bounce's rays by origin cell and direction before tracing */
 #define RN_PT_NO_RAY_SORT 32u     /* wavefront: never bin (default without either flag: the tuned choice) */
+#define RN_PT_LBVH 64u            /* physical renders and ray queries: the GPU-built BVH (rn_pt_scene_build_lbvh),
+                                     traversed nearest child first */
 
 /* Physical-mode materials. */
 #define RN_PT_LAMBERT 0
@@ -70,6 +72,15 @@ rn_status rn_pt_scene_create(const rn_pt_scene_desc *desc, rn_scene **out);
 /* Build the reference BVH (src/BVH.cpp:6-63, identical tree and triangle
  * order) and upload the scene now instead of at the first query. */
 rn_status rn_pt_scene_prepare(rn_scene *scene);
+
+/* Build a second BVH on the GPU (a linear BVH: Morton codes, radix sort, Karras'
+ * hierarchy, bottom-up boxes; one triangle per leaf) for callers that rebuild
+ * often. Calls given RN_PT_LBVH use it with nearest-child-first traversal and ties
+ * on the hit distance broken by leaf position: their closest hits agree with the
+ * reference tree's except for exact ties and hits the reference's box test misses.
+ * The reference tree stays the default. build_ms (may be NULL) receives the build
+ * time including the upload of the vertices. Prepares the scene first. */
+rn_status rn_pt_scene_build_lbvh(rn_scene *scene, void *stream, double *build_ms);
 
 /* Facts about the prepared scene. */
 typedef struct {

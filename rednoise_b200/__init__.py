@@ -255,7 +255,8 @@ class Scene:
                                                _ptr(links)), "dump_bvh")
         return {"order": order, "bounds": bounds, "links": links}
 
-    def trace_closest(self, origins, directions, ignore=None, nearest_first: bool = False, width2: bool = False):
+    def trace_closest(self, origins, directions, ignore=None, nearest_first: bool = False, width2: bool = False,
+                      lbvh: bool = False):
         """Closest hit per ray: (tri, t, u, v) numpy arrays (tri = -1 on a miss).
         ``width2`` traverses the 2-wide reference tree instead of its 4-wide collapse."""
         self._check_open()
@@ -269,12 +270,13 @@ class Scene:
         t = np.empty(n, np.float32)
         u = np.empty(n, np.float32)
         v = np.empty(n, np.float32)
-        flags = (_native.RN_PT_ORDER_NEAREST if nearest_first else 0) | (_native.RN_PT_WIDTH2 if width2 else 0)
+        flags = (_native.RN_PT_ORDER_NEAREST if nearest_first else 0) | (_native.RN_PT_WIDTH2 if width2 else 0) | (
+            _native.RN_PT_LBVH if lbvh else 0)
         _native.check(_native.load().rn_pt_trace_closest(self._handle, n, _ptr(o), _ptr(d), _ptr(ig), flags, None,
                                                          _ptr(tri), _ptr(t), _ptr(u), _ptr(v)), "trace_closest")
         return tri, t, u, v
 
-    def trace_any(self, origins, directions, tmax, ignore=None, width2: bool = False) -> np.ndarray:
+    def trace_any(self, origins, directions, tmax, ignore=None, width2: bool = False, lbvh: bool = False) -> np.ndarray:
         """Occlusion per ray (1 if anything is hit strictly before ``tmax``)."""
         self._check_open()
         o = _f32(origins, 3).reshape(-1, 3)
@@ -285,7 +287,7 @@ class Scene:
             raise ValueError("tmax must have one value per ray")
         ig = None if ignore is None else _i32(ignore).reshape(-1)
         occ = np.empty(n, np.int32)
-        flags = _native.RN_PT_WIDTH2 if width2 else 0
+        flags = (_native.RN_PT_WIDTH2 if width2 else 0) | (_native.RN_PT_LBVH if lbvh else 0)
         _native.check(_native.load().rn_pt_trace_any(self._handle, n, _ptr(o), _ptr(d), _ptr(tm), _ptr(ig), flags,
                                                      None, _ptr(occ)), "trace_any")
         return occ
@@ -417,6 +419,14 @@ class Scene:
                                                                 ctypes.byref(count)), "render_photon_mapped")
         return (canvas, int(count.value)) if return_count else canvas
 
+    def build_lbvh(self) -> float:
+        """Build the GPU linear BVH (used by calls given ``lbvh=True``); returns its build time in ms."""
+        self._check_open()
+        ms = ctypes.c_double(0.0)
+        _native.check(_native.load().rn_pt_scene_build_lbvh(self._handle, None, ctypes.byref(ms)),
+                      "rn_pt_scene_build_lbvh")
+        return ms.value
+
     def vertex_normals(self) -> np.ndarray:
         """Per-corner vertex normals, (n, 9) float32 (the OBJ loader's smoothing)."""
         self._check_open()
@@ -426,13 +436,14 @@ class Scene:
 
     def render_physical(self, camera: "Camera", settings: "Settings", nearest_first: bool = False,
                         out: Optional[np.ndarray] = None, wavefront_static: bool = False,
-                        ray_sort: Optional[bool] = None) -> np.ndarray:
+                        ray_sort: Optional[bool] = None, lbvh: bool = False) -> np.ndarray:
         """Physical-mode render: per-pixel mean radiance as (height, width, 3) float32.
         ``ray_sort`` forces the wavefront's ray binning on or off (None: the tuned choice)."""
         self._check_open()
         rgb = out if out is not None else np.empty((camera.height, camera.width, 3), np.float32)
         flags = (_native.RN_PT_ORDER_NEAREST if nearest_first else 0) | (
-            _native.RN_PT_WAVEFRONT_STATIC if wavefront_static else 0) | _sort_flag(ray_sort)
+            _native.RN_PT_WAVEFRONT_STATIC if wavefront_static else 0) | _sort_flag(ray_sort) | (
+            _native.RN_PT_LBVH if lbvh else 0)
         _native.check(_native.load().rn_pt_render(self._handle, ctypes.byref(camera), ctypes.byref(settings), flags,
                                                   None, _ptr(rgb)), "rn_pt_render")
         return rgb

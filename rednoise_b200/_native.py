@@ -19,6 +19,7 @@ RN_PT_WIDTH2 = 4
 RN_PT_WAVEFRONT_STATIC = 8
 RN_PT_RAY_SORT = 16
 RN_PT_NO_RAY_SORT = 32
+RN_PT_LBVH = 64
 RN_PT_SHADING_FLAT, RN_PT_SHADING_GOURAUD, RN_PT_SHADING_PHONG = 0, 1, 2
 RN_PT_STATIC_MAX_PIXELS = 512 * 512
 
@@ -231,6 +232,7 @@ SIGNATURES = {
     "rn_pt_render_raytraced": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_float, vp,
                                               ctypes.c_uint, vp, vp]),
     "rn_pt_scene_get_vertex_normals": (ctypes.c_int, [vp, vp]),
+    "rn_pt_scene_build_lbvh": (ctypes.c_int, [vp, vp, ctypes.POINTER(ctypes.c_double)]),
     "rn_pt_tonemap": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_uint,
                                      vp]),
     "rn_pt_bloom": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_uint,

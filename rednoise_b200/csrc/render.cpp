@@ -78,6 +78,14 @@ rn_status make_phys_inputs(rn_scene *s, const rn_pt_camera *c, const rn_pt_setti
 	pst.max_depth = st->max_depth;
 	pst.rr_depth = st->rr_depth;
 	pst.order = (flags & RN_PT_ORDER_NEAREST) ? kOrderNearest : kOrderReference;
+	if (flags & RN_PT_LBVH) { // the GPU-built tree, nearest child first
+		if (!s->lbvh_ready) {
+			set_last_error("render: RN_PT_LBVH needs rn_pt_scene_build_lbvh first");
+			return RN_ERR_INVALID_ARGUMENT;
+		}
+		ps.sv = s->lbvh_view;
+		pst.order = kOrderNearest;
+	}
 	pst.seed = st->seed;
 	pst.sample_offset = st->sample_offset;
 	for (int a = 0; a < 3; a++)

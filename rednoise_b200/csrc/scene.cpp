@@ -5,6 +5,7 @@
 #include <new>
 #include <string>
 
+#include "lbvh.hpp"
 #include "scene_impl.hpp"
 
 namespace rnb {
@@ -402,6 +403,72 @@ rn_status rn_pt_scene_dump_bvh(rn_scene *scene, int *order, int *node_count, flo
 	return RN_OK;
 }
 
+rn_status rn_pt_scene_build_lbvh(rn_scene *scene, void *stream, double *build_ms) {
+	if (!scene) {
+		set_last_error("rn_pt_scene_build_lbvh: NULL scene");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	rn_status st = rn_pt_scene_prepare(scene);
+	if (st != RN_OK)
+		return st;
+	cudaStream_t cs = pick_stream(scene, stream);
+	std::lock_guard<std::mutex> lock(scene->scratch_mu);
+	const int n = static_cast<int>(scene->tris.size());
+	const auto t0 = std::chrono::steady_clock::now();
+	const size_t vbytes = (scene->tris.v.size() * sizeof(float) + 255) & ~size_t(255);
+	const size_t sbytes = lbvh_scratch_bytes(n);
+	RNB_CUDA(scene->scratch.ensure(vbytes + sbytes));
+	float *d_v9 = scene->scratch.as<float>();
+	RNB_CUDA(cudaMemcpyAsync(d_v9, scene->tris.v.data(), scene->tris.v.size() * sizeof(float), cudaMemcpyHostToDevice,
+	                         cs));
+	RNB_CUDA(scene->d_lbvh_nodes.ensure(static_cast<size_t>(n > 1 ? n - 1 : 1) * 4 * sizeof(float4)));
+	RNB_CUDA(scene->d_lbvh_tris.ensure(static_cast<size_t>(n) * 3 * sizeof(float4)));
+	LbvhResult res{};
+	RNB_CUDA(lbvh_build(d_v9, n, scene->scratch.as<char>() + vbytes, sbytes, scene->d_lbvh_nodes.as<float4>(),
+	                    scene->d_lbvh_tris.as<float4>(), res, cs));
+	if (res.depth > kStack - 2) {
+		scene->lbvh_ready = false;
+		set_last_error("rn_pt_scene_build_lbvh: the tree is deeper than the traversal stack (" +
+		               std::to_string(res.depth) + " levels)");
+		return RN_ERR_UNSUPPORTED;
+	}
+	SceneView v{};
+	v.nodes = scene->d_lbvh_nodes.as<float4>();
+	v.nodes4 = nullptr;
+	v.tris = scene->d_lbvh_tris.as<float4>();
+	for (int a = 0; a < 3; a++) {
+		v.root_lo[a] = res.root_lo[a];
+		v.root_hi[a] = res.root_hi[a];
+	}
+	v.root_ref = res.root_ref;
+	v.root4_ref = 0;
+	v.n_tris = n;
+	scene->lbvh_view = v;
+	scene->lbvh_depth = res.depth;
+	scene->lbvh_ready = true;
+	if (build_ms)
+		*build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+	return RN_OK;
+}
+
+// The tree a query runs on: the GPU-built one for RN_PT_LBVH (which implies
+// nearest-first order), else the reference tree.
+static rn_status query_view(rn_scene *scene, unsigned flags, const char *what, SceneView &view, int &order) {
+	order = (flags & RN_PT_ORDER_NEAREST) ? kOrderNearest : kOrderReference;
+	view = scene->view;
+	if (flags & RN_PT_LBVH) {
+		if (!scene->lbvh_ready) {
+			set_last_error(std::string(what) + ": RN_PT_LBVH needs rn_pt_scene_build_lbvh first");
+			return RN_ERR_INVALID_ARGUMENT;
+		}
+		view = scene->lbvh_view;
+		order = kOrderNearest;
+	}
+	if (flags & RN_PT_WIDTH2)
+		view.nodes4 = nullptr;
+	return RN_OK;
+}
+
 rn_status rn_pt_trace_closest(rn_scene *scene, int n, const float *origins, const float *directions, const int *ignore,
                               unsigned flags, void *stream, int *tri, float *t, float *u, float *v) {
 	if (!scene || n < 0 || (n > 0 && (!origins || !directions || !tri))) {
@@ -411,11 +478,12 @@ rn_status rn_pt_trace_closest(rn_scene *scene, int n, const float *origins, cons
 	rn_status st = rn_pt_scene_prepare(scene);
 	if (st != RN_OK || n == 0)
 		return st;
-	const int order = (flags & RN_PT_ORDER_NEAREST) ? kOrderNearest : kOrderReference;
+	int order = kOrderReference;
+	SceneView view;
+	st = query_view(scene, flags, "rn_pt_trace_closest", view, order);
+	if (st != RN_OK)
+		return st;
 	cudaStream_t cs = pick_stream(scene, stream);
-	SceneView view = scene->view;
-	if (flags & RN_PT_WIDTH2)
-		view.nodes4 = nullptr;
 	std::lock_guard<std::mutex> lock(scene->scratch_mu);
 	const size_t nn = static_cast<size_t>(n);
 	RNB_CUDA(scene->scratch.ensure(nn * 4 * 13 + 256 * 12));
@@ -455,10 +523,12 @@ rn_status rn_pt_trace_any(rn_scene *scene, int n, const float *origins, const fl
 	rn_status st = rn_pt_scene_prepare(scene);
 	if (st != RN_OK || n == 0)
 		return st;
+	int order = kOrderReference;
+	SceneView view;
+	st = query_view(scene, flags, "rn_pt_trace_any", view, order);
+	if (st != RN_OK)
+		return st;
 	cudaStream_t cs = pick_stream(scene, stream);
-	SceneView view = scene->view;
-	if (flags & RN_PT_WIDTH2)
-		view.nodes4 = nullptr;
 	std::lock_guard<std::mutex> lock(scene->scratch_mu);
 	const size_t nn = static_cast<size_t>(n);
 	RNB_CUDA(scene->scratch.ensure(nn * 4 * 10 + 256 * 8));

@@ -30,6 +30,11 @@ struct rn_scene {
 	cudaStream_t stream = nullptr;
 	rnb::DevBuf d_nodes, d_nodes4, d_tris, d_ref_shade, d_phys_shade, d_emitters;
 	rnb::DevBuf d_ref_geom; // ray-traced renderer: vertices and vertex normals, uploaded on first use
+	// GPU-built linear BVH (rn_pt_scene_build_lbvh), selected by RN_PT_LBVH
+	rnb::DevBuf d_lbvh_nodes, d_lbvh_tris;
+	rnb::SceneView lbvh_view{};
+	bool lbvh_ready = false;
+	int lbvh_depth = 0;
 	bool ref_geom_ready = false;
 	rnb::DevBuf d_status; // error word for asynchronous (device-pointer) calls
 	rnb::SceneView view{};
