@@ -50,10 +50,10 @@ def parse():
     p.add_argument("--integrator", default="auto", choices=["auto", "megakernel", "wavefront"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-grad", action="store_true", help="skip the gradient-vs-primal timing")
-    p.add_argument("--workload", default="frame", choices=["frame", "batch64", "inverse", "raytraced", "photon"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batch64", "inverse", "raytraced", "photon", "lbvh"],
                    help="frame: the 1.31M-triangle 1080p frame (the bench line); batch64: 64 scenes per "
                         "launch; inverse: 16-view albedo recovery; raytraced: Whitted ray tracing; "
-                        "photon: photon mapping")
+                        "photon: photon mapping; lbvh: the GPU-built BVH")
     p.add_argument("--inverse-steps", type=int, default=200)
     return p.parse_args()
 
@@ -771,6 +771,42 @@ def run_photon(args):
     print(json.dumps(line), flush=True)
 
 
+def run_lbvh(args):
+    """The GPU-built linear BVH on the 1.31M-triangle scene: build time (with the
+    vertex upload) against the reference-tree build on the host threads, and the
+    bench frame rendered on each tree (nearest-first traversal on both)."""
+    import torch
+
+    import rednoise_b200 as rn
+    from rednoise_b200 import scenes
+
+    torch.cuda.set_device(0)
+    sc = scenes.icosphere_scene(level=args.level)
+    s = rn.Scene.from_arrays(sc["vertices"], albedo=sc["albedo"], emission=sc["emission"],
+                             material=sc["material"], material_param=sc["material_param"])
+    s.prepare()
+    host_ms = s.info()["build_ms"]
+    builds = [s.build_lbvh() for _ in range(args.warmup + args.steps)][args.warmup:]
+    W, H, spp = args.width, args.height, args.spp
+    c = scenes.camera(W, H)
+    cam = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], W, H)
+    st = rn.Settings.make(spp=spp, max_depth=args.depth, rr_depth=args.rr, seed=1)
+    rates = {}
+    for name, kw in (("reference_tree_nearest", dict(nearest_first=True)), ("lbvh", dict(lbvh=True))):
+        s.autotune(cam, st, nearest_first=True) if name != "lbvh" else None
+        s.render_physical(cam, st, **kw)
+        t0 = time.perf_counter()
+        s.render_physical(cam, st, **kw)
+        rates[name] = W * H * spp / (time.perf_counter() - t0)
+    line = {"metric": "ms per BVH build (1.31M triangles)", "value": float(np.median(builds)), "unit": "ms",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "icosphere-cornell-1.31M-tris: GPU linear BVH build, upload included"},
+            "reference_tree_host_build_ms": host_ms,
+            "frame_samples_per_s": rates}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -783,6 +819,8 @@ def main():
         run_raytraced(args)
     elif args.workload == "photon":
         run_photon(args)
+    elif args.workload == "lbvh":
+        run_lbvh(args)
     else:
         run_ours(args)
 
