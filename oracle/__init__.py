@@ -65,6 +65,8 @@ def ref() -> ctypes.CDLL:
             "refsh_bloom": (None, [vp, ci, ci, cf, cf]),
             "refsh_fxaa": (None, [vp, ci, ci]),
             "refsh_accum": (None, [ci, vp, ci, ci, vp]),
+            "refsh_render_bidirectional": (None, [vp, ci, ci, cf, vp, vp, ci, cf, vp]),
+            "refsh_render_metropolis": (None, [vp, ci, ci, cf, vp, vp, ci, cf, vp]),
             "rn_scene_load_obj": (vp, [ctypes.c_char_p, cf]),
             "rn_scene_free": (None, [vp]),
             "rn_render": (ci, [vp, ci, ci, ci, cf, ci, vp]),
@@ -96,6 +98,10 @@ def orc() -> ctypes.CDLL:
             "orc_pt_count": (None, [vp, vp, ci, ci, ci, ci, ci, ctypes.c_ulonglong, ctypes.c_uint, vp, ci, vp, vp]),
             "orc_pt_backward": (None, [vp, vp, ci, ci, ci, ci, ci, ctypes.c_ulonglong, ctypes.c_uint, vp, vp, ci,
                                        vp, vp]),
+            "orc_bdpt_render": (None, [vp, vp, vp, ci, ci, ci, ci, cf, vp, vp, ci, cf, ci, ctypes.c_ulonglong, ci,
+                                       vp, vp]),
+            "orc_mlt_render": (None, [vp, vp, vp, ci, ci, cf, vp, vp, ctypes.c_longlong, ci, ci, ctypes.c_ulonglong,
+                                      cf, ci, vp, vp, vp]),
         }
         for k, (r, a) in sig.items():
             getattr(lib, k).restype = r
@@ -195,6 +201,24 @@ class RefModel:
         out = np.zeros((h, w), np.uint32)
         ref().refsh_render_photon_mapped(self.h, w, h, focal, P(pos), P(target), int(num_photons), int(gather_rays),
                                          0 if lt is None else lt.shape[0], P(lt), P(out))
+        return out
+
+    def render_bidirectional(self, w, h, samples=64, exposure=40.0, focal=2.0, pos=(0, 0, 4),
+                             target=(0, 0, 0)) -> np.ndarray:
+        """The reference renderBidirectional (src/BDPT.cpp:65-144): 0xAARRGGBB canvas."""
+        pos = np.asarray(pos, np.float32)
+        target = np.asarray(target, np.float32)
+        out = np.zeros((h, w), np.uint32)
+        ref().refsh_render_bidirectional(self.h, w, h, focal, P(pos), P(target), int(samples), float(exposure), P(out))
+        return out
+
+    def render_metropolis(self, w, h, mutations=4000000, exposure=16.0, focal=2.0, pos=(0, 0, 4),
+                          target=(0, 0, 0)) -> np.ndarray:
+        """The reference renderMetropolis (src/Metropolis.cpp:85-192): 0xAARRGGBB canvas."""
+        pos = np.asarray(pos, np.float32)
+        target = np.asarray(target, np.float32)
+        out = np.zeros((h, w), np.uint32)
+        ref().refsh_render_metropolis(self.h, w, h, focal, P(pos), P(target), int(mutations), float(exposure), P(out))
         return out
 
     def bvh(self):
@@ -325,6 +349,36 @@ class OrcBvh:
         orc().orc_render_reference(self.h, P(nrm), P(mat), P(col), P(rough), w, h, y0, y1, focal, P(pos), P(target),
                                    samples, max_depth, 0 if lt is None else lt.shape[0], P(lt), P(out), P(mean))
         return (out, mean) if want_mean else out
+
+    def render_bidirectional(self, normal, rgb, w, h, samples, exposure=40.0, stream=0, seed=0, y0=0, y1=None,
+                             focal=2.0, pos=(0, 0, 4), target=(0, 0, 0), rtl=True, want_acc=False):
+        """The restated bidirectional estimator (stream 0: the reference's per-row
+        mt19937 streams; 1: Philox under seed). Rows [y0, y1)."""
+        y1 = h if y1 is None else y1
+        nrm = np.ascontiguousarray(normal, np.float32)
+        col = np.ascontiguousarray(rgb, np.int32)
+        pos = np.asarray(pos, np.float32)
+        target = np.asarray(target, np.float32)
+        out = np.zeros((y1 - y0, w), np.uint32)
+        acc = np.zeros((y1 - y0, w, 3), np.float32) if want_acc else None
+        orc().orc_bdpt_render(self.h, P(nrm), P(col), w, h, y0, y1, focal, P(pos), P(target), int(samples),
+                              float(exposure), int(stream), int(seed), int(bool(rtl)), P(out), P(acc))
+        return (out, acc) if want_acc else out
+
+    def render_metropolis(self, normal, rgb, w, h, mutations, chains, bootstrap=100000, seed=0, exposure=16.0,
+                          focal=2.0, pos=(0, 0, 4), target=(0, 0, 0), rtl=True):
+        """The restated many-chain Metropolis sampler: (canvas, unscaled deposits (h, w, 3), b)."""
+        nrm = np.ascontiguousarray(normal, np.float32)
+        col = np.ascontiguousarray(rgb, np.int32)
+        pos = np.asarray(pos, np.float32)
+        target = np.asarray(target, np.float32)
+        img = np.zeros((h, w, 3), np.float32)
+        b = ctypes.c_double(0.0)
+        out = np.zeros((h, w), np.uint32)
+        orc().orc_mlt_render(self.h, P(nrm), P(col), w, h, focal, P(pos), P(target), int(mutations), int(chains),
+                             int(bootstrap), int(seed), float(exposure), int(bool(rtl)), P(img), ctypes.byref(b),
+                             P(out))
+        return out, img, b.value
 
     def __del__(self):
         try:

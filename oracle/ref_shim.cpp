@@ -9,6 +9,8 @@
 //   * renderPathTraced                               (src/Renderer.cpp:1119-1170)
 //   * renderRaytraced                                (src/Renderer.cpp:909-948)
 //   * renderPhotonMapped                             (src/Renderer.cpp:1300-1349)
+//   * renderBidirectional                            (src/BDPT.cpp:65-144)
+//   * renderMetropolis                               (src/Metropolis.cpp:85-192)
 //   * loadOBJ                                        (src/ObjLoader.cpp:102-214)
 // BVH's node array and triangle order are private in the reference; this shim
 // exposes them (for dumping the tree it built) by compiling BVH.h with
@@ -21,6 +23,9 @@
 #define private public
 #include "BVH.h"
 #undef private
+
+#include "BDPT.h"
+#include "Metropolis.h"
 
 #include "Camera.h"
 #include "Geometry.h"
@@ -276,6 +281,27 @@ void refsh_render_photon_mapped(const void *model, int w, int h, float focal, co
 	cam.lookAt(glm::vec3(target3[0], target3[1], target3[2]));
 	Canvas canvas(static_cast<size_t>(w), static_cast<size_t>(h));
 	renderPhotonMapped(m->tris, cam, canvas, num_photons, unpackLights(n_lights, lights), {}, gather_rays);
+	std::memcpy(out, canvas.pixels.data(), sizeof(uint32_t) * static_cast<size_t>(w) * static_cast<size_t>(h));
+}
+
+// renderBidirectional / renderMetropolis with the camera built as above.
+void refsh_render_bidirectional(const void *model, int w, int h, float focal, const float *pos3, const float *target3,
+                                int samples, float exposure, uint32_t *out) {
+	const Model *m = static_cast<const Model *>(model);
+	Camera cam(w, h, focal, glm::vec3(pos3[0], pos3[1], pos3[2]));
+	cam.lookAt(glm::vec3(target3[0], target3[1], target3[2]));
+	Canvas canvas(static_cast<size_t>(w), static_cast<size_t>(h));
+	renderBidirectional(m->tris, cam, canvas, samples, exposure);
+	std::memcpy(out, canvas.pixels.data(), sizeof(uint32_t) * static_cast<size_t>(w) * static_cast<size_t>(h));
+}
+
+void refsh_render_metropolis(const void *model, int w, int h, float focal, const float *pos3, const float *target3,
+                             int mutations, float exposure, uint32_t *out) {
+	const Model *m = static_cast<const Model *>(model);
+	Camera cam(w, h, focal, glm::vec3(pos3[0], pos3[1], pos3[2]));
+	cam.lookAt(glm::vec3(target3[0], target3[1], target3[2]));
+	Canvas canvas(static_cast<size_t>(w), static_cast<size_t>(h));
+	renderMetropolis(m->tris, cam, canvas, mutations, exposure);
 	std::memcpy(out, canvas.pixels.data(), sizeof(uint32_t) * static_cast<size_t>(w) * static_cast<size_t>(h));
 }
 

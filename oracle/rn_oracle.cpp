@@ -1274,3 +1274,430 @@ void orc_pt_render(const void *h, const float *cam10, int w, int hgt, int spp, i
 }
 
 } // extern "C"
+
+// ---- bidirectional path tracing and PSSMLT ---------------------------------------
+// Restated from src/BDPT.cpp:8-144 and src/Metropolis.cpp:8-192: diffuse-only
+// estimators lit by the fixed 0.36 x 0.36 ceiling patch at (0, 0.33, 0) facing -y,
+// Le = 30. Two random sources drive the bidirectional estimator:
+//   * stream 0: the reference's own -- std::mt19937(9871 + y) per image row, drawn
+//     through uniform_real_distribution<float>, in the reference's draw order;
+//   * stream 1: counter-based -- Philox-4x32-10 keyed by the seed, counter
+//     (pixel, sample, block, 0), each 32-bit word mapped as the reference maps an
+//     engine output (float(x) / 2^32, clamped below 1).
+// The Metropolis sampler restates the reference's mutation and deposition rules
+// for the many-chain GPU scheme: chains start from bootstrap paths drawn with
+// probability proportional to luminance, and every random number comes from a
+// Philox stream (see orc_mlt_render).
+// rtl != 0 evaluates the two random arguments of one glm::vec3 constructor or
+// cosineHemisphere call right to left, as GCC's x86-64 code does.
+namespace {
+
+const float kGiPi = 3.14159265f;
+const float kGiEps = 1e-3f;
+const float kGiLightHalf = 0.18f;
+const float kGiLightArea = (2.0f * kGiLightHalf) * (2.0f * kGiLightHalf);
+const float kGiLe = 30.0f;
+const int kGiMaxDepth = 4;
+const int kMltMaxDims = 2 + 4 * kGiMaxDepth;
+
+struct GiScene {
+	const Bvh *bvh;
+	std::vector<V3> normal;
+	std::vector<V3> albedo; // vec3(colour) / 255
+};
+
+struct GiCam {
+	V3 pos, right, up, fwd;
+	float f;
+};
+
+GiCam gi_cam(float focal, const float *pos3, const float *target3) {
+	GiCam c;
+	c.pos = mk(pos3[0], pos3[1], pos3[2]);
+	V3 tgt = mk(target3[0], target3[1], target3[2]);
+	c.fwd = normalize(c.pos - tgt);
+	c.right = normalize(cross(mk(0, 1, 0), c.fwd));
+	c.up = cross(c.fwd, c.right);
+	c.f = focal * 150.0f;
+	return c;
+}
+
+// faceViewer (src/BDPT.cpp:34-36, src/Metropolis.cpp:38-40)
+V3 gi_face(V3 n, V3 d) { return dot(n, d) < 0.0f ? n : -n; }
+
+// cosineHemisphere on two given uniforms (src/Metropolis.cpp:42-50)
+V3 gi_cosine(V3 n, float u1, float u2) {
+	float r = std::sqrt(u1), th = 2.0f * kGiPi * u2;
+	float x = r * std::cos(th), y = r * std::sin(th), z = std::sqrt(std::max(0.0f, 1.0f - u1));
+	V3 up = std::fabs(n.z) < 0.99f ? mk(0, 0, 1) : mk(1, 0, 0);
+	V3 t = normalize(cross(up, n)), b = cross(n, t);
+	return normalize(t * x + b * y + n * z);
+}
+
+// one engine word -> uniform_real_distribution<float>(0, 1)
+float gi_canon(uint32_t x) {
+	float c = static_cast<float>(x) / 4294967296.0f;
+	if (c >= 1.0f)
+		c = std::nextafter(1.0f, 0.0f);
+	return c * (1.0f - 0.0f) + 0.0f;
+}
+
+uint32_t u4_word(orc::U4 v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+
+struct MtDraw {
+	Rng rng;
+	explicit MtDraw(uint32_t s) : rng(s) {}
+	float operator()() { return U01(rng); }
+};
+
+// Philox words of counter (a, b, block, tag) under the key (seed), consumed in order.
+struct CtrDraw {
+	uint32_t a, b, tag, k0, k1;
+	int n = 0;
+	orc::U4 blk{};
+	float operator()() {
+		if ((n & 3) == 0)
+			blk = orc::philox4x32_10(orc::U4{a, b, static_cast<uint32_t>(n >> 2), tag}, k0, k1);
+		return gi_canon(u4_word(blk, n++ & 3));
+	}
+};
+
+struct GVert {
+	V3 p, n, albedo, beta;
+	bool light;
+};
+
+// tracePath (src/BDPT.cpp:43-61)
+template <class D> int gi_subpath(const GiScene &s, V3 o, V3 d, V3 beta, GVert *out, D &draw) {
+	int k = 0;
+	for (int depth = 0; depth < kGiMaxDepth; depth++) {
+		Hit h = intersect(*s.bvh, o, d, -1, nullptr);
+		if (!h.hit)
+			return k;
+		GVert v;
+		v.p = h.point;
+		v.n = gi_face(s.normal[h.idx], d);
+		v.albedo = s.albedo[h.idx];
+		v.beta = beta;
+		v.light = false;
+		out[k++] = v;
+		float u1 = draw(), u2 = draw();
+		V3 nd = gi_cosine(v.n, u1, u2);
+		beta = beta * v.albedo;
+		o = v.p + kGiEps * nd;
+		d = nd;
+	}
+	return k;
+}
+
+// One sample of renderBidirectional's pixel loop (src/BDPT.cpp:89-134), added to acc.
+template <class D>
+void bdpt_sample(const GiScene &s, const GiCam &c, int x, int y, int W, int H, D &draw, bool rtl, V3 &acc) {
+	float a0 = draw(), a1 = draw();
+	float ux = rtl ? a1 : a0, uy = rtl ? a0 : a1;
+	V3 dc = mk((static_cast<float>(x) + ux - static_cast<float>(W) / 2.0f) / c.f,
+	           -(static_cast<float>(y) + uy - static_cast<float>(H) / 2.0f) / c.f, -1.0f);
+	V3 dir = normalize(c.right * dc.x + c.up * dc.y + c.fwd * dc.z);
+	GVert cam[kGiMaxDepth];
+	int nc = gi_subpath(s, c.pos, dir, mk(1, 1, 1), cam, draw);
+	float b0 = draw(), b1 = draw();
+	float lx = rtl ? b1 : b0, lz = rtl ? b0 : b1;
+	V3 lp = mk(0.0f, 0.33f, 0.0f) + mk((lx * 2.0f - 1.0f) * kGiLightHalf, 0.0f, (lz * 2.0f - 1.0f) * kGiLightHalf);
+	const V3 ln = mk(0.0f, -1.0f, 0.0f);
+	const V3 le = mk(kGiLe, kGiLe, kGiLe) * kGiLightArea;
+	GVert lv[kGiMaxDepth + 1];
+	lv[0] = GVert{lp, ln, mk(0, 0, 0), le, true};
+	float d1 = draw(), d2 = draw();
+	V3 ldir = gi_cosine(ln, d1, d2);
+	int nl = 1 + gi_subpath(s, lp + kGiEps * ldir, ldir, le, lv + 1, draw);
+	for (int i = 0; i < nc; i++) {
+		const GVert &cv = cam[i];
+		for (int j = 0; j < nl; j++) {
+			const GVert &l = lv[j];
+			V3 d = l.p - cv.p;
+			float dist2 = dot(d, d);
+			float dist = std::sqrt(dist2);
+			d = d / dist;
+			float cosC = dot(cv.n, d);
+			float cosL = dot(l.n, -d);
+			if (cosC <= 0.0f || cosL <= 0.0f)
+				continue;
+			if (occluded(*s.bvh, cv.p + cv.n * kGiEps, d, dist - 2.0f * kGiEps, -1, nullptr))
+				continue;
+			float G = cosC * cosL / dist2;
+			V3 fC = cv.albedo / kGiPi;
+			V3 contrib = cv.beta * fC * G * l.beta;
+			if (!l.light)
+				contrib = contrib * (l.albedo / kGiPi);
+			float w = 1.0f / static_cast<float>(i + j + 2);
+			acc = acc + contrib * w;
+		}
+	}
+}
+
+int cvt_i(float v) {
+	return (v >= -2147483648.0f && v < 2147483648.0f) ? static_cast<int>(v) : static_cast<int>(0x80000000u);
+}
+
+// Reinhard and the 8-bit pack of src/BDPT.cpp:136-141 and src/Metropolis.cpp:184-189.
+uint32_t gi_pack(V3 c) {
+	c = 255.0f * mk(c.x / (c.x + 1.0f), c.y / (c.y + 1.0f), c.z / (c.z + 1.0f));
+	int r = std::min(255, cvt_i(c.x)), g = std::min(255, cvt_i(c.y)), b = std::min(255, cvt_i(c.z));
+	return (255u << 24) | ((static_cast<uint32_t>(r) & 0xFF) << 16) | ((static_cast<uint32_t>(g) & 0xFF) << 8) |
+	       (static_cast<uint32_t>(b) & 0xFF);
+}
+
+float luminance(V3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+
+// The primary-sample vector of one Metropolis state (src/Metropolis.cpp:26-36):
+// coordinates past n are drawn on first use from `ext`.
+template <class E> struct MltSampler {
+	float *u;
+	int *n;
+	E &ext;
+	int idx = 0;
+	float next() {
+		if (idx >= *n) {
+			u[*n] = ext(idx);
+			(*n)++;
+		}
+		return u[idx++];
+	}
+};
+
+// tracePath with next-event estimation (src/Metropolis.cpp:53-81)
+template <class S> V3 mlt_trace(const GiScene &s, S &smp, V3 o, V3 d, bool rtl) {
+	V3 L = mk(0, 0, 0), beta = mk(1, 1, 1);
+	const V3 ln = mk(0.0f, -1.0f, 0.0f);
+	for (int depth = 0; depth < kGiMaxDepth; depth++) {
+		Hit h = intersect(*s.bvh, o, d, -1, nullptr);
+		if (!h.hit)
+			break;
+		V3 n = gi_face(s.normal[h.idx], d);
+		V3 albedo = s.albedo[h.idx];
+		V3 point = h.point;
+		float a0 = smp.next(), a1 = smp.next();
+		float ux = rtl ? a1 : a0, uz = rtl ? a0 : a1;
+		V3 lp = mk(0.0f, 0.33f, 0.0f) + mk((ux * 2.0f - 1.0f) * kGiLightHalf, 0.0f, (uz * 2.0f - 1.0f) * kGiLightHalf);
+		V3 toL = lp - point;
+		float dist = length(toL);
+		toL = toL / dist;
+		float cosS = dot(n, toL), cosL = dot(ln, -toL);
+		if (cosS > 0.0f && cosL > 0.0f && !occluded(*s.bvh, point + n * kGiEps, toL, dist - 2.0f * kGiEps, -1, nullptr)) {
+			float G = cosS * cosL / (dist * dist);
+			L = L + beta * (albedo / kGiPi) * G * mk(kGiLe, kGiLe, kGiLe) * kGiLightArea;
+		}
+		float c0 = smp.next(), c1 = smp.next();
+		V3 nd = gi_cosine(n, rtl ? c1 : c0, rtl ? c0 : c1);
+		beta = beta * albedo;
+		o = point + kGiEps * nd;
+		d = nd;
+	}
+	return L;
+}
+
+// eval (src/Metropolis.cpp:96-105): pixel from the first two coordinates.
+template <class S> V3 mlt_eval(const GiScene &s, const GiCam &c, int W, int H, S &smp, bool rtl, int &pixel) {
+	float fx = smp.next(), fy = smp.next();
+	int px = std::min(W - 1, static_cast<int>(fx * static_cast<float>(W)));
+	int py = std::min(H - 1, static_cast<int>(fy * static_cast<float>(H)));
+	pixel = py * W + px;
+	V3 dc = mk((static_cast<float>(px) + 0.5f - static_cast<float>(W) / 2.0f) / c.f,
+	           -(static_cast<float>(py) + 0.5f - static_cast<float>(H) / 2.0f) / c.f, -1.0f);
+	V3 dir = normalize(c.right * dc.x + c.up * dc.y + c.fwd * dc.z);
+	return mlt_trace(s, smp, c.pos, dir, rtl);
+}
+
+// Standard normal from two uniforms (Box and Muller 1958), evaluated in double.
+float gi_normal(float u1, float u2) {
+	return static_cast<float>(std::sqrt(-2.0 * std::log(1.0 - static_cast<double>(u1))) *
+	                          std::cos(6.283185307179586 * static_cast<double>(u2)));
+}
+
+GiScene gi_scene(const void *bvh, const float *normal3, const int *rgb) {
+	GiScene s;
+	s.bvh = static_cast<const Bvh *>(bvh);
+	const size_t n = s.bvh->tris.size();
+	s.normal.resize(n);
+	s.albedo.resize(n);
+	for (size_t i = 0; i < n; i++) {
+		s.normal[i] = mk(normal3[3 * i], normal3[3 * i + 1], normal3[3 * i + 2]);
+		s.albedo[i] = mk(static_cast<float>(rgb[3 * i]), static_cast<float>(rgb[3 * i + 1]),
+		                 static_cast<float>(rgb[3 * i + 2])) /
+		              255.0f;
+	}
+	return s;
+}
+
+} // namespace
+
+extern "C" {
+
+// renderBidirectional over rows [y0, y1) of a w x h image; camera as orc_render_reference.
+// stream 0: the reference's per-row mt19937 streams; 1: Philox under `seed`.
+// argb: w x (y1 - y0); acc (may be null): 3 floats per pixel, accum * (exposure / samples).
+void orc_bdpt_render(const void *bvh, const float *normal3, const int *rgb, int w, int h, int y0, int y1, float focal,
+                     const float *pos3, const float *target3, int samples, float exposure, int stream,
+                     unsigned long long seed, int rtl, uint32_t *argb, float *acc) {
+	const GiScene s = gi_scene(bvh, normal3, rgb);
+	const GiCam c = gi_cam(focal, pos3, target3);
+#pragma omp parallel for schedule(dynamic, 1)
+	for (int y = y0; y < y1; y++) {
+		MtDraw mt(static_cast<uint32_t>(9871 + y));
+		for (int x = 0; x < w; x++) {
+			V3 sum = mk(0, 0, 0);
+			for (int k = 0; k < samples; k++) {
+				if (stream == 0) {
+					bdpt_sample(s, c, x, y, w, h, mt, rtl != 0, sum);
+				} else {
+					CtrDraw d{static_cast<uint32_t>(y * w + x), static_cast<uint32_t>(k), 0u,
+					          static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32)};
+					bdpt_sample(s, c, x, y, w, h, d, rtl != 0, sum);
+				}
+			}
+			V3 col = sum * (exposure / static_cast<float>(samples));
+			size_t i = static_cast<size_t>(y - y0) * static_cast<size_t>(w) + static_cast<size_t>(x);
+			argb[i] = gi_pack(col);
+			if (acc) {
+				acc[3 * i] = col.x;
+				acc[3 * i + 1] = col.y;
+				acc[3 * i + 2] = col.z;
+			}
+		}
+	}
+}
+
+// The many-chain Metropolis sampler of rednoise_b200 (counter-based random numbers):
+//  1. bootstrap: `bootstrap` independent paths, path i drawing coordinate m from
+//     Philox counter (i, 0, m / 4, 1) word m % 4; their luminances are summed in
+//     1024 contiguous segments (double), then segment by segment: total and b.
+//  2. chain c starts at the bootstrap path whose inclusive luminance prefix first
+//     exceeds xi * total, xi from counter (c, 0, 0, 2) word 0.
+//  3. chain c runs mutations / chains steps (one more for c < mutations % chains);
+//     step t draws from counter (c, t, k / 4, 3) word k % 4: k = 0 large-step test,
+//     1 acceptance test, 2 + 2m and 3 + 2m coordinate m's mutation (a fresh uniform,
+//     or Box-Muller for the small step), 40 + m coordinate m's first draw.
+// image (w*h*3) receives the deposits (unscaled); b_out the bootstrap mean luminance.
+// argb (may be null): the reference's canvas (scale b * w * h / mutations, exposure, Reinhard).
+void orc_mlt_render(const void *bvh, const float *normal3, const int *rgb, int w, int h, float focal,
+                    const float *pos3, const float *target3, long long mutations, int chains, int bootstrap,
+                    unsigned long long seed, float exposure, int rtl, float *image, double *b_out, uint32_t *argb) {
+	const GiScene s = gi_scene(bvh, normal3, rgb);
+	const GiCam c = gi_cam(focal, pos3, target3);
+	const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
+	const bool r = rtl != 0;
+	std::vector<float> lum(static_cast<size_t>(bootstrap));
+	std::vector<int> len(static_cast<size_t>(bootstrap));
+	for (int i = 0; i < bootstrap; i++) {
+		float u[kMltMaxDims];
+		int n = 0, pix = 0;
+		CtrDraw d{static_cast<uint32_t>(i), 0u, 1u, k0, k1};
+		auto ext = [&](int) { return d(); };
+		MltSampler<decltype(ext)> smp{u, &n, ext};
+		lum[i] = luminance(mlt_eval(s, c, w, h, smp, r, pix));
+		len[i] = n;
+	}
+	const int seg = (bootstrap + 1023) / 1024;
+	std::vector<double> cdf(static_cast<size_t>(bootstrap));
+	double total = 0.0;
+	for (int t = 0; t < 1024; t++) {
+		double run = total;
+		for (int i = t * seg; i < std::min(bootstrap, (t + 1) * seg); i++) {
+			run += static_cast<double>(lum[i]);
+			cdf[i] = run;
+		}
+		double part = 0.0;
+		for (int i = t * seg; i < std::min(bootstrap, (t + 1) * seg); i++)
+			part += static_cast<double>(lum[i]);
+		total += part;
+	}
+	*b_out = total / static_cast<double>(bootstrap);
+	std::fill(image, image + 3 * static_cast<size_t>(w) * h, 0.0f);
+	if (total > 0.0) {
+		const float sigma = 0.02f, p_large = 0.3f;
+		for (int ch = 0; ch < chains; ch++) {
+			const float xi = gi_canon(orc::philox4x32_10(orc::U4{static_cast<uint32_t>(ch), 0u, 0u, 2u}, k0, k1).x);
+			const double target = static_cast<double>(xi) * total;
+			int lo = 0, hi = bootstrap - 1;
+			while (lo < hi) {
+				int mid = (lo + hi) / 2;
+				if (cdf[mid] > target)
+					hi = mid;
+				else
+					lo = mid + 1;
+			}
+			float cur[kMltMaxDims];
+			int cn = 0, cur_pix = 0;
+			{
+				CtrDraw d{static_cast<uint32_t>(lo), 0u, 1u, k0, k1};
+				for (int m = 0; m < len[lo]; m++)
+					cur[m] = d();
+				cn = len[lo];
+			}
+			auto never = [](int) { return 0.0f; };
+			MltSampler<decltype(never)> s0{cur, &cn, never};
+			V3 curL = mlt_eval(s, c, w, h, s0, r, cur_pix);
+			float curLum = luminance(curL);
+			const long long steps = mutations / chains + (ch < mutations % chains ? 1 : 0);
+			for (long long t = 0; t < steps; t++) {
+				const uint32_t tc = static_cast<uint32_t>(t);
+				auto W = [&](int k) {
+					orc::U4 v = orc::philox4x32_10(orc::U4{static_cast<uint32_t>(ch), tc, static_cast<uint32_t>(k >> 2), 3u},
+					                               k0, k1);
+					return gi_canon(u4_word(v, k & 3));
+				};
+				const bool large = W(0) < p_large;
+				float prop[kMltMaxDims];
+				int pn = cn;
+				for (int m = 0; m < cn; m++) {
+					if (large) {
+						prop[m] = W(2 + 2 * m);
+					} else {
+						float v = cur[m] + sigma * gi_normal(W(2 + 2 * m), W(3 + 2 * m));
+						v = v - std::floor(v);
+						prop[m] = v;
+					}
+				}
+				auto ext = [&](int m) { return W(40 + m); };
+				MltSampler<decltype(ext)> sp{prop, &pn, ext};
+				int prop_pix = 0;
+				V3 propL = mlt_eval(s, c, w, h, sp, r, prop_pix);
+				float propLum = luminance(propL);
+				float a = (curLum > 0.0f) ? std::min(1.0f, propLum / curLum) : 1.0f;
+				if (propLum > 0.0f) {
+					V3 dep = propL * (a / propLum);
+					image[3 * prop_pix] += dep.x;
+					image[3 * prop_pix + 1] += dep.y;
+					image[3 * prop_pix + 2] += dep.z;
+				}
+				if (curLum > 0.0f) {
+					V3 dep = curL * ((1.0f - a) / curLum);
+					image[3 * cur_pix] += dep.x;
+					image[3 * cur_pix + 1] += dep.y;
+					image[3 * cur_pix + 2] += dep.z;
+				}
+				if (W(1) < a) {
+					std::memcpy(cur, prop, sizeof(float) * static_cast<size_t>(pn));
+					cn = pn;
+					cur_pix = prop_pix;
+					curL = propL;
+					curLum = propLum;
+				}
+			}
+		}
+	}
+	if (argb) {
+		const float b = static_cast<float>(*b_out);
+		if (!(b > 0.0f)) {
+			std::fill(argb, argb + static_cast<size_t>(w) * h, 0u);
+			return;
+		}
+		const float scale = b * static_cast<float>(w) * static_cast<float>(h) / static_cast<float>(mutations);
+		for (size_t i = 0; i < static_cast<size_t>(w) * h; i++) {
+			V3 v = mk(image[3 * i], image[3 * i + 1], image[3 * i + 2]) * scale * exposure;
+			argb[i] = gi_pack(v);
+		}
+	}
+}
+
+} // extern "C"

@@ -145,3 +145,63 @@ def test_golden_render_is_reference_c_abi(assets):
                                   assets["cornell_roughness"], 64, 48, 4)
     rgba = np.stack([(canvas >> 16) & 255, (canvas >> 8) & 255, canvas & 255, canvas >> 24], -1).astype(np.uint8)
     assert np.array_equal(rgba, g)
+
+
+def _channels(canvas):
+    c = np.asarray(canvas, np.uint32)
+    return np.stack([(c >> 16) & 255, (c >> 8) & 255, c & 255], -1).astype(np.float64)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("w,h,spp,pos", [(40, 30, 4, (0, 0, 4)), (48, 36, 3, (0.3, 0.2, 3.5))])
+def test_oracle_bidirectional_matches_reference(assets, w, h, spp, pos):
+    """The restated renderBidirectional (reference per-row mt19937 streams) equals the
+    reference build's canvas bit for bit; with the two random constructor arguments
+    evaluated left to right instead it does not (GCC's order is right to left)."""
+    v9 = assets["cornell_v"]
+    m = oracle.RefModel.from_arrays(v9, assets["cornell_rgb"], assets["cornell_material"],
+                                    assets["cornell_roughness"], assets["cornell_normal"])
+    want = m.render_bidirectional(w, h, spp, pos=pos)
+    orc = oracle.OrcBvh(v9)
+    got = orc.render_bidirectional(assets["cornell_normal"], assets["cornell_rgb"], w, h, spp, pos=pos)
+    assert np.array_equal(want, got)
+    ltr = orc.render_bidirectional(assets["cornell_normal"], assets["cornell_rgb"], w, h, spp, pos=pos, rtl=False)
+    assert (ltr == want).mean() < 0.5
+    rows = orc.render_bidirectional(assets["cornell_normal"], assets["cornell_rgb"], w, h, spp, y0=5, y1=9, pos=pos)
+    assert np.array_equal(rows, want[5:9])
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+def test_oracle_bidirectional_counter_stream_estimates_the_same_image(assets):
+    """The counter-stream estimator converges to the reference's image: at 64 spp the
+    mean 8-bit level agrees within 1% and the per-pixel difference is noise-sized."""
+    v9 = assets["cornell_v"]
+    m = oracle.RefModel.from_arrays(v9, assets["cornell_rgb"], assets["cornell_material"],
+                                    assets["cornell_roughness"], assets["cornell_normal"])
+    want = _channels(m.render_bidirectional(32, 24, 64))
+    orc = oracle.OrcBvh(v9)
+    got = _channels(orc.render_bidirectional(assets["cornell_normal"], assets["cornell_rgb"], 32, 24, 64, stream=1,
+                                             seed=11))
+    assert abs(got.mean() - want.mean()) < 0.01 * want.mean()
+    assert np.abs(got - want).mean() < 4.0
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+def test_oracle_metropolis_estimates_the_reference_image(assets):
+    """The many-chain Metropolis restatement and the reference's 16-chain sampler
+    estimate the same image: equal mean level within 1.5%, per-pixel differences
+    within twice the reference's own run-to-run spread at 4x the mutations."""
+    v9 = assets["cornell_v"]
+    m = oracle.RefModel.from_arrays(v9, assets["cornell_rgb"], assets["cornell_material"],
+                                    assets["cornell_roughness"], assets["cornell_normal"])
+    w, h, muts = 32, 24, 200000
+    want = _channels(m.render_metropolis(w, h, muts))
+    want4 = _channels(m.render_metropolis(w, h, 4 * muts))
+    orc = oracle.OrcBvh(v9)
+    canvas, img, b = orc.render_metropolis(assets["cornell_normal"], assets["cornell_rgb"], w, h, muts, muts // 64,
+                                           bootstrap=20000, seed=5)
+    got = _channels(canvas)
+    assert b > 0 and img.sum() > 0
+    assert abs(got.mean() - want4.mean()) < 0.015 * want4.mean()
+    spread = np.abs(want - want4).mean()
+    assert np.abs(got - want4).mean() < 2.0 * spread + 1.0
