@@ -193,6 +193,40 @@ rn_status rn_pt_render_raytraced(rn_scene *scene, const rn_pt_ref_params *params
 rn_status rn_pt_render_photon_mapped(rn_scene *scene, const rn_pt_ref_params *params, int num_photons, int gather_rays,
                                      unsigned flags, void *stream, uint32_t *argb, unsigned *num_stored);
 
+/* Random-number streams of rn_pt_render_bidirectional. */
+#define RN_PT_RNG_REFERENCE 0 /* the reference's std::mt19937(9871 + y) per image row: the reference's canvas */
+#define RN_PT_RNG_COUNTER 1   /* Philox-4x32-10 per (pixel, sample) under `seed`: same estimator, fully parallel */
+
+/* Bidirectional path tracing with reference semantics (renderBidirectional,
+ * src/BDPT.cpp:65-144): per sample a camera subpath and a subpath from the fixed
+ * 0.36 x 0.36 ceiling emitter at (0, 0.33, 0) (Le = 30), both diffuse with up to four
+ * bounces, every camera vertex connected to every light vertex with a shadow ray and
+ * the uniform MIS weight 1 / (i + j + 2); then exposure, Reinhard and the 8-bit
+ * canvas. The reference's defaults are samples = 64, exposure = 40. Only the camera
+ * fields of params are used (width, height, position, target, focal_length, scale).
+ * argb: width*height pixels 0xAARRGGBB; rgb (may be NULL): width*height*3 floats,
+ * accum * exposure / samples before tone mapping. seed is used by RN_PT_RNG_COUNTER. */
+rn_status rn_pt_render_bidirectional(rn_scene *scene, const rn_pt_ref_params *params, int samples, float exposure,
+                                     int rng, unsigned long long seed, unsigned flags, void *stream, uint32_t *argb,
+                                     float *rgb);
+
+/* Primary-sample-space Metropolis light transport with reference semantics
+ * (renderMetropolis, src/Metropolis.cpp:85-192): the reference's diffuse path
+ * tracer with next-event estimation to the same emitter as a function of its random
+ * numbers, a bootstrap of `bootstrap` paths for the normalisation (the reference uses
+ * 100000), and `mutations` Markov-chain steps in total (reference default 4000000)
+ * with the reference's large-step (p = 0.3) and Gaussian small-step (sigma = 0.02)
+ * mutations, acceptance and expected-value deposits; exposure (reference default 16)
+ * and Reinhard onto the canvas. The steps are split over `chains` chains run in
+ * parallel (0: mutations / 64, at most 262144), each started from a bootstrap path
+ * drawn in proportion to its luminance; random numbers are Philox streams under
+ * `seed`. argb: width*height pixels; rgb (may be NULL): width*height*3 floats of
+ * the normalised radiance estimate before exposure; mean_luminance (may be NULL): the
+ * bootstrap's mean luminance b. Only the camera fields of params are used. */
+rn_status rn_pt_render_metropolis(rn_scene *scene, const rn_pt_ref_params *params, long long mutations, float exposure,
+                                  int chains, int bootstrap, unsigned long long seed, unsigned flags, void *stream,
+                                  uint32_t *argb, float *rgb, double *mean_luminance);
+
 /* ---- canvas post-processing (src/Renderer.cpp:1353-1470), reference semantics ----
  * Canvases are width*height pixels 0xAARRGGBB, processed in place; host arrays
  * unless flags has RN_PT_DEVICE_POINTERS. */

@@ -343,6 +343,78 @@ class Scene:
                                                             _ptr(mean)), "render_reference")
         return (canvas, mean) if want_mean else canvas
 
+    def _camera_params(self, width, height, position, target, focal_length, scale) -> "_native.RefParams":
+        p = _native.RefParams()
+        _native.load().rn_pt_ref_params_init(ctypes.byref(p), int(width), int(height), ctypes.c_float(4.0), 1)
+        p.position[:] = tuple(float(x) for x in position)
+        p.target[:] = tuple(float(x) for x in target)
+        p.focal_length = focal_length
+        p.scale = scale
+        return p
+
+    def render_bidirectional(
+        self,
+        width: int,
+        height: int,
+        samples: int = 64,
+        exposure: float = 40.0,
+        *,
+        rng: str = "reference",
+        seed: int = 0,
+        position: Sequence[float] = (0.0, 0.0, 4.0),
+        target: Sequence[float] = (0.0, 0.0, 0.0),
+        focal_length: float = 2.0,
+        scale: float = 150.0,
+        want_rgb: bool = False,
+    ):
+        """renderBidirectional semantics (src/BDPT.cpp:65-144): the Canvas as
+        (height, width) uint32 0xAARRGGBB. rng "reference" draws from the
+        reference's per-row std::mt19937 streams (the reference's canvas); "counter"
+        from Philox streams under seed. want_rgb adds the (height, width, 3) float
+        image before tone mapping."""
+        self._check_open()
+        if rng not in ("reference", "counter"):
+            raise ValueError("rng must be 'reference' or 'counter'")
+        p = self._camera_params(width, height, position, target, focal_length, scale)
+        canvas = np.empty((height, width), np.uint32)
+        rgb = np.empty((height, width, 3), np.float32) if want_rgb else None
+        mode = _native.RN_PT_RNG_REFERENCE if rng == "reference" else _native.RN_PT_RNG_COUNTER
+        _native.check(_native.load().rn_pt_render_bidirectional(self._handle, ctypes.byref(p), int(samples),
+                                                                ctypes.c_float(exposure), mode, int(seed), 0, None,
+                                                                _ptr(canvas), _ptr(rgb)), "render_bidirectional")
+        return (canvas, rgb) if want_rgb else canvas
+
+    def render_metropolis(
+        self,
+        width: int,
+        height: int,
+        mutations: int = 4000000,
+        exposure: float = 16.0,
+        *,
+        chains: int = 0,
+        bootstrap: int = 100000,
+        seed: int = 0,
+        position: Sequence[float] = (0.0, 0.0, 4.0),
+        target: Sequence[float] = (0.0, 0.0, 0.0),
+        focal_length: float = 2.0,
+        scale: float = 150.0,
+        want_rgb: bool = False,
+    ):
+        """renderMetropolis semantics (src/Metropolis.cpp:85-192) with the steps
+        split over parallel chains: the Canvas as (height, width) uint32. want_rgb
+        adds the normalised (height, width, 3) radiance estimate and the bootstrap
+        mean luminance b."""
+        self._check_open()
+        p = self._camera_params(width, height, position, target, focal_length, scale)
+        canvas = np.empty((height, width), np.uint32)
+        rgb = np.empty((height, width, 3), np.float32) if want_rgb else None
+        b = ctypes.c_double(0.0)
+        _native.check(_native.load().rn_pt_render_metropolis(self._handle, ctypes.byref(p), int(mutations),
+                                                             ctypes.c_float(exposure), int(chains), int(bootstrap),
+                                                             int(seed), 0, None, _ptr(canvas), _ptr(rgb),
+                                                             ctypes.byref(b)), "render_metropolis")
+        return (canvas, rgb, b.value) if want_rgb else canvas
+
     def render_raytraced(
         self,
         width: int,

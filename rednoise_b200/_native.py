@@ -22,6 +22,7 @@ RN_PT_NO_RAY_SORT = 32
 RN_PT_LBVH = 64
 RN_PT_SHADING_FLAT, RN_PT_SHADING_GOURAUD, RN_PT_SHADING_PHONG = 0, 1, 2
 RN_PT_STATIC_MAX_PIXELS = 512 * 512
+RN_PT_RNG_REFERENCE, RN_PT_RNG_COUNTER = 0, 1
 
 STATUS_NAMES = {
     0: "RN_OK",
@@ -242,6 +243,11 @@ SIGNATURES = {
     "rn_pt_accum_resolve": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, vp]),
     "rn_pt_render_photon_mapped": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_uint, vp, vp, vp]),
+    "rn_pt_render_bidirectional": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_float,
+                                                  ctypes.c_int, ctypes.c_ulonglong, ctypes.c_uint, vp, vp, vp]),
+    "rn_pt_render_metropolis": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_longlong, ctypes.c_float,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, ctypes.c_uint, vp, vp,
+                                               vp, vp]),
     "rn_pt_render": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint, vp, vp]),
     "rn_pt_render_accumulate": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                                vp, vp]),

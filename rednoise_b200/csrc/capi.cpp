@@ -1,9 +1,12 @@
 // Drop-in rn_render / rn_save_png and the reference-mode entry point.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
+#include "gi.hpp"
 #include "photon.hpp"
 #include "refmode.hpp"
 #include "scene_impl.hpp"
@@ -359,6 +362,129 @@ rn_status rn_pt_render_photon_mapped(rn_scene *scene, const rn_pt_ref_params *pr
 	RNB_CUDA(cudaStreamSynchronize(cs));
 	if (h) {
 		set_last_error("rn_pt_render_photon_mapped: traversal stack bound exceeded (corrupt scene)");
+		return RN_ERR_INTERNAL;
+	}
+	return RN_OK;
+}
+
+namespace {
+
+// Validation and the camera shared by the bidirectional and Metropolis renderers.
+rn_status gi_params(const char *fn, rn_scene *scene, const rn_pt_ref_params *prm, float exposure, GiParams &p) {
+	if (!scene || !prm || prm->width <= 0 || prm->height <= 0 || !std::isfinite(exposure)) {
+		set_last_error(std::string(fn) + ": invalid argument");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (static_cast<long>(prm->width) * prm->height > (1L << 26)) {
+		set_last_error(std::string(fn) + ": image too large");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	p = GiParams{};
+	p.width = prm->width;
+	p.height = prm->height;
+	std::memcpy(p.position, prm->position, 12);
+	look_at(prm->position, prm->target, p.orient);
+	p.f = prm->focal_length * prm->scale;
+	p.exposure = exposure;
+	return rn_pt_scene_prepare(scene);
+}
+
+} // namespace
+
+rn_status rn_pt_render_bidirectional(rn_scene *scene, const rn_pt_ref_params *prm, int samples, float exposure, int rng,
+                                     unsigned long long seed, unsigned flags, void *stream, uint32_t *argb,
+                                     float *rgb) {
+	GiParams p;
+	rn_status st = gi_params("rn_pt_render_bidirectional", scene, prm, exposure, p);
+	if (st != RN_OK)
+		return st;
+	if (!argb || samples < 1 || samples > (1 << 16) || (rng != RN_PT_RNG_REFERENCE && rng != RN_PT_RNG_COUNTER)) {
+		set_last_error("rn_pt_render_bidirectional: need argb, 1 <= samples <= 65536 and a known rng");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	p.samples = samples;
+	p.seed = seed;
+	const bool ref_stream = rng == RN_PT_RNG_REFERENCE;
+	const size_t budget = size_t(512) << 20;
+	const long npix = static_cast<long>(p.width) * p.height;
+	const bool dev = (flags & RN_PT_DEVICE_POINTERS) != 0;
+	cudaStream_t cs = pick_stream(scene, stream);
+	std::lock_guard<std::mutex> lock(scene->scratch_mu);
+	const size_t img = dev ? 0 : ((static_cast<size_t>(npix) * 4 + 255) & ~size_t(255));
+	const size_t frgb = (dev || !rgb) ? 0 : ((static_cast<size_t>(npix) * 12 + 255) & ~size_t(255));
+	RNB_CUDA(scene->scratch.ensure(256 + img + frgb + bdpt_scratch_bytes(p, ref_stream, budget)));
+	char *base = scene->scratch.as<char>();
+	int *d_err = reinterpret_cast<int *>(base);
+	uint32_t *d_argb = dev ? argb : reinterpret_cast<uint32_t *>(base + 256);
+	float *d_rgb = dev ? rgb : (rgb ? reinterpret_cast<float *>(base + 256 + img) : nullptr);
+	RNB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), cs));
+	RNB_CUDA(launch_bdpt(scene->view, scene->d_ref_shade.as<float4>(), p, ref_stream, budget, base + 256 + img + frgb,
+	                     d_argb, d_rgb, d_err, cs));
+	if (!dev) {
+		RNB_CUDA(cudaMemcpyAsync(argb, d_argb, static_cast<size_t>(npix) * 4, cudaMemcpyDeviceToHost, cs));
+		if (rgb)
+			RNB_CUDA(cudaMemcpyAsync(rgb, d_rgb, static_cast<size_t>(npix) * 12, cudaMemcpyDeviceToHost, cs));
+	}
+	int h = 0;
+	RNB_CUDA(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, cs));
+	RNB_CUDA(cudaStreamSynchronize(cs));
+	if (h) {
+		set_last_error("rn_pt_render_bidirectional: traversal stack bound exceeded (corrupt scene)");
+		return RN_ERR_INTERNAL;
+	}
+	return RN_OK;
+}
+
+rn_status rn_pt_render_metropolis(rn_scene *scene, const rn_pt_ref_params *prm, long long mutations, float exposure,
+                                  int chains, int bootstrap, unsigned long long seed, unsigned flags, void *stream,
+                                  uint32_t *argb, float *rgb, double *mean_luminance) {
+	GiParams p;
+	rn_status st = gi_params("rn_pt_render_metropolis", scene, prm, exposure, p);
+	if (st != RN_OK)
+		return st;
+	if (!argb || mutations < 1 || mutations > (1LL << 40) || chains < 0 || chains > (1 << 22) || bootstrap < 1 ||
+	    bootstrap > kMltMaxBootstrap) {
+		set_last_error("rn_pt_render_metropolis: need argb, 1 <= mutations <= 2^40, 0 <= chains <= 2^22 and "
+		               "1 <= bootstrap <= 2^24");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (chains == 0)
+		chains = static_cast<int>(std::max<long long>(1, std::min<long long>(mutations / 64, 1 << 18)));
+	if (chains > mutations || mutations / chains >= (1LL << 32)) {
+		set_last_error("rn_pt_render_metropolis: need chains <= mutations and mutations / chains < 2^32");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	p.mutations = mutations;
+	p.chains = chains;
+	p.bootstrap = bootstrap;
+	p.seed = seed;
+	const long npix = static_cast<long>(p.width) * p.height;
+	const bool dev = (flags & RN_PT_DEVICE_POINTERS) != 0;
+	cudaStream_t cs = pick_stream(scene, stream);
+	std::lock_guard<std::mutex> lock(scene->scratch_mu);
+	const size_t img = dev ? 0 : ((static_cast<size_t>(npix) * 4 + 255) & ~size_t(255));
+	const size_t frgb = (dev || !rgb) ? 0 : ((static_cast<size_t>(npix) * 12 + 255) & ~size_t(255));
+	RNB_CUDA(scene->scratch.ensure(256 + img + frgb + mlt_scratch_bytes(p)));
+	char *base = scene->scratch.as<char>();
+	int *d_err = reinterpret_cast<int *>(base);
+	double *d_b = reinterpret_cast<double *>(base + 8);
+	uint32_t *d_argb = dev ? argb : reinterpret_cast<uint32_t *>(base + 256);
+	float *d_rgb = dev ? rgb : (rgb ? reinterpret_cast<float *>(base + 256 + img) : nullptr);
+	RNB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), cs));
+	RNB_CUDA(launch_mlt(scene->view, scene->d_ref_shade.as<float4>(), p, base + 256 + img + frgb, d_argb, d_rgb,
+	                    dev && mean_luminance ? mean_luminance : d_b, d_err, cs));
+	if (!dev) {
+		RNB_CUDA(cudaMemcpyAsync(argb, d_argb, static_cast<size_t>(npix) * 4, cudaMemcpyDeviceToHost, cs));
+		if (rgb)
+			RNB_CUDA(cudaMemcpyAsync(rgb, d_rgb, static_cast<size_t>(npix) * 12, cudaMemcpyDeviceToHost, cs));
+		if (mean_luminance)
+			RNB_CUDA(cudaMemcpyAsync(mean_luminance, d_b, sizeof(double), cudaMemcpyDeviceToHost, cs));
+	}
+	int h = 0;
+	RNB_CUDA(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, cs));
+	RNB_CUDA(cudaStreamSynchronize(cs));
+	if (h) {
+		set_last_error("rn_pt_render_metropolis: traversal stack bound exceeded (corrupt scene)");
 		return RN_ERR_INTERNAL;
 	}
 	return RN_OK;
