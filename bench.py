@@ -50,10 +50,14 @@ def parse():
     p.add_argument("--integrator", default="auto", choices=["auto", "megakernel", "wavefront"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-grad", action="store_true", help="skip the gradient-vs-primal timing")
-    p.add_argument("--workload", default="frame", choices=["frame", "batch64", "inverse", "raytraced", "photon", "lbvh"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batch64", "inverse", "raytraced", "photon", "lbvh",
+                                                       "bidirectional", "metropolis"],
                    help="frame: the 1.31M-triangle 1080p frame (the bench line); batch64: 64 scenes per "
                         "launch; inverse: 16-view albedo recovery; raytraced: Whitted ray tracing; "
-                        "photon: photon mapping; lbvh: the GPU-built BVH")
+                        "photon: photon mapping; lbvh: the GPU-built BVH; bidirectional: bidirectional path "
+                        "tracing; metropolis: Metropolis light transport")
+    p.add_argument("--small", action="store_true",
+                   help="bidirectional / metropolis: the 160x120 case (16 spp / 400 000 mutations) used for profiles")
     p.add_argument("--inverse-steps", type=int, default=200)
     return p.parse_args()
 
@@ -807,6 +811,92 @@ def run_lbvh(args):
     print(json.dumps(line), flush=True)
 
 
+def cornell_pair():
+    """The reference's Cornell box (assets/cornell-box.obj at scale 0.35, as its app
+    loads it; a committed fixture) as a GPU scene and as a reference model."""
+    import oracle
+
+    import rednoise_b200 as rn
+
+    a = np.load(os.path.join(ROOT, "tests", "golden", "assets_ref.npz"))
+    s = rn.Scene.from_arrays(a["cornell_v"], ref_rgb=a["cornell_rgb"], ref_material=a["cornell_material"],
+                             ref_normal=a["cornell_normal"], ref_roughness=a["cornell_roughness"])
+    s.prepare()
+    m = oracle.RefModel.from_arrays(a["cornell_v"], a["cornell_rgb"], a["cornell_material"], a["cornell_roughness"],
+                                    a["cornell_normal"])
+    return s, m
+
+
+def time_calls(fn, warmup, steps):
+    for _ in range(warmup):
+        fn()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        out = fn()
+    return (time.perf_counter() - t0) / steps, out
+
+
+def run_bidirectional(args):
+    """Bidirectional path tracing (renderBidirectional: 64 spp, exposure 40) of the
+    reference's Cornell box at 640x480 with the reference's camera, through the C
+    ABI with a host canvas: the reference row streams (the reference's canvas) and
+    the counter streams, against the reference on the host cores (one frame)."""
+    import torch
+
+    torch.cuda.set_device(0)
+    s, m = cornell_pair()
+    W, H, spp = (160, 120, 16) if args.small else (640, 480, 64)
+    ref_s, img = time_calls(lambda: s.render_bidirectional(W, H, spp), args.warmup, args.steps)
+    ctr_s, _ = time_calls(lambda: s.render_bidirectional(W, H, spp, rng="counter"), args.warmup, args.steps)
+    t0 = time.perf_counter()
+    want = m.render_bidirectional(W, H, spp)
+    cpu_s = time.perf_counter() - t0
+    line = {"metric": "frames/s (bidirectional path tracing, end to end through the C ABI)", "value": 1.0 / ref_s,
+            "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ref_s * 1e3,
+            "higher_is_better": True, "dtype": "f32", "data": "reference asset (Cornell box, 32 triangles)",
+            "config": {"workload": f"cornell-box {W}x{H} renderBidirectional, {spp} spp, exposure 40, camera (0,0,4)",
+                       "rng": "reference per-row std::mt19937 streams", "output": "host canvas, copy included"},
+            "samples_per_s": W * H * spp / ref_s,
+            "identical_pixels_vs_reference": float((img == want).mean()),
+            "counter_stream": {"value": 1.0 / ctr_s, "unit": "frames/s", "ms_per_step": ctr_s * 1e3,
+                               "samples_per_s": W * H * spp / ctr_s},
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "frames/s", "cores": os.cpu_count(), "kind": "reference",
+                             "sample": f"reference renderBidirectional (oracle/_ref, OpenMP), one frame ({cpu_s:.2f} s)"}}
+    print(json.dumps(line), flush=True)
+
+
+def run_metropolis(args):
+    """Primary-sample Metropolis light transport (renderMetropolis: 4 000 000
+    mutations, 100 000 bootstrap paths, exposure 16) of the reference's Cornell box
+    at 640x480, through the C ABI with a host canvas, against the reference on the
+    host cores (one frame)."""
+    import torch
+
+    torch.cuda.set_device(0)
+    s, m = cornell_pair()
+    W, H, muts = (160, 120, 400000) if args.small else (640, 480, 4000000)
+    gpu_s, img = time_calls(lambda: s.render_metropolis(W, H, muts), args.warmup, args.steps)
+    big_s, _ = time_calls(lambda: s.render_metropolis(W, H, 16 * muts), 1, 1)
+    t0 = time.perf_counter()
+    want = m.render_metropolis(W, H, muts)
+    cpu_s = time.perf_counter() - t0
+    ch = lambda c: np.stack([(c >> 16) & 255, (c >> 8) & 255, c & 255], -1).astype(np.float64)  # noqa: E731
+    line = {"metric": "frames/s (Metropolis light transport, end to end through the C ABI)", "value": 1.0 / gpu_s,
+            "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": gpu_s * 1e3,
+            "higher_is_better": True, "dtype": "f32", "data": "reference asset (Cornell box, 32 triangles)",
+            "config": {"workload": f"cornell-box {W}x{H} renderMetropolis, {muts} mutations, 100000 bootstrap paths, "
+                                   "exposure 16, camera (0,0,4)",
+                       "chains": muts // 16, "output": "host canvas, copy included"},
+            "mutations_per_s": muts / gpu_s,
+            "mutations_per_s_64M": 16 * muts / big_s,
+            "mean_level": {"gpu": float(ch(img).mean()), "reference": float(ch(want).mean())},
+            "mean_abs_level_difference_vs_reference": float(np.abs(ch(img) - ch(want)).mean()),
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "frames/s", "cores": os.cpu_count(), "kind": "reference",
+                             "sample": f"reference renderMetropolis (oracle/_ref, 16 OpenMP chains), one frame "
+                                       f"({cpu_s:.2f} s)"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -821,6 +911,10 @@ def main():
         run_photon(args)
     elif args.workload == "lbvh":
         run_lbvh(args)
+    elif args.workload == "bidirectional":
+        run_bidirectional(args)
+    elif args.workload == "metropolis":
+        run_metropolis(args)
     else:
         run_ours(args)
 

@@ -218,7 +218,7 @@ rn_status rn_pt_render_bidirectional(rn_scene *scene, const rn_pt_ref_params *pa
  * with the reference's large-step (p = 0.3) and Gaussian small-step (sigma = 0.02)
  * mutations, acceptance and expected-value deposits; exposure (reference default 16)
  * and Reinhard onto the canvas. The steps are split over `chains` chains run in
- * parallel (0: mutations / 64, at most 262144), each started from a bootstrap path
+ * parallel (0: mutations / 16, at most 2097152), each started from a bootstrap path
  * drawn in proportion to its luminance; random numbers are Philox streams under
  * `seed`. argb: width*height pixels; rgb (may be NULL): width*height*3 floats of
  * the normalised radiance estimate before exposure; mean_luminance (may be NULL): the

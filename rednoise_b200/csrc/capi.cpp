@@ -449,7 +449,7 @@ rn_status rn_pt_render_metropolis(rn_scene *scene, const rn_pt_ref_params *prm, 
 		return RN_ERR_INVALID_ARGUMENT;
 	}
 	if (chains == 0)
-		chains = static_cast<int>(std::max<long long>(1, std::min<long long>(mutations / 64, 1 << 18)));
+		chains = static_cast<int>(std::max<long long>(1, std::min<long long>(mutations / 16, 1 << 21)));
 	if (chains > mutations || mutations / chains >= (1LL << 32)) {
 		set_last_error("rn_pt_render_metropolis: need chains <= mutations and mutations / chains < 2^32");
 		return RN_ERR_INVALID_ARGUMENT;

@@ -46,23 +46,23 @@ constexpr int kRowsPerBlock = 1;
 
 __device__ __forceinline__ float gi_light_area() { return (2.0f * kGiLightHalf) * (2.0f * kGiLightHalf); }
 
-// std::mt19937 of one image row kept in device memory, word k at s[k * stride].
+// std::mt19937 of one image row kept in device memory: 624 contiguous words, so
+// the row's lone thread finds its state in a few cache lines.
 struct MtRow {
 	uint32_t *s;
-	int stride;
 	int i;
 	__device__ void twist() {
 		for (int k = 0; k < 624; k++) {
-			const uint32_t y = (s[k * stride] & 0x80000000u) | (s[(k + 1 < 624 ? k + 1 : 0) * stride] & 0x7fffffffu);
+			const uint32_t y = (s[k] & 0x80000000u) | (s[k + 1 < 624 ? k + 1 : 0] & 0x7fffffffu);
 			const int m = k + 397 < 624 ? k + 397 : k + 397 - 624;
-			s[k * stride] = s[m * stride] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+			s[k] = s[m] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
 		}
 		i = 0;
 	}
 	__device__ float operator()() {
 		if (i >= 624)
 			twist();
-		uint32_t y = s[(i++) * stride];
+		uint32_t y = s[i++];
 		y ^= y >> 11;
 		y ^= (y << 7) & 0x9d2c5680u;
 		y ^= (y << 15) & 0xefc60000u;
@@ -111,13 +111,32 @@ __device__ __forceinline__ V3 tri_albedo(const float4 *ref_shade, int idx) {
 	return mk(s1.x, s1.y, s1.z) / 255.0f;
 }
 
+// Closest hit for a thread that runs alone (the row pass): the same result as
+// intersect(), with each leaf's triangle tests overlapped.
+__device__ __forceinline__ Hit intersect_alone(Ctx &c, V3 o, V3 d) {
+	const RayPre r = make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
+	HitRec h;
+	if (c.sv.nodes4 && finite_inverse(r)) {
+		LocalStack<unsigned long long> st;
+		h = trace_closest4_flat(c.sv, r, -1, c.err, st);
+	} else {
+		h = trace_closest<kOrderReference>(c.sv, r, -1, c.err);
+	}
+	Hit out;
+	out.hit = h.idx >= 0;
+	out.idx = h.idx;
+	out.t = h.t;
+	out.point = o + h.t * d;
+	return out;
+}
+
 // tracePath (src/BDPT.cpp:43-61). code (may be null) receives 2 * triangle + 1 if
 // faceViewer flipped the normal.
-template <class D>
+template <bool kAlone, class D>
 __device__ int gi_subpath(Ctx &c, V3 o, V3 d, V3 beta, GV *out, int *code, D &draw) {
 	int k = 0;
 	for (int depth = 0; depth < kGiMaxDepth; depth++) {
-		const Hit h = intersect(c, o, d, -1);
+		const Hit h = kAlone ? intersect_alone(c, o, d) : intersect(c, o, d, -1);
 		if (!h.hit)
 			break;
 		const V3 tn = tri_normal(c.ref_shade, h.idx);
@@ -142,7 +161,7 @@ __device__ int gi_subpath(Ctx &c, V3 o, V3 d, V3 beta, GV *out, int *code, D &dr
 
 // The camera and light subpaths of one sample (src/BDPT.cpp:90-108). lv[0] is the
 // point on the emitter; nl counts it.
-template <class D>
+template <bool kAlone, class D>
 __device__ void bdpt_subpaths(Ctx &c, const GiParams &p, const GiCam &cam, int x, int y, D &draw, GV *cv, int *ccode,
                               int &nc, GV *lv, int *lcode, int &nl) {
 	// glm::vec3((x + U - W/2) / f, -(y + U - H/2) / f, -1): GCC evaluates the two
@@ -151,7 +170,7 @@ __device__ void bdpt_subpaths(Ctx &c, const GiParams &p, const GiCam &cam, int x
 	const float sx = (static_cast<float>(x) + ux - static_cast<float>(p.width) / 2.0f) / p.f;
 	const float sy = -(static_cast<float>(y) + uy - static_cast<float>(p.height) / 2.0f) / p.f;
 	const V3 dir = normalize(cam.right * sx + cam.up * sy + cam.fwd * -1.0f);
-	nc = gi_subpath(c, cam.pos, dir, mk(1.0f, 1.0f, 1.0f), cv, ccode, draw);
+	nc = gi_subpath<kAlone>(c, cam.pos, dir, mk(1.0f, 1.0f, 1.0f), cv, ccode, draw);
 	const float lz = draw(), lx = draw(); // right to left again
 	const V3 lp =
 	    mk(0.0f, 0.33f, 0.0f) + mk((lx * 2.0f - 1.0f) * kGiLightHalf, 0.0f, (lz * 2.0f - 1.0f) * kGiLightHalf);
@@ -160,7 +179,7 @@ __device__ void bdpt_subpaths(Ctx &c, const GiParams &p, const GiCam &cam, int x
 	lv[0] = GV{lp, ln, mk(0.0f, 0.0f, 0.0f), le};
 	const float d1 = draw(), d2 = draw();
 	const V3 ldir = cosine_hemisphere_u(ln, d1, d2);
-	nl = 1 + gi_subpath(c, lp + kGiEps * ldir, ldir, le, lv + 1, lcode, draw);
+	nl = 1 + gi_subpath<kAlone>(c, lp + kGiEps * ldir, ldir, le, lv + 1, lcode, draw);
 }
 
 // Every camera vertex to every light vertex with the uniform MIS weight
@@ -212,11 +231,12 @@ __global__ void k_mt_seed_rows(uint32_t *s, int *idx, int rows) {
 	const int y = blockIdx.x * blockDim.x + threadIdx.x;
 	if (y >= rows)
 		return;
+	uint32_t *row = s + 624 * static_cast<size_t>(y);
 	uint32_t v = 9871u + static_cast<uint32_t>(y);
-	s[y] = v;
+	row[0] = v;
 	for (int k = 1; k < 624; k++) {
 		v = 1812433253u * (v ^ (v >> 30)) + static_cast<uint32_t>(k);
-		s[static_cast<size_t>(k) * rows + y] = v;
+		row[k] = v;
 	}
 	idx[y] = 624;
 }
@@ -232,14 +252,14 @@ __global__ void __launch_bounds__(32) k_bdpt_rows(SceneView sv, const float4 *__
 		return;
 	Ctx c{sv, ref_shade, nullptr, 0};
 	const GiCam cam = gi_cam(p);
-	MtRow rng{mt_s + y, p.height, mt_i[y]};
+	MtRow rng{mt_s + 624 * static_cast<size_t>(y), mt_i[y]};
 	const int cw = x1 - x0;
 	for (int x = x0; x < x1; x++) {
 		for (int s = 0; s < p.samples; s++) {
 			const size_t sample = (static_cast<size_t>(y) * cw + (x - x0)) * p.samples + s;
 			GV cv[kGiMaxDepth], lv[kGiMaxDepth + 1];
 			int cc[kGiMaxDepth], lc[kGiMaxDepth], nc, nl;
-			bdpt_subpaths(c, p, cam, x, y, rng, cv, cc, nc, lv, lc, nl);
+			bdpt_subpaths<true>(c, p, cam, x, y, rng, cv, cc, nc, lv, lc, nl);
 			float4 *r = rec + sample * kBdptRecordSlots;
 			for (int i = 0; i < nc; i++)
 				r[i] = make_float4(cv[i].p.x, cv[i].p.y, cv[i].p.z, __int_as_float(cc[i]));
@@ -318,7 +338,8 @@ __global__ void __launch_bounds__(128) k_bdpt_counter(SceneView sv, const float4
 		          static_cast<uint32_t>(p.seed >> 32), 0, U4{0u, 0u, 0u, 0u}};
 		GV cv[kGiMaxDepth], lv[kGiMaxDepth + 1];
 		int nc, nl;
-		bdpt_subpaths(c, p, cam, x, y, d, cv, static_cast<int *>(nullptr), nc, lv, static_cast<int *>(nullptr), nl);
+		bdpt_subpaths<false>(c, p, cam, x, y, d, cv, static_cast<int *>(nullptr), nc, lv, static_cast<int *>(nullptr),
+		                     nl);
 		bdpt_connect(c, cv, nc, lv, nl, acc);
 	}
 	gi_store(p, pix, acc * (p.exposure / static_cast<float>(p.samples)), argb, rgb);

@@ -515,6 +515,139 @@ __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPr
 	return h;
 }
 
+// tri_test without early exits: every quantity is formed with tri_test's
+// operations, so t, u, v and the verdict are tri_test's. Straight-line code lets a
+// thread that runs alone overlap the tests of one leaf.
+__device__ __forceinline__ bool tri_test_flat(const float4 a, const float4 b, const float4 c, const RayPre &r,
+                                              float &t, float &u, float &v) {
+	const float spx = __fsub_rn(r.ox, a.x);
+	const float spy = __fsub_rn(r.oy, a.y);
+	const float spz = __fsub_rn(r.oz, a.z);
+	const float c00 = __fsub_rn(__fmul_rn(b.y, c.z), __fmul_rn(c.y, b.z));
+	const float A = __fsub_rn(__fmul_rn(r.ndy, c.z), __fmul_rn(c.y, r.ndz));
+	const float B = __fsub_rn(__fmul_rn(r.ndy, b.z), __fmul_rn(b.y, r.ndz));
+	const float det = __fadd_rn(__fsub_rn(__fmul_rn(r.ndx, c00), __fmul_rn(b.x, A)), __fmul_rn(c.x, B));
+	const float k = __fdiv_rn(1.0f, det);
+	const float i01 = __fmul_rn(-A, k);
+	const float i11 = __fmul_rn(__fsub_rn(__fmul_rn(r.ndx, c.z), __fmul_rn(c.x, r.ndz)), k);
+	const float i21 = __fmul_rn(-__fsub_rn(__fmul_rn(r.ndx, c.y), __fmul_rn(c.x, r.ndy)), k);
+	u = __fadd_rn(__fadd_rn(__fmul_rn(i01, spx), __fmul_rn(i11, spy)), __fmul_rn(i21, spz));
+	const float i02 = __fmul_rn(B, k);
+	const float i12 = __fmul_rn(-__fsub_rn(__fmul_rn(r.ndx, b.z), __fmul_rn(b.x, r.ndz)), k);
+	const float i22 = __fmul_rn(__fsub_rn(__fmul_rn(r.ndx, b.y), __fmul_rn(b.x, r.ndy)), k);
+	v = __fadd_rn(__fadd_rn(__fmul_rn(i02, spx), __fmul_rn(i12, spy)), __fmul_rn(i22, spz));
+	const float i00 = __fmul_rn(c00, k);
+	const float i10 = __fmul_rn(-__fsub_rn(__fmul_rn(b.x, c.z), __fmul_rn(c.x, b.z)), k);
+	const float i20 = __fmul_rn(__fsub_rn(__fmul_rn(b.x, c.y), __fmul_rn(c.x, b.y)), k);
+	t = __fadd_rn(__fadd_rn(__fmul_rn(i00, spx), __fmul_rn(i10, spy)), __fmul_rn(i20, spz));
+	return !(fabsf(det) < 1e-8f) && (u >= 0.0f) && (v >= 0.0f) && (__fadd_rn(u, v) <= 1.0f) && (t > 1e-5f);
+}
+
+// trace_closest4 (reference order) for a thread that runs alone: a leaf's first
+// four triangles are tested as independent straight-line work, then merged in leaf
+// order with the same strict '<', so the result is trace_closest4's.
+template <class Stack>
+__device__ __forceinline__ HitRec trace_closest4_flat(const SceneView &s, const RayPre &r, int ignore, int &err,
+                                                      Stack &st) {
+	const RayPair r2 = make_pair_ray(r);
+	HitRec h;
+	h.idx = -1;
+	h.rank = 0x7fffffff;
+	h.t = __int_as_float(0x7f800000);
+	h.u = 0.0f;
+	h.v = 0.0f;
+	int sp = 0;
+	float te;
+	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te)) {
+		st.put(0, pack_entry(s.root4_ref, te));
+		sp = 1;
+	}
+	while (sp > 0) {
+		--sp;
+		const unsigned long long e = st.get(sp);
+		int ref = static_cast<int>(static_cast<unsigned>(e));
+		if (!(__int_as_float(static_cast<int>(e >> 32)) < h.t))
+			continue;
+		while (ref >= 0) {
+			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ref);
+			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
+			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
+			const ulonglong2 z01 = __ldg(nq + 4), z23 = __ldg(nq + 5);
+			const float4 rf = __ldg(nd + 6);
+			const int cnt = __float_as_int(__ldg(nd + 7).x);
+			float t0, t1, t2, t3;
+			const bool b0 = slab2(x01.x, y01.x, z01.x, r2, t0);
+			const bool b1 = slab2(x01.y, y01.y, z01.y, r2, t1);
+			const bool b2 = cnt > 2 && slab2(x23.x, y23.x, z23.x, r2, t2);
+			const bool b3 = cnt > 3 && slab2(x23.y, y23.y, z23.y, r2, t3);
+			if (sp + 3 > kStack) {
+				err = 1;
+				return h;
+			}
+			if (b3)
+				st.put(sp++, pack_entry(__float_as_int(rf.w), t3));
+			if (b2)
+				st.put(sp++, pack_entry(__float_as_int(rf.z), t2));
+			if (b1)
+				st.put(sp++, pack_entry(__float_as_int(rf.y), t1));
+			if (b0 && t0 < h.t) {
+				ref = __float_as_int(rf.x);
+			} else {
+				ref = 0x7fffffff;
+				break;
+			}
+		}
+		if (ref == 0x7fffffff)
+			continue;
+		const int start = leaf_start(ref);
+		const int count = leaf_count(ref);
+		if (count == 0)
+			continue;
+		float4 ta[4], tb[4], tc[4];
+#pragma unroll
+		for (int q = 0; q < 4; q++) {
+			const float4 *tp = s.tris + 3 * static_cast<size_t>(start + (q < count ? q : 0));
+			ta[q] = __ldg(tp + 0);
+			tb[q] = __ldg(tp + 1);
+			tc[q] = __ldg(tp + 2);
+		}
+		bool ok[4];
+		float tt[4], uu[4], vv[4];
+#pragma unroll
+		for (int q = 0; q < 4; q++)
+			ok[q] = tri_test_flat(ta[q], tb[q], tc[q], r, tt[q], uu[q], vv[q]) && q < count &&
+			        __float_as_int(ta[q].w) != ignore;
+#pragma unroll
+		for (int q = 0; q < 4; q++) {
+			if (ok[q] && tt[q] < h.t) {
+				h.idx = __float_as_int(ta[q].w);
+				h.t = tt[q];
+				h.u = uu[q];
+				h.v = vv[q];
+				h.rank = __float_as_int(tb[q].w);
+			}
+		}
+		for (int p = start + 4; p < start + count; p++) {
+			const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
+			const float4 a = __ldg(tp + 0);
+			const int ti = __float_as_int(a.w);
+			if (ti == ignore)
+				continue;
+			const float4 b = __ldg(tp + 1);
+			const float4 c = __ldg(tp + 2);
+			float t, u, v;
+			if (tri_test(a, b, c, r, t, u, v) && t < h.t) {
+				h.idx = ti;
+				h.t = t;
+				h.u = u;
+				h.v = v;
+				h.rank = __float_as_int(b.w);
+			}
+		}
+	}
+	return h;
+}
+
 __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPre &r, int ignore, int &err) {
 	LocalStack<unsigned long long> st;
 	return trace_closest4(s, r, ignore, err, st);
