@@ -51,13 +51,15 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-grad", action="store_true", help="skip the gradient-vs-primal timing")
     p.add_argument("--workload", default="frame", choices=["frame", "batch64", "inverse", "raytraced", "photon", "lbvh",
-                                                       "bidirectional", "metropolis"],
+                                                       "bidirectional", "metropolis", "dropin"],
                    help="frame: the 1.31M-triangle 1080p frame (the bench line); batch64: 64 scenes per "
                         "launch; inverse: 16-view albedo recovery; raytraced: Whitted ray tracing; "
                         "photon: photon mapping; lbvh: the GPU-built BVH; bidirectional: bidirectional path "
-                        "tracing; metropolis: Metropolis light transport")
+                        "tracing; metropolis: Metropolis light transport; dropin: the rn_render path tracer "
+                        "(reference semantics) alone")
     p.add_argument("--small", action="store_true",
-                   help="bidirectional / metropolis: the 160x120 case (16 spp / 400 000 mutations) used for profiles")
+                   help="bidirectional / metropolis / dropin: the small case used for profiles (160x120 at 16 spp, "
+                        "400 000 mutations, 480x270 at 1 spp)")
     p.add_argument("--inverse-steps", type=int, default=200)
     return p.parse_args()
 
@@ -897,6 +899,26 @@ def run_metropolis(args):
     print(json.dumps(line), flush=True)
 
 
+def run_dropin(args):
+    """The drop-in path tracer alone (rn_render's renderPathTraced semantics: depth
+    4, the default disk light with its 9 shadow rays per diffuse vertex, per-pixel
+    mt19937, 8-bit canvas) on the 1.31M-triangle scene at 1920x1080, 2 spp, through
+    the C ABI with a host canvas."""
+    import torch
+
+    torch.cuda.set_device(0)
+    from rednoise_b200 import scenes
+
+    sc = scenes.icosphere_scene(level=args.level)
+    W, H, spp = (480, 270, 1) if args.small else (1920, 1080, 2)
+    r = reference_semantics_rate(sc, W, H, args, spp=spp)
+    line = {"metric": "samples/s (drop-in path tracer, reference semantics, end to end through the C ABI)",
+            "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": 3, "warmup": 1, "ms_per_step": r["ms_per_frame"],
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"icosphere-cornell-1.31M-tris {r['workload']}"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -915,6 +937,8 @@ def main():
         run_bidirectional(args)
     elif args.workload == "metropolis":
         run_metropolis(args)
+    elif args.workload == "dropin":
+        run_dropin(args)
     else:
         run_ours(args)
 
