@@ -174,9 +174,13 @@ rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *prm, u
 
 	cudaStream_t cs = pick_stream(scene, stream);
 	std::lock_guard<std::mutex> lock(scene->scratch_mu);
-	const size_t need = 256 + ((sizeof(RefParams) + 255) & ~size_t(255)) + static_cast<size_t>(npix) * 4 + 256 +
-	                    static_cast<size_t>(npix) * 12 + 256;
-	RNB_CUDA(scene->scratch.ensure(need));
+	// Path records and shadow-ray results: the whole frame when it fits in 2 GiB,
+	// else pixel chunks.
+	const size_t per_pixel = ref_defer_bytes_per_pixel(p);
+	const size_t defer = 1024 + std::min(static_cast<size_t>(npix) * per_pixel, std::max(size_t(2) << 30, per_pixel));
+	const size_t head = 256 + ((sizeof(RefParams) + 255) & ~size_t(255)) + ((static_cast<size_t>(npix) * 4 + 255) &
+	                    ~size_t(255)) + ((static_cast<size_t>(npix) * 12 + 255) & ~size_t(255));
+	RNB_CUDA(scene->scratch.ensure(head + defer));
 	char *base = scene->scratch.as<char>();
 	int *d_err = reinterpret_cast<int *>(base);
 	RefParams *d_p = reinterpret_cast<RefParams *>(base + 256);
@@ -188,8 +192,8 @@ rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *prm, u
 	RNB_CUDA(cudaMemcpyAsync(d_p, &p, sizeof(p), cudaMemcpyHostToDevice, cs));
 	uint32_t *o_argb = argb ? (dev ? argb : d_argb) : d_argb;
 	float *o_mean = mean_rgb ? (dev ? mean_rgb : d_mean) : nullptr;
-	RNB_CUDA(launch_render_reference(scene->view, scene->d_ref_shade.as<float4>(), d_p, p.width, p.height, o_argb,
-	                                 o_mean, d_err, cs));
+	RNB_CUDA(launch_render_reference(scene->view, scene->d_ref_shade.as<float4>(), p, d_p, o_argb, o_mean, d_err,
+	                                 base + head, defer, cs));
 	if (!dev) {
 		if (argb)
 			RNB_CUDA(cudaMemcpyAsync(argb, d_argb, static_cast<size_t>(npix) * 4, cudaMemcpyDeviceToHost, cs));

@@ -16,6 +16,7 @@
 //   * closest hit / occlusion use the reference-order traversal (traverse.cuh).
 // Per pixel the output is then the reference's 8-bit value except where a libm
 // last-bit difference moves a path or a truncation boundary.
+#include <algorithm>
 #include <cstdint>
 
 #include "refshade.cuh"
@@ -23,22 +24,152 @@
 namespace rnb {
 
 namespace {
-constexpr int kMaxLevels = kMaxRefDepth + 1; // recursion levels max_depth..0
 
-// One pathTrace(origin, dir, depth = max_depth) evaluation (src/Renderer.cpp:820-907),
-// unrolled: each level records R_k = add + mul * R_{k+1} (kind 2), mul * R_{k+1}
-// (kind 1) or R_{k+1} (kind 0), then the levels are folded deepest first.
-__device__ V3 path_trace(Ctx &c, V3 origin, V3 direction, MT &rng) {
-	V3 add[kMaxLevels], mul[kMaxLevels];
-	int kind[kMaxLevels];
-	int levels = 0;
-	V3 result = mk(0, 0, 0);
+// src/Renderer.cpp:1103-1117
+__device__ void sample_aperture(int blades, float u1, float u2, float &lx, float &ly) {
+	if (blades < 3) {
+		const float ang = 2.0f * 3.14159265f * u1, rad = sqrtf(u2);
+		lx = lm_cos(ang) * rad;
+		ly = lm_sin(ang) * rad;
+		return;
+	}
+	const int wedge = min(blades - 1, static_cast<int>(u1 * blades));
+	const float a0 = 2.0f * 3.14159265f * wedge / blades, a1 = 2.0f * 3.14159265f * (wedge + 1) / blades;
+	const float v0x = lm_cos(a0), v0y = lm_sin(a0), v1x = lm_cos(a1), v1y = lm_sin(a1);
+	float s = u1 * blades - wedge, t = u2;
+	if (s + t > 1.0f) {
+		s = 1.0f - s;
+		t = 1.0f - t;
+	}
+	lx = v0x * s + v1x * t;
+	ly = v0y * s + v1y * t;
+}
+
+struct CamBasis {
+	V3 right, upv, fwd, pos, motion;
+};
+__device__ __forceinline__ CamBasis cam_basis(const RefParams &p) {
+	return {mk(p.orient[0], p.orient[1], p.orient[2]), mk(p.orient[3], p.orient[4], p.orient[5]),
+	        mk(p.orient[6], p.orient[7], p.orient[8]), l3(p.position), l3(p.camera_motion)};
+}
+
+// One camera sample of renderPathTraced's pixel loop (src/Renderer.cpp:1139-1166):
+// jitter, orthographic or perspective ray, motion blur, depth of field.
+template <class Rng>
+__device__ __forceinline__ void camera_sample(const RefParams &p, const CamBasis &b, int x, int y, Rng &rng, V3 &origin,
+                                              V3 &dir) {
+	const float jx = rng.uniform(-0.5f, 0.5f);
+	const float jy = rng.uniform(-0.5f, 0.5f);
+	const float sx = static_cast<float>(x) + 0.5f + jx - static_cast<float>(p.width) / 2.0f;
+	const float sy = -(static_cast<float>(y) + 0.5f + jy - static_cast<float>(p.height) / 2.0f);
+	V3 ro;
+	if (p.orthographic) {
+		const V3 v = mk(sx / p.f * p.ortho_scale, sy / p.f * p.ortho_scale, 0.0f);
+		ro = b.pos + (b.right * v.x + b.upv * v.y + b.fwd * v.z);
+		dir = normalize(b.right * 0.0f + b.upv * 0.0f + b.fwd * -1.0f);
+	} else {
+		const V3 v = mk(sx / p.f, sy / p.f, -1.0f);
+		ro = b.pos;
+		dir = normalize(b.right * v.x + b.upv * v.y + b.fwd * v.z);
+	}
+	const V3 cam = ro + b.motion * rng.uniform(0.0f, 1.0f);
+	origin = cam;
+	if (p.aperture > 0.0f && !p.orthographic) {
+		const V3 focal = cam + dir * p.focus_distance;
+		// sampleAperture(blades, U(rng), U(rng)): GCC evaluates these two call
+		// arguments right to left, so the second argument is drawn first.
+		float ua, ub;
+		if (p.aperture_args_right_to_left) {
+			ub = rng.uniform(0.0f, 1.0f);
+			ua = rng.uniform(0.0f, 1.0f);
+		} else {
+			ua = rng.uniform(0.0f, 1.0f);
+			ub = rng.uniform(0.0f, 1.0f);
+		}
+		float lx, ly;
+		sample_aperture(p.aperture_blades, ua, ub, lx, ly);
+		lx = lx * p.aperture;
+		ly = ly * p.aperture;
+		origin = cam + (b.right * lx + b.upv * ly);
+		dir = normalize(focal - origin);
+	}
+}
+
+__device__ __forceinline__ void store_pixel(long pix, V3 sum, int samples, uint32_t *argb, float *mean_rgb) {
+	const V3 colour = sum / static_cast<float>(samples) * 255.0f;
+	const int r = min(255, cvt_trunc(colour.x));
+	const int g = min(255, cvt_trunc(colour.y));
+	const int b = min(255, cvt_trunc(colour.z));
+	argb[pix] = (255u << 24) | ((static_cast<uint32_t>(r) & 0xFFu) << 16) | ((static_cast<uint32_t>(g) & 0xFFu) << 8) |
+	            (static_cast<uint32_t>(b) & 0xFFu);
+	if (mean_rgb) {
+		const V3 m = sum / static_cast<float>(samples);
+		mean_rgb[3 * pix] = m.x;
+		mean_rgb[3 * pix + 1] = m.y;
+		mean_rgb[3 * pix + 2] = m.z;
+	}
+}
+
+__device__ __forceinline__ uint32_t pixel_seed(int x, int y, int width) {
+	return static_cast<uint32_t>(
+	    (static_cast<uint32_t>(y) * static_cast<uint32_t>(width) + static_cast<uint32_t>(x)) * 9781u + 1u);
+}
+
+// ---- the drop-in path tracer in three passes ----
+// Visibility draws no random numbers, so a path's vertices do not depend on it:
+//  1. k_ref_paths: one thread per pixel walks every sample's path on the pixel's
+//     mt19937 stream (closest hits, material choices, bounces) and records each
+//     level; levels that need direct light join a compact shading list;
+//  2. k_ref_shadow: one thread per (shading entry, light, tap) traces that tap's
+//     shadow ray -- the taps of one point sit in adjacent lanes, so a warp's rays
+//     leave a few nearby points toward the same light;
+//  3. k_ref_fold: one thread per pixel forms directLight (and the subsurface term)
+//     from the recorded occlusions with the reference's operations and folds each
+//     path from its deepest level, in the reference's order.
+// Each level is three float4: (point, kind), (normal, ignore), (albedo or value,
+// shading entry).
+enum LevelKind : int { kLvPass = 0, kLvMul = 1, kLvDiffuse = 2, kLvSub = 3, kLvDiffuseEnd = 4, kLvSubEnd = 5, kLvValue = 6 };
+
+struct DeferView {
+	float4 *rec;
+	int *list;
+	unsigned *list_count;
+	uint8_t *occl;
+	int levels;
+	int taps;
+	long pix0;
+	long npix;
+};
+
+__device__ __forceinline__ int shading_append(unsigned *count) {
+	const unsigned mask = __activemask();
+	const int lane = static_cast<int>(threadIdx.x & 31);
+	const int leader = __ffs(mask) - 1;
+	unsigned base = 0;
+	if (lane == leader)
+		base = atomicAdd(count, static_cast<unsigned>(__popc(mask)));
+	base = __shfl_sync(mask, base, leader);
+	return static_cast<int>(base) + __popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void put_level(float4 *r, int kind, V3 a, V3 n, int ignore, V3 b, int entry) {
+	r[0] = make_float4(a.x, a.y, a.z, __int_as_float(kind));
+	r[1] = make_float4(n.x, n.y, n.z, __int_as_float(ignore));
+	r[2] = make_float4(b.x, b.y, b.z, __int_as_float(entry));
+}
+
+// pathTrace (src/Renderer.cpp:820-907) without the direct-light terms: the same
+// intersections, branches and random draws, recorded level by level.
+template <class Rng>
+__device__ void record_path(Ctx &c, V3 origin, V3 direction, Rng &rng, const DeferView &dv, size_t rec_index) {
 	int depth = c.p->max_depth;
-	for (;;) {
+	for (int level = 0; level < dv.levels; level++) {
+		float4 *r = dv.rec + 3 * (rec_index + level);
+		const V3 zero = mk(0.0f, 0.0f, 0.0f);
 		const Hit hit = intersect(c, origin, direction, -1);
 		if (!hit.hit) {
-			result = environment(direction) / 255.0f;
-			break;
+			put_level(r, kLvValue, zero, zero, -1, environment(direction) / 255.0f, -1);
+			return;
 		}
 		const float4 s0 = __ldg(c.ref_shade + 2 * static_cast<size_t>(hit.idx));
 		const float4 s1 = __ldg(c.ref_shade + 2 * static_cast<size_t>(hit.idx) + 1);
@@ -49,13 +180,13 @@ __device__ V3 path_trace(Ctx &c, V3 origin, V3 direction, MT &rng) {
 		const V3 point = hit.point;
 		const int ignore = hit.idx;
 		if (material == kRefEmissive) {
-			result = rgb / 255.0f * 4.0f;
-			break;
+			put_level(r, kLvValue, zero, zero, -1, rgb / 255.0f * 4.0f, -1);
+			return;
 		}
 		if (material == kRefMirror && depth > 0) {
 			const V3 n = face_viewer(tnormal, direction);
 			const V3 refl = reflect(direction, n);
-			kind[levels++] = 0;
+			put_level(r, kLvPass, zero, zero, -1, zero, -1);
 			origin = point + 1e-4f * refl;
 			direction = refl;
 			depth--;
@@ -82,7 +213,7 @@ __device__ V3 path_trace(Ctx &c, V3 origin, V3 direction, MT &rng) {
 			if (!do_reflect)
 				do_reflect = rng.uniform(0.0f, 1.0f) < fresnel;
 			const V3 dir = do_reflect ? reflect(direction, n) : refr;
-			kind[levels++] = 0;
+			put_level(r, kLvPass, zero, zero, -1, zero, -1);
 			origin = point + 1e-4f * dir;
 			direction = dir;
 			depth--;
@@ -96,163 +227,167 @@ __device__ V3 path_trace(Ctx &c, V3 origin, V3 direction, MT &rng) {
 			V3 dir = normalize(mix(refl, diff, r2));
 			if (dot(dir, n) <= 0.0f)
 				dir = refl;
-			const V3 albedo = base_colour(material, rgb, point) / 255.0f;
-			mul[levels] = albedo;
-			kind[levels++] = 1;
+			put_level(r, kLvMul, zero, zero, -1, base_colour(material, rgb, point) / 255.0f, -1);
 			origin = point + 1e-4f * dir;
 			direction = dir;
 			depth--;
 			continue;
 		}
-		if (material == kRefSubsurface) {
-			const V3 n = face_viewer(tnormal, direction);
-			const V3 albedo = base_colour(material, rgb, point) / 255.0f;
-			V3 shade = mk(0, 0, 0);
-			const float wrap = 0.5f;
-			for (int li = 0; li < c.p->num_lights; li++) {
-				const RefLight &L = c.p->lights[li];
-				const V3 to = l3(L.position) - point;
-				const float dist = length(to);
-				const V3 ld = to / dist;
-				const float atten =
-				    L.intensity / (L.atten_constant + L.atten_linear * dist + L.atten_quadratic * dist * dist);
-				const float wrap_diff = smax(0.0f, (dot(n, ld) + wrap) / (1.0f + wrap));
-				shade = shade + albedo * l3(L.colour) * (visibility(c, L, point, ignore) * atten * wrap_diff);
-				const Hit ex = intersect(c, point - n * 1e-3f, ld, ignore);
-				const float thickness = ex.hit ? ex.t : 0.0f;
-				shade = shade + albedo * l3(L.colour) * (atten * lm_exp(-3.0f * thickness) * 0.6f);
-			}
-			const V3 direct = vmin(shade, mk(1.5f, 1.5f, 1.5f));
-			if (depth <= 0) {
-				result = direct;
-				break;
-			}
-			const V3 sb = cosine_hemisphere(n, rng);
-			add[levels] = direct;
-			mul[levels] = albedo;
-			kind[levels++] = 2;
-			origin = point + 1e-4f * sb;
-			direction = sb;
-			depth--;
-			continue;
-		}
-		// Diffuse (and every branch above once depth reaches 0).
+		const bool sub = material == kRefSubsurface;
 		const V3 n = face_viewer(tnormal, direction);
 		const V3 albedo = base_colour(material, rgb, point) / 255.0f;
-		const V3 direct = direct_light(c, point, n, albedo, ignore);
+		const int entry = shading_append(dv.list_count);
+		dv.list[entry] = static_cast<int>(rec_index + level);
 		if (depth <= 0) {
-			result = direct;
-			break;
+			put_level(r, sub ? kLvSubEnd : kLvDiffuseEnd, point, n, ignore, albedo, entry);
+			return;
 		}
 		const V3 bounce = cosine_hemisphere(n, rng);
-		add[levels] = direct;
-		mul[levels] = albedo;
-		kind[levels++] = 2;
+		put_level(r, sub ? kLvSub : kLvDiffuse, point, n, ignore, albedo, entry);
 		origin = point + 1e-4f * bounce;
 		direction = bounce;
 		depth--;
 	}
-	for (int k = levels - 1; k >= 0; k--) {
-		if (kind[k] == 2)
-			result = add[k] + mul[k] * result;
-		else if (kind[k] == 1)
-			result = mul[k] * result;
-	}
-	return result;
 }
 
-// src/Renderer.cpp:1103-1117
-__device__ void sample_aperture(int blades, float u1, float u2, float &lx, float &ly) {
-	if (blades < 3) {
-		const float ang = 2.0f * 3.14159265f * u1, rad = sqrtf(u2);
-		lx = lm_cos(ang) * rad;
-		ly = lm_sin(ang) * rad;
-		return;
-	}
-	const int wedge = min(blades - 1, static_cast<int>(u1 * blades));
-	const float a0 = 2.0f * 3.14159265f * wedge / blades, a1 = 2.0f * 3.14159265f * (wedge + 1) / blades;
-	const float v0x = lm_cos(a0), v0y = lm_sin(a0), v1x = lm_cos(a1), v1y = lm_sin(a1);
-	float s = u1 * blades - wedge, t = u2;
-	if (s + t > 1.0f) {
-		s = 1.0f - s;
-		t = 1.0f - t;
-	}
-	lx = v0x * s + v1x * t;
-	ly = v0y * s + v1y * t;
-}
-
-__global__ void __launch_bounds__(128, 10) k_render_reference(SceneView sv, const float4 *__restrict__ ref_shade,
-                                                          const RefParams *__restrict__ params,
-                                                          uint32_t *__restrict__ argb, float *__restrict__ mean_rgb,
-                                                          int *status) {
+__global__ void __launch_bounds__(128) k_ref_paths(SceneView sv, const float4 *__restrict__ ref_shade,
+                                                   const RefParams *__restrict__ params, DeferView dv, int *status) {
 	const RefParams &p = *params;
-	const long pix = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-	if (pix >= static_cast<long>(p.width) * p.height)
+	const long li = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (li >= dv.npix)
 		return;
+	const long pix = dv.pix0 + li;
 	const int x = static_cast<int>(pix % p.width), y = static_cast<int>(pix / p.width);
 	Ctx c{sv, ref_shade, &p, 0};
-	MT rng;
-	rng.seed(static_cast<uint32_t>((static_cast<uint32_t>(y) * static_cast<uint32_t>(p.width) +
-	                                static_cast<uint32_t>(x)) *
-	                                   9781u +
-	                               1u));
-	const V3 right = mk(p.orient[0], p.orient[1], p.orient[2]);
-	const V3 upv = mk(p.orient[3], p.orient[4], p.orient[5]);
-	const V3 fwd = mk(p.orient[6], p.orient[7], p.orient[8]);
-	const V3 pos = l3(p.position);
-	const V3 motion = l3(p.camera_motion);
-	const float f = p.f;
+	MtFresh rng;
+	rng.seed(pixel_seed(x, y, p.width));
+	const CamBasis b = cam_basis(p);
+	for (int s = 0; s < p.samples; s++) {
+		V3 origin, dir;
+		camera_sample(p, b, x, y, rng, origin, dir);
+		record_path(c, origin, dir, rng, dv, (static_cast<size_t>(li) * p.samples + s) * dv.levels);
+	}
+	if (c.err)
+		atomicOr(status, 1);
+}
+
+__global__ void __launch_bounds__(128) k_ref_shadow(SceneView sv, const RefParams *__restrict__ params, DeferView dv,
+                                                    int *status) {
+	const RefParams &p = *params;
+	Ctx c{sv, nullptr, &p, 0};
+	const long total = static_cast<long>(*dv.list_count) * dv.taps;
+	for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+	     i += static_cast<long>(gridDim.x) * blockDim.x) {
+		const long e = i / dv.taps;
+		int k = static_cast<int>(i - e * dv.taps);
+		int l = 0;
+		for (int n = vis_tap_count(p.lights[0]); k >= n; n = vis_tap_count(p.lights[l])) {
+			k -= n;
+			l++;
+		}
+		const size_t ri = static_cast<size_t>(dv.list[e]);
+		const float4 r0 = dv.rec[3 * ri], r1 = dv.rec[3 * ri + 1];
+		const V3 point = mk(r0.x, r0.y, r0.z);
+		const VisTaps T = vis_taps(p.lights[l], point);
+		uint8_t occ = 0;
+		if (!T.all_visible) {
+			V3 dir;
+			float dist;
+			vis_tap(T, point, k, dir, dist);
+			occ = occluded(c, point, dir, dist, __float_as_int(r1.w)) ? 1 : 0;
+		}
+		dv.occl[i] = occ;
+	}
+	if (c.err)
+		atomicOr(status, 1);
+}
+
+__device__ __forceinline__ int unoccluded(const uint8_t *occ, int n) {
+	int u = 0;
+	for (int k = 0; k < n; k++)
+		u += occ[k] ? 0 : 1;
+	return u;
+}
+
+// directLight (src/Renderer.cpp:791-814) with each light's visibility counted from
+// the recorded taps.
+__device__ V3 direct_light_recorded(const RefParams &p, V3 point, V3 normal, V3 albedo, const uint8_t *occ) {
+	V3 sum = mk(0, 0, 0);
+	for (int li = 0; li < p.num_lights; li++) {
+		const RefLight &L = p.lights[li];
+		V3 ld;
+		float atten;
+		light_dir(L, point, ld, atten);
+		float cone = 1.0f;
+		if (L.type == kLightSpot)
+			cone = (dot(-ld, normalize(l3(L.direction))) > L.cone_cos) ? 1.0f : 0.0f;
+		const int n = vis_tap_count(L);
+		const float vis = vis_fraction(unoccluded(occ, n), n);
+		occ += n;
+		const float incidence = smax(0.0f, dot(normal, ld));
+		sum = sum + l3(L.colour) * (vis * cone * atten * incidence);
+	}
+	return albedo * vmin(sum, mk(1.0f, 1.0f, 1.0f));
+}
+
+// The subsurface branch's direct term (src/Renderer.cpp:857-880) with recorded visibility.
+__device__ V3 subsurface_recorded(Ctx &c, V3 point, V3 n, V3 albedo, int ignore, const uint8_t *occ) {
+	V3 shade = mk(0, 0, 0);
+	const float wrap = 0.5f;
+	for (int li = 0; li < c.p->num_lights; li++) {
+		const RefLight &L = c.p->lights[li];
+		const V3 to = l3(L.position) - point;
+		const float dist = length(to);
+		const V3 ld = to / dist;
+		const float atten = L.intensity / (L.atten_constant + L.atten_linear * dist + L.atten_quadratic * dist * dist);
+		const float wrap_diff = smax(0.0f, (dot(n, ld) + wrap) / (1.0f + wrap));
+		const int nt = vis_tap_count(L);
+		const float vis = vis_fraction(unoccluded(occ, nt), nt);
+		occ += nt;
+		shade = shade + albedo * l3(L.colour) * (vis * atten * wrap_diff);
+		const Hit ex = intersect(c, point - n * 1e-3f, ld, ignore);
+		const float thickness = ex.hit ? ex.t : 0.0f;
+		shade = shade + albedo * l3(L.colour) * (atten * lm_exp(-3.0f * thickness) * 0.6f);
+	}
+	return vmin(shade, mk(1.5f, 1.5f, 1.5f));
+}
+
+__global__ void __launch_bounds__(128) k_ref_fold(SceneView sv, const float4 *__restrict__ ref_shade,
+                                                  const RefParams *__restrict__ params, DeferView dv,
+                                                  uint32_t *__restrict__ argb, float *__restrict__ mean_rgb,
+                                                  int *status) {
+	const RefParams &p = *params;
+	const long li = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (li >= dv.npix)
+		return;
+	Ctx c{sv, ref_shade, &p, 0};
 	V3 sum = mk(0, 0, 0);
 	for (int s = 0; s < p.samples; s++) {
-		const float jx = rng.uniform(-0.5f, 0.5f);
-		const float jy = rng.uniform(-0.5f, 0.5f);
-		const float sx = static_cast<float>(x) + 0.5f + jx - static_cast<float>(p.width) / 2.0f;
-		const float sy = -(static_cast<float>(y) + 0.5f + jy - static_cast<float>(p.height) / 2.0f);
-		V3 ro, dir;
-		if (p.orthographic) {
-			const V3 v = mk(sx / f * p.ortho_scale, sy / f * p.ortho_scale, 0.0f);
-			ro = pos + (right * v.x + upv * v.y + fwd * v.z);
-			dir = normalize(right * 0.0f + upv * 0.0f + fwd * -1.0f);
-		} else {
-			const V3 v = mk(sx / f, sy / f, -1.0f);
-			ro = pos;
-			dir = normalize(right * v.x + upv * v.y + fwd * v.z);
-		}
-		const V3 cam = ro + motion * rng.uniform(0.0f, 1.0f);
-		V3 origin = cam;
-		if (p.aperture > 0.0f && !p.orthographic) {
-			const V3 focal = cam + dir * p.focus_distance;
-			// sampleAperture(blades, U(rng), U(rng)): GCC evaluates these two call
-			// arguments right to left, so the second argument is drawn first.
-			float ua, ub;
-			if (p.aperture_args_right_to_left) {
-				ub = rng.uniform(0.0f, 1.0f);
-				ua = rng.uniform(0.0f, 1.0f);
-			} else {
-				ua = rng.uniform(0.0f, 1.0f);
-				ub = rng.uniform(0.0f, 1.0f);
+		const float4 *rec = dv.rec + 3 * ((static_cast<size_t>(li) * p.samples + s) * dv.levels);
+		int last = 0;
+		while (__float_as_int(rec[3 * last].w) < kLvDiffuseEnd)
+			last++;
+		V3 result = mk(0, 0, 0);
+		for (int k = last; k >= 0; k--) {
+			const float4 r0 = rec[3 * k], r1 = rec[3 * k + 1], r2 = rec[3 * k + 2];
+			const int kind = __float_as_int(r0.w);
+			const V3 b = mk(r2.x, r2.y, r2.z);
+			if (kind == kLvValue) {
+				result = b;
+			} else if (kind == kLvMul) {
+				result = b * result;
+			} else if (kind != kLvPass) {
+				const V3 point = mk(r0.x, r0.y, r0.z), n = mk(r1.x, r1.y, r1.z);
+				const uint8_t *occ = dv.occl + static_cast<size_t>(__float_as_int(r2.w)) * dv.taps;
+				const V3 direct = (kind == kLvSub || kind == kLvSubEnd)
+				                      ? subsurface_recorded(c, point, n, b, __float_as_int(r1.w), occ)
+				                      : direct_light_recorded(p, point, n, b, occ);
+				result = (kind == kLvDiffuseEnd || kind == kLvSubEnd) ? direct : direct + b * result;
 			}
-			float lx, ly;
-			sample_aperture(p.aperture_blades, ua, ub, lx, ly);
-			lx = lx * p.aperture;
-			ly = ly * p.aperture;
-			origin = cam + (right * lx + upv * ly);
-			dir = normalize(focal - origin);
 		}
-		sum = sum + path_trace(c, origin, dir, rng);
+		sum = sum + result;
 	}
-	const V3 colour = sum / static_cast<float>(p.samples) * 255.0f;
-	const int r = min(255, cvt_trunc(colour.x));
-	const int g = min(255, cvt_trunc(colour.y));
-	const int b = min(255, cvt_trunc(colour.z));
-	argb[pix] = (255u << 24) | ((static_cast<uint32_t>(r) & 0xFFu) << 16) | ((static_cast<uint32_t>(g) & 0xFFu) << 8) |
-	            (static_cast<uint32_t>(b) & 0xFFu);
-	if (mean_rgb) {
-		const V3 m = sum / static_cast<float>(p.samples);
-		mean_rgb[3 * pix] = m.x;
-		mean_rgb[3 * pix + 1] = m.y;
-		mean_rgb[3 * pix + 2] = m.z;
-	}
+	store_pixel(dv.pix0 + li, sum, p.samples, argb, mean_rgb);
 	if (c.err)
 		atomicOr(status, 1);
 }
@@ -538,13 +673,50 @@ cudaError_t launch_render_raytraced(const SceneView &sv, const float4 *ref_shade
 	return cudaGetLastError();
 }
 
-cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade, const RefParams *d_params, int width,
-                                    int height, uint32_t *argb, float *mean_rgb, int *status, cudaStream_t st) {
-	const long n = static_cast<long>(width) * height;
+size_t ref_defer_bytes_per_pixel(const RefParams &p) {
+	int taps = 0;
+	for (int i = 0; i < p.num_lights; i++)
+		taps += ref_tap_count(p.lights[i]);
+	const size_t records = static_cast<size_t>(std::max(p.samples, 0)) * (p.max_depth + 1);
+	return records * (48 + 4 + static_cast<size_t>(taps));
+}
+
+cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade, const RefParams &p,
+                                    const RefParams *d_params, uint32_t *argb, float *mean_rgb, int *status,
+                                    void *scratch, size_t scratch_bytes, cudaStream_t st) {
+	const long n = static_cast<long>(p.width) * p.height;
 	if (n <= 0)
 		return cudaSuccess;
+	int taps = 0;
+	for (int i = 0; i < p.num_lights; i++)
+		taps += ref_tap_count(p.lights[i]);
+	// samples <= 0 records nothing; the fold then writes the reference's 0 / samples.
+	const size_t records = static_cast<size_t>(std::max(p.samples, 0)) * (p.max_depth + 1);
+	const size_t per_pixel = ref_defer_bytes_per_pixel(p);
+	const long chunk =
+	    per_pixel == 0 ? n : std::max<long>(1, std::min<long>(n, static_cast<long>((scratch_bytes - 1024) / per_pixel)));
+	char *base = static_cast<char *>(scratch);
+	DeferView dv;
+	dv.list_count = reinterpret_cast<unsigned *>(base);
+	base += 256;
+	dv.rec = reinterpret_cast<float4 *>(base);
+	base += (static_cast<size_t>(chunk) * records * 48 + 255) & ~size_t(255);
+	dv.list = reinterpret_cast<int *>(base);
+	base += (static_cast<size_t>(chunk) * records * 4 + 255) & ~size_t(255);
+	dv.occl = reinterpret_cast<uint8_t *>(base);
+	dv.levels = p.max_depth + 1;
+	dv.taps = taps;
 	const int bs = 128;
-	k_render_reference<<<ceil_div(n, bs), bs, 0, st>>>(sv, ref_shade, d_params, argb, mean_rgb, status);
+	for (long p0 = 0; p0 < n; p0 += chunk) {
+		dv.pix0 = p0;
+		dv.npix = std::min(chunk, n - p0);
+		cudaError_t e = cudaMemsetAsync(dv.list_count, 0, sizeof(unsigned), st);
+		if (e != cudaSuccess)
+			return e;
+		k_ref_paths<<<ceil_div(dv.npix, bs), bs, 0, st>>>(sv, ref_shade, d_params, dv, status);
+		k_ref_shadow<<<148 * 16, bs, 0, st>>>(sv, d_params, dv, status);
+		k_ref_fold<<<ceil_div(dv.npix, bs), bs, 0, st>>>(sv, ref_shade, d_params, dv, argb, mean_rgb, status);
+	}
 	return cudaGetLastError();
 }
 

@@ -64,7 +64,23 @@ cudaError_t launch_render_raytraced(const SceneView &sv, const float4 *ref_shade
                                     const RefParams *d_params, int width, int height, uint32_t *argb, int *status,
                                     cudaStream_t st);
 
-cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade, const RefParams *d_params, int width,
-                                    int height, uint32_t *argb, float *mean_rgb, int *status, cudaStream_t st);
+// Shadow rays a light's visibility pattern casts (src/Renderer.cpp:390-498).
+__host__ __device__ inline int ref_tap_count(const RefLight &L) {
+	if (L.type == kLightDirectional)
+		return 1;
+	if (L.type == kLightRectangle || L.type == kLightTriangle)
+		return 9;
+	if (L.radius <= 0.0f)
+		return 1;
+	return L.type == kLightVolume ? 12 : 9;
+}
+
+// The drop-in path tracer (renderPathTraced semantics) in three passes: paths,
+// shadow rays, fold. Scratch: at least ref_defer_bytes_per_pixel(p) + 1024 bytes;
+// larger images run in pixel chunks that fit.
+size_t ref_defer_bytes_per_pixel(const RefParams &p);
+cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade, const RefParams &p,
+                                    const RefParams *d_params, uint32_t *argb, float *mean_rgb, int *status,
+                                    void *scratch, size_t scratch_bytes, cudaStream_t st);
 
 } // namespace rnb

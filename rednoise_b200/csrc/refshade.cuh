@@ -105,6 +105,56 @@ struct MT {
 	}
 };
 
+// std::mt19937 for streams that are freshly seeded per pixel: the first 227
+// outputs of a seeded state's first twist depend only on the seed sequence
+// s[i], s[i + 1] and s[i + 397], which two running cursors over the seeding
+// recurrence provide in registers -- no 2.5 KB state is written or read. From
+// output 227 on (where the twist needs words it has already replaced) the full
+// state is built as MT does, so every output equals MT's.
+struct MtFresh {
+	uint32_t seed_v, a, b; // seed value; cursors: a = s[i], b = s[i + 397]
+	int i;                 // outputs drawn so far
+	bool full;
+	MT mt;
+	__device__ void seed(uint32_t v) {
+		seed_v = v;
+		a = v;
+		b = v;
+		for (int k = 1; k <= 397; k++)
+			b = 1812433253u * (b ^ (b >> 30)) + static_cast<uint32_t>(k);
+		i = 0;
+		full = false;
+	}
+	__device__ uint32_t next() {
+		if (!full) {
+			if (i < 227) {
+				const uint32_t a1 = 1812433253u * (a ^ (a >> 30)) + static_cast<uint32_t>(i + 1);
+				const uint32_t y0 = (a & 0x80000000u) | (a1 & 0x7fffffffu);
+				uint32_t y = b ^ (y0 >> 1) ^ ((y0 & 1u) ? 0x9908b0dfu : 0u);
+				a = a1;
+				b = 1812433253u * (b ^ (b >> 30)) + static_cast<uint32_t>(i + 398);
+				i++;
+				y ^= y >> 11;
+				y ^= (y << 7) & 0x9d2c5680u;
+				y ^= (y << 15) & 0xefc60000u;
+				y ^= y >> 18;
+				return y;
+			}
+			mt.seed(seed_v);
+			mt.twist();
+			mt.i = 227;
+			full = true;
+		}
+		return mt.next();
+	}
+	__device__ float uniform(float lo, float hi) {
+		float c = __uint2float_rn(next()) / 4294967296.0f;
+		if (c >= 1.0f)
+			c = 0.99999994f;
+		return c * (hi - lo) + lo;
+	}
+};
+
 // ---- Ken Perlin's improved noise (2002), as the reference's procedural colour uses ----
 __constant__ uint8_t kPerm[256] = {
     151, 160, 137, 91,  90,  15,  131, 13,  201, 95,  96,  53,  194, 233, 7,   225, 140, 36,  103, 30,  69,  142,
@@ -191,6 +241,124 @@ __device__ __forceinline__ bool occluded(Ctx &c, V3 o, V3 d, float maxd, int ign
 }
 
 __device__ __forceinline__ V3 l3(const float *a) { return mk(a[0], a[1], a[2]); }
+
+// The shadow-ray patterns of visibility (src/Renderer.cpp:390-498) one tap at a
+// time, for renderers that trace the taps in a separate pass: a light's taps and,
+// for tap k, the direction and length of its ray from the shading point, each
+// formed with the reference's operations (the same rays visibility() below traces
+// in its per-pattern loops).
+struct VisTaps {
+	int kind; // 0 single ray, 1 rectangle, 2 triangle, 3 volume cone, 4 disk
+	int n;
+	bool all_visible; // volume light enclosing the point: visibility 1 without rays
+	V3 pos, a, b, dir; // rectangle/triangle: u, v axes; disk and volume: tangent, bitangent
+	float d, ct0, st0, ct1, st1, radius;
+};
+
+// Taps per light for the pattern of light L (the count does not depend on the point).
+__device__ __forceinline__ int vis_tap_count(const RefLight &L) { return ref_tap_count(L); }
+
+__device__ __forceinline__ VisTaps vis_taps(const RefLight &L, V3 point) {
+	VisTaps T;
+	T.all_visible = false;
+	T.n = vis_tap_count(L);
+	T.pos = l3(L.position);
+	if (L.type == kLightDirectional) {
+		T.kind = 0;
+		T.dir = -normalize(l3(L.direction));
+		T.d = 1e6f;
+		return T;
+	}
+	if (L.type == kLightRectangle || L.type == kLightTriangle) {
+		T.kind = L.type == kLightRectangle ? 1 : 2;
+		T.a = l3(L.u_axis);
+		T.b = l3(L.v_axis);
+		return T;
+	}
+	if (L.radius <= 0.0f) {
+		T.kind = 0;
+		const V3 to = T.pos - point;
+		T.d = length(to);
+		T.dir = to / T.d;
+		return T;
+	}
+	if (L.type == kLightVolume) {
+		T.kind = 3;
+		const V3 toc = T.pos - point;
+		T.d = length(toc);
+		T.dir = toc / T.d;
+		const float sin_max = smin(1.0f, L.radius / T.d);
+		if (sin_max >= 1.0f) {
+			T.all_visible = true;
+			return T;
+		}
+		const float cos_max = sqrtf(smax(0.0f, 1.0f - sin_max * sin_max));
+		const V3 up = fabsf(T.dir.y) < 0.99f ? mk(0, 1, 0) : mk(1, 0, 0);
+		T.a = normalize(cross(up, T.dir));
+		T.b = cross(T.dir, T.a);
+		T.ct0 = 1.0f - 0.85f * (1.0f - cos_max);
+		T.st0 = sqrtf(smax(0.0f, 1.0f - T.ct0 * T.ct0));
+		T.ct1 = 1.0f - 0.4f * (1.0f - cos_max);
+		T.st1 = sqrtf(smax(0.0f, 1.0f - T.ct1 * T.ct1));
+		return T;
+	}
+	// Disk light: fixed 9-point pattern (src/Renderer.cpp:483-497).
+	T.kind = 4;
+	T.radius = L.radius;
+	const V3 axis = normalize(point - T.pos);
+	const V3 up = fabsf(axis.y) < 0.99f ? mk(0, 1, 0) : mk(1, 0, 0);
+	T.a = normalize(cross(up, axis));
+	T.b = cross(axis, T.a);
+	return T;
+}
+
+__device__ __forceinline__ void vis_tap(const VisTaps &T, V3 point, int k, V3 &dir, float &dist) {
+	if (T.kind == 0) {
+		dir = T.dir;
+		dist = T.d;
+		return;
+	}
+	if (T.kind == 3) {
+		if (k == 0) {
+			dir = T.dir;
+		} else {
+			// rings of 5 (offset 0) and 6 (offset 0.5) directions
+			const float kPi = 3.14159265358979323846f;
+			const bool outer = k > 5;
+			const int i = outer ? k - 6 : k - 1;
+			const int count = outer ? 6 : 5;
+			const float off = outer ? 0.5f : 0.0f;
+			const float ct = outer ? T.ct1 : T.ct0, st = outer ? T.st1 : T.st0;
+			const float phi = 2.0f * kPi * ((static_cast<float>(i) + off) / static_cast<float>(count));
+			const V3 sd = T.dir * ct + (T.a * lm_cos(phi) + T.b * lm_sin(phi)) * st;
+			dir = normalize(sd);
+		}
+		dist = T.d;
+		return;
+	}
+	V3 sp;
+	if (T.kind == 1) {
+		const float gx = static_cast<float>(k % 3 - 1), gy = static_cast<float>(k / 3 - 1);
+		sp = T.pos + T.a * gx + T.b * gy;
+	} else if (T.kind == 2) {
+		const float bx[9] = {0.0f, 1.0f, 0.0f, 0.5f, 0.0f, 0.5f, 0.25f, 0.5f, 1.0f / 3.0f};
+		const float by[9] = {0.0f, 0.0f, 1.0f, 0.0f, 0.5f, 0.5f, 0.25f, 0.25f, 1.0f / 3.0f};
+		sp = T.pos + T.a * bx[k] + T.b * by[k];
+	} else {
+		const float sx[9] = {0, 1, -1, 0, 0, 0.7f, -0.7f, 0.7f, -0.7f};
+		const float sy[9] = {0, 0, 0, 1, -1, 0.7f, 0.7f, -0.7f, -0.7f};
+		sp = T.pos + (T.a * sx[k] + T.b * sy[k]) * T.radius;
+	}
+	const V3 to = sp - point;
+	dist = length(to);
+	dir = to / dist;
+}
+
+// visibility from the number of unoccluded taps: unocc / 9.0f, unocc / 12 or the
+// single ray's 0 / 1, as the reference divides.
+__device__ __forceinline__ float vis_fraction(int unocc, int n) {
+	return static_cast<float>(unocc) / static_cast<float>(n);
+}
 
 // src/Renderer.cpp:390-498
 __device__ float visibility(Ctx &c, const RefLight &L, V3 point, int ignore) {
@@ -332,7 +500,7 @@ __device__ V3 cosine_hemisphere_u(V3 n, float u1, float u2) {
 	return normalize(t * x + b * y + n * z);
 }
 
-__device__ V3 cosine_hemisphere(V3 n, MT &rng) {
+template <class Rng> __device__ V3 cosine_hemisphere(V3 n, Rng &rng) {
 	const float u1 = rng.uniform(0.0f, 1.0f), u2 = rng.uniform(0.0f, 1.0f);
 	return cosine_hemisphere_u(n, u1, u2);
 }

@@ -135,6 +135,35 @@ def test_reference_mode_depth_of_field_and_motion(assets):
         agree(argb_to_rgba(got), argb_to_rgba(want))
 
 
+def test_reference_mode_long_pixel_streams_match_reference_live(assets):
+    """96 spp draws about a thousand numbers per pixel: past the first twist's 227
+    outputs (computed without a state array) and into the second twist."""
+    v9 = assets["cornell_v"]
+    m = oracle.RefModel.from_arrays(v9, assets["cornell_rgb"], assets["cornell_material"],
+                                    assets["cornell_roughness"], assets["cornell_normal"])
+    s = rn.Scene.from_arrays(v9, ref_rgb=assets["cornell_rgb"], ref_material=assets["cornell_material"],
+                             ref_normal=assets["cornell_normal"], ref_roughness=assets["cornell_roughness"])
+    want = m.render(24, 18, 96)
+    got = s.render_reference(24, 18, 96)
+    m.close()
+    agree(argb_to_rgba(got), argb_to_rgba(want), min_equal=0.999, max_outlier_frac=0.001)
+
+
+def test_reference_mode_pixel_chunks(assets):
+    """1024 x 1024 at 64 spp needs several pixel chunks of path records; the last
+    rows (in the last chunk) equal the oracle's rows, which equal the reference's."""
+    v9 = assets["cornell_v"]
+    s = rn.Scene.from_arrays(v9, ref_rgb=assets["cornell_rgb"], ref_material=assets["cornell_material"],
+                             ref_normal=assets["cornell_normal"], ref_roughness=assets["cornell_roughness"])
+    w = h = 1024
+    got = s.render_reference(w, h, 64)
+    orc = oracle.OrcBvh(v9)
+    for y0 in (0, h - 3):
+        want = orc.render_reference(assets["cornell_normal"], assets["cornell_material"], assets["cornell_rgb"],
+                                    assets["cornell_roughness"], w, h, 64, y0=y0, y1=y0 + 3)
+        agree(argb_to_rgba(got[y0:y0 + 3]), argb_to_rgba(want), min_equal=0.999, max_outlier_frac=0.001)
+
+
 def test_mean_taps_are_consistent(assets):
     v9 = assets["cornell_v"]
     s = rn.Scene.from_arrays(v9, ref_rgb=assets["cornell_rgb"], ref_material=assets["cornell_material"],
