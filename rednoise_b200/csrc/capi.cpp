@@ -177,7 +177,8 @@ rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *prm, u
 	// Path records and shadow-ray results: the whole frame when it fits in 2 GiB,
 	// else pixel chunks.
 	const size_t per_pixel = ref_defer_bytes_per_pixel(p);
-	const size_t defer = 1024 + std::min(static_cast<size_t>(npix) * per_pixel, std::max(size_t(2) << 30, per_pixel));
+	const size_t defer =
+	    kRefDeferFixedBytes + std::min(static_cast<size_t>(npix) * per_pixel, std::max(size_t(2) << 30, per_pixel));
 	const size_t head = 256 + ((sizeof(RefParams) + 255) & ~size_t(255)) + ((static_cast<size_t>(npix) * 4 + 255) &
 	                    ~size_t(255)) + ((static_cast<size_t>(npix) * 12 + 255) & ~size_t(255));
 	RNB_CUDA(scene->scratch.ensure(head + defer));

@@ -130,11 +130,16 @@ __device__ __forceinline__ uint32_t pixel_seed(int x, int y, int width) {
 // shading entry).
 enum LevelKind : int { kLvPass = 0, kLvMul = 1, kLvDiffuse = 2, kLvSub = 3, kLvDiffuseEnd = 4, kLvSubEnd = 5, kLvValue = 6 };
 
+constexpr int kShadeKeyBits = 15; // 5 bits per axis of the scene box
+
 struct DeferView {
 	float4 *rec;
 	int *list;
 	unsigned *list_count;
 	uint8_t *occl;
+	uint16_t *key;    // per shading entry: Morton cell of its point
+	int *sorted;      // shading entries ordered by cell
+	unsigned *bins;   // 2^kShadeKeyBits counters, then offsets
 	int levels;
 	int taps;
 	long pix0;
@@ -150,6 +155,25 @@ __device__ __forceinline__ int shading_append(unsigned *count) {
 		base = atomicAdd(count, static_cast<unsigned>(__popc(mask)));
 	base = __shfl_sync(mask, base, leader);
 	return static_cast<int>(base) + __popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ uint32_t spread5(uint32_t v) {
+	v &= 31u;
+	v = (v | (v << 8)) & 0x100Fu;
+	v = (v | (v << 4)) & 0x10C3u;
+	v = (v | (v << 2)) & 0x1249u;
+	return v;
+}
+// 15-bit Morton cell of a point in the scene's root box (5 bits per axis).
+__device__ __forceinline__ uint16_t shade_key(const SceneView &sv, V3 p) {
+	const float q[3] = {p.x, p.y, p.z};
+	uint32_t c[3];
+	for (int a = 0; a < 3; a++) {
+		const float ext = sv.root_hi[a] - sv.root_lo[a];
+		const float f = ext > 0.0f ? (q[a] - sv.root_lo[a]) / ext : 0.0f;
+		c[a] = static_cast<uint32_t>(fminf(fmaxf(f * 32.0f, 0.0f), 31.0f));
+	}
+	return static_cast<uint16_t>(spread5(c[0]) | (spread5(c[1]) << 1) | (spread5(c[2]) << 2));
 }
 
 __device__ __forceinline__ void put_level(float4 *r, int kind, V3 a, V3 n, int ignore, V3 b, int entry) {
@@ -238,6 +262,7 @@ __device__ void record_path(Ctx &c, V3 origin, V3 direction, Rng &rng, const Def
 		const V3 albedo = base_colour(material, rgb, point) / 255.0f;
 		const int entry = shading_append(dv.list_count);
 		dv.list[entry] = static_cast<int>(rec_index + level);
+		dv.key[entry] = shade_key(c.sv, point);
 		if (depth <= 0) {
 			put_level(r, sub ? kLvSubEnd : kLvDiffuseEnd, point, n, ignore, albedo, entry);
 			return;
@@ -271,6 +296,43 @@ __global__ void __launch_bounds__(128) k_ref_paths(SceneView sv, const float4 *_
 		atomicOr(status, 1);
 }
 
+// Counting sort of the shading entries by cell, so that a warp's shadow rays
+// start from nearby points.
+__global__ void k_shade_count(DeferView dv) {
+	const long n = *dv.list_count;
+	for (long e = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+	     e += static_cast<long>(gridDim.x) * blockDim.x)
+		atomicAdd(dv.bins + dv.key[e], 1u);
+}
+__global__ void __launch_bounds__(1024) k_shade_scan(DeferView dv) {
+	constexpr int kBins = 1 << kShadeKeyBits, kPer = kBins / 1024;
+	__shared__ unsigned part[1024];
+	const int t = threadIdx.x;
+	unsigned sum = 0;
+	for (int j = 0; j < kPer; j++)
+		sum += dv.bins[t * kPer + j];
+	part[t] = sum;
+	__syncthreads();
+	for (int off = 1; off < 1024; off <<= 1) {
+		const unsigned v = t >= off ? part[t - off] : 0u;
+		__syncthreads();
+		part[t] += v;
+		__syncthreads();
+	}
+	unsigned run = part[t] - sum; // exclusive prefix of this thread's bins
+	for (int j = 0; j < kPer; j++) {
+		const unsigned c = dv.bins[t * kPer + j];
+		dv.bins[t * kPer + j] = run;
+		run += c;
+	}
+}
+__global__ void k_shade_scatter(DeferView dv) {
+	const long n = *dv.list_count;
+	for (long e = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+	     e += static_cast<long>(gridDim.x) * blockDim.x)
+		dv.sorted[atomicAdd(dv.bins + dv.key[e], 1u)] = static_cast<int>(e);
+}
+
 __global__ void __launch_bounds__(128) k_ref_shadow(SceneView sv, const RefParams *__restrict__ params, DeferView dv,
                                                     int *status) {
 	const RefParams &p = *params;
@@ -278,8 +340,9 @@ __global__ void __launch_bounds__(128) k_ref_shadow(SceneView sv, const RefParam
 	const long total = static_cast<long>(*dv.list_count) * dv.taps;
 	for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
 	     i += static_cast<long>(gridDim.x) * blockDim.x) {
-		const long e = i / dv.taps;
-		int k = static_cast<int>(i - e * dv.taps);
+		const long slot = i / dv.taps;
+		int k = static_cast<int>(i - slot * dv.taps);
+		const long e = dv.sorted[slot];
 		int l = 0;
 		for (int n = vis_tap_count(p.lights[0]); k >= n; n = vis_tap_count(p.lights[l])) {
 			k -= n;
@@ -296,7 +359,7 @@ __global__ void __launch_bounds__(128) k_ref_shadow(SceneView sv, const RefParam
 			vis_tap(T, point, k, dir, dist);
 			occ = occluded(c, point, dir, dist, __float_as_int(r1.w)) ? 1 : 0;
 		}
-		dv.occl[i] = occ;
+		dv.occl[e * dv.taps + (i - slot * dv.taps)] = occ;
 	}
 	if (c.err)
 		atomicOr(status, 1);
@@ -678,7 +741,7 @@ size_t ref_defer_bytes_per_pixel(const RefParams &p) {
 	for (int i = 0; i < p.num_lights; i++)
 		taps += ref_tap_count(p.lights[i]);
 	const size_t records = static_cast<size_t>(std::max(p.samples, 0)) * (p.max_depth + 1);
-	return records * (48 + 4 + static_cast<size_t>(taps));
+	return records * (48 + 4 + 2 + 4 + static_cast<size_t>(taps));
 }
 
 cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade, const RefParams &p,
@@ -693,15 +756,21 @@ cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade
 	// samples <= 0 records nothing; the fold then writes the reference's 0 / samples.
 	const size_t records = static_cast<size_t>(std::max(p.samples, 0)) * (p.max_depth + 1);
 	const size_t per_pixel = ref_defer_bytes_per_pixel(p);
-	const long chunk =
-	    per_pixel == 0 ? n : std::max<long>(1, std::min<long>(n, static_cast<long>((scratch_bytes - 1024) / per_pixel)));
+	const long fit = per_pixel == 0 ? n : static_cast<long>((scratch_bytes - kRefDeferFixedBytes) / per_pixel);
+	const long chunk = std::max<long>(1, std::min<long>(n, fit));
 	char *base = static_cast<char *>(scratch);
 	DeferView dv;
 	dv.list_count = reinterpret_cast<unsigned *>(base);
 	base += 256;
+	dv.bins = reinterpret_cast<unsigned *>(base);
+	base += sizeof(unsigned) << kShadeKeyBits;
 	dv.rec = reinterpret_cast<float4 *>(base);
 	base += (static_cast<size_t>(chunk) * records * 48 + 255) & ~size_t(255);
 	dv.list = reinterpret_cast<int *>(base);
+	base += (static_cast<size_t>(chunk) * records * 4 + 255) & ~size_t(255);
+	dv.key = reinterpret_cast<uint16_t *>(base);
+	base += (static_cast<size_t>(chunk) * records * 2 + 255) & ~size_t(255);
+	dv.sorted = reinterpret_cast<int *>(base);
 	base += (static_cast<size_t>(chunk) * records * 4 + 255) & ~size_t(255);
 	dv.occl = reinterpret_cast<uint8_t *>(base);
 	dv.levels = p.max_depth + 1;
@@ -713,7 +782,13 @@ cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade
 		cudaError_t e = cudaMemsetAsync(dv.list_count, 0, sizeof(unsigned), st);
 		if (e != cudaSuccess)
 			return e;
+		e = cudaMemsetAsync(dv.bins, 0, sizeof(unsigned) << kShadeKeyBits, st);
+		if (e != cudaSuccess)
+			return e;
 		k_ref_paths<<<ceil_div(dv.npix, bs), bs, 0, st>>>(sv, ref_shade, d_params, dv, status);
+		k_shade_count<<<148 * 8, 256, 0, st>>>(dv);
+		k_shade_scan<<<1, 1024, 0, st>>>(dv);
+		k_shade_scatter<<<148 * 8, 256, 0, st>>>(dv);
 		k_ref_shadow<<<148 * 16, bs, 0, st>>>(sv, d_params, dv, status);
 		k_ref_fold<<<ceil_div(dv.npix, bs), bs, 0, st>>>(sv, ref_shade, d_params, dv, argb, mean_rgb, status);
 	}

@@ -76,8 +76,9 @@ __host__ __device__ inline int ref_tap_count(const RefLight &L) {
 }
 
 // The drop-in path tracer (renderPathTraced semantics) in three passes: paths,
-// shadow rays, fold. Scratch: at least ref_defer_bytes_per_pixel(p) + 1024 bytes;
-// larger images run in pixel chunks that fit.
+// shadow rays, fold. Scratch: at least ref_defer_bytes_per_pixel(p) +
+// kRefDeferFixedBytes; larger images run in pixel chunks that fit.
+constexpr size_t kRefDeferFixedBytes = 256 + (size_t(4) << 15) + 2048;
 size_t ref_defer_bytes_per_pixel(const RefParams &p);
 cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade, const RefParams &p,
                                     const RefParams *d_params, uint32_t *argb, float *mean_rgb, int *status,
