@@ -149,18 +149,19 @@ def test_reference_mode_long_pixel_streams_match_reference_live(assets):
     agree(argb_to_rgba(got), argb_to_rgba(want), min_equal=0.999, max_outlier_frac=0.001)
 
 
-def test_reference_mode_pixel_chunks(assets):
-    """1024 x 1024 at 64 spp needs several pixel chunks of path records; the last
-    rows (in the last chunk) equal the oracle's rows, which equal the reference's."""
+@pytest.mark.parametrize("spp", [16, 64])
+def test_reference_mode_pixel_chunks(assets, spp):
+    """1024 x 1024 at 16 and 64 spp needs several pixel chunks of path records; the
+    first and last rows equal the oracle's rows, which equal the reference's."""
     v9 = assets["cornell_v"]
     s = rn.Scene.from_arrays(v9, ref_rgb=assets["cornell_rgb"], ref_material=assets["cornell_material"],
                              ref_normal=assets["cornell_normal"], ref_roughness=assets["cornell_roughness"])
     w = h = 1024
-    got = s.render_reference(w, h, 64)
+    got = s.render_reference(w, h, spp)
     orc = oracle.OrcBvh(v9)
     for y0 in (0, h - 3):
         want = orc.render_reference(assets["cornell_normal"], assets["cornell_material"], assets["cornell_rgb"],
-                                    assets["cornell_roughness"], w, h, 64, y0=y0, y1=y0 + 3)
+                                    assets["cornell_roughness"], w, h, spp, y0=y0, y1=y0 + 3)
         agree(argb_to_rgba(got[y0:y0 + 3]), argb_to_rgba(want), min_equal=0.999, max_outlier_frac=0.001)
 
 
