@@ -137,6 +137,7 @@ struct DeferView {
 	int *list;
 	unsigned *list_count;
 	uint8_t *occl;
+	unsigned *pix_next; // next pixel of the chunk for the path pass to take
 	uint16_t *key;    // per shading entry: Morton cell of its point
 	int *sorted;      // shading entries ordered by cell
 	unsigned *bins;   // 2^kShadeKeyBits counters, then offsets
@@ -275,22 +276,26 @@ __device__ void record_path(Ctx &c, V3 origin, V3 direction, Rng &rng, const Def
 	}
 }
 
+// Persistent: a lane that has finished its pixel takes the next one, so lanes
+// whose paths end early do not idle until the warp's longest pixel is done.
 __global__ void __launch_bounds__(128) k_ref_paths(SceneView sv, const float4 *__restrict__ ref_shade,
                                                    const RefParams *__restrict__ params, DeferView dv, int *status) {
 	const RefParams &p = *params;
-	const long li = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-	if (li >= dv.npix)
-		return;
-	const long pix = dv.pix0 + li;
-	const int x = static_cast<int>(pix % p.width), y = static_cast<int>(pix / p.width);
 	Ctx c{sv, ref_shade, &p, 0};
-	MtFresh rng;
-	rng.seed(pixel_seed(x, y, p.width));
 	const CamBasis b = cam_basis(p);
-	for (int s = 0; s < p.samples; s++) {
-		V3 origin, dir;
-		camera_sample(p, b, x, y, rng, origin, dir);
-		record_path(c, origin, dir, rng, dv, (static_cast<size_t>(li) * p.samples + s) * dv.levels);
+	for (;;) {
+		const long li = atomicAdd(dv.pix_next, 1u);
+		if (li >= dv.npix)
+			break;
+		const long pix = dv.pix0 + li;
+		const int x = static_cast<int>(pix % p.width), y = static_cast<int>(pix / p.width);
+		MtFresh rng;
+		rng.seed(pixel_seed(x, y, p.width));
+		for (int s = 0; s < p.samples; s++) {
+			V3 origin, dir;
+			camera_sample(p, b, x, y, rng, origin, dir);
+			record_path(c, origin, dir, rng, dv, (static_cast<size_t>(li) * p.samples + s) * dv.levels);
+		}
 	}
 	if (c.err)
 		atomicOr(status, 1);
@@ -761,6 +766,7 @@ cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade
 	char *base = static_cast<char *>(scratch);
 	DeferView dv;
 	dv.list_count = reinterpret_cast<unsigned *>(base);
+	dv.pix_next = dv.list_count + 1;
 	base += 256;
 	dv.bins = reinterpret_cast<unsigned *>(base);
 	base += sizeof(unsigned) << kShadeKeyBits;
@@ -779,13 +785,13 @@ cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade
 	for (long p0 = 0; p0 < n; p0 += chunk) {
 		dv.pix0 = p0;
 		dv.npix = std::min(chunk, n - p0);
-		cudaError_t e = cudaMemsetAsync(dv.list_count, 0, sizeof(unsigned), st);
+		cudaError_t e = cudaMemsetAsync(dv.list_count, 0, 2 * sizeof(unsigned), st);
 		if (e != cudaSuccess)
 			return e;
 		e = cudaMemsetAsync(dv.bins, 0, sizeof(unsigned) << kShadeKeyBits, st);
 		if (e != cudaSuccess)
 			return e;
-		k_ref_paths<<<ceil_div(dv.npix, bs), bs, 0, st>>>(sv, ref_shade, d_params, dv, status);
+		k_ref_paths<<<std::min(ceil_div(dv.npix, bs), 148 * 8), bs, 0, st>>>(sv, ref_shade, d_params, dv, status);
 		k_shade_count<<<148 * 8, 256, 0, st>>>(dv);
 		k_shade_scan<<<1, 1024, 0, st>>>(dv);
 		k_shade_scatter<<<148 * 8, 256, 0, st>>>(dv);
