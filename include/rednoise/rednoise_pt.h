@@ -193,6 +193,13 @@ rn_status rn_pt_render_raytraced(rn_scene *scene, const rn_pt_ref_params *params
 rn_status rn_pt_render_photon_mapped(rn_scene *scene, const rn_pt_ref_params *params, int num_photons, int gather_rays,
                                      unsigned flags, void *stream, uint32_t *argb, unsigned *num_stored);
 
+/* Testing hook, no reference counterpart: after `after` more successful device
+ * allocations the next one fails as if the device were out of memory (the call
+ * that made it returns RN_ERR_OUT_OF_MEMORY), once; after < 0 turns it off. For
+ * checking that every call fails cleanly and the library stays usable after a
+ * failed allocation. Process-wide; not for use while other threads render. */
+rn_status rn_pt_inject_allocation_failure(long long after);
+
 /* Random-number streams of rn_pt_render_bidirectional. */
 #define RN_PT_RNG_REFERENCE 0 /* the reference's std::mt19937(9871 + y) per image row: the reference's canvas */
 #define RN_PT_RNG_COUNTER 1   /* Philox-4x32-10 per (pixel, sample) under `seed`: same estimator, fully parallel */

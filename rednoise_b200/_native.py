@@ -13,6 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "librednoise_b200.so")
 
 RN_OK = 0
+RN_ERR_OUT_OF_MEMORY = 3
 RN_PT_DEVICE_POINTERS = 1
 RN_PT_ORDER_NEAREST = 2
 RN_PT_WIDTH2 = 4
@@ -243,6 +244,7 @@ SIGNATURES = {
     "rn_pt_accum_resolve": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, vp]),
     "rn_pt_render_photon_mapped": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_uint, vp, vp, vp]),
+    "rn_pt_inject_allocation_failure": (ctypes.c_int, [ctypes.c_longlong]),
     "rn_pt_render_bidirectional": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_int, ctypes.c_float,
                                                   ctypes.c_int, ctypes.c_ulonglong, ctypes.c_uint, vp, vp, vp]),
     "rn_pt_render_metropolis": (ctypes.c_int, [vp, ctypes.POINTER(RefParams), ctypes.c_longlong, ctypes.c_float,

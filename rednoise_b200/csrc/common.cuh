@@ -15,6 +15,10 @@ namespace rnb {
 void set_last_error(const std::string &msg);
 const char *get_last_error();
 
+// Testing hook (rn_pt_inject_allocation_failure): true when this device
+// allocation is the one chosen to fail.
+bool injected_allocation_failure();
+
 // Record a CUDA failure and map it to a status.
 rn_status cuda_fail(cudaError_t e, const char *what);
 
@@ -44,6 +48,8 @@ struct DevBuf {
 		if (n <= bytes)
 			return cudaSuccess;
 		release();
+		if (injected_allocation_failure())
+			return cudaErrorMemoryAllocation;
 		cudaError_t e = cudaMalloc(&p, n);
 		if (e == cudaSuccess)
 			bytes = n;

@@ -1,4 +1,5 @@
 // rn_scene lifetime, lazy device preparation and the ray-query entry points.
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -16,6 +17,19 @@ thread_local std::string g_last_error;
 
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 const char *get_last_error() { return g_last_error.c_str(); }
+
+namespace {
+std::atomic<long long> g_alloc_countdown{-1};
+} // namespace
+
+bool injected_allocation_failure() {
+	long long v = g_alloc_countdown.load();
+	while (v >= 0) {
+		if (g_alloc_countdown.compare_exchange_weak(v, v - 1))
+			return v == 0;
+	}
+	return false;
+}
 
 rn_status cuda_fail(cudaError_t e, const char *what) {
 	set_last_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
@@ -421,6 +435,7 @@ rn_status rn_pt_scene_build_lbvh(rn_scene *scene, void *stream, double *build_ms
 	float *d_v9 = scene->scratch.as<float>();
 	RNB_CUDA(cudaMemcpyAsync(d_v9, scene->tris.v.data(), scene->tris.v.size() * sizeof(float), cudaMemcpyHostToDevice,
 	                         cs));
+	scene->lbvh_ready = false; // the buffers below may move; the view is rebuilt on success
 	RNB_CUDA(scene->d_lbvh_nodes.ensure(static_cast<size_t>(n > 1 ? n - 1 : 1) * 4 * sizeof(float4)));
 	RNB_CUDA(scene->d_lbvh_tris.ensure(static_cast<size_t>(n) * 3 * sizeof(float4)));
 	LbvhResult res{};
@@ -554,3 +569,8 @@ rn_status rn_pt_trace_any(rn_scene *scene, int n, const float *origins, const fl
 }
 
 } // extern "C"
+
+rn_status rn_pt_inject_allocation_failure(long long after) {
+	g_alloc_countdown.store(after < 0 ? -1 : after);
+	return RN_OK;
+}

@@ -22,6 +22,9 @@ rn_status WfContext::ensure_pool(int capacity) {
 	if (capacity <= capacity_)
 		return RN_OK;
 	release_graph();
+	// The buffers grow one by one and a grown buffer frees its old memory: until
+	// all of them have grown, the pool describes no usable capacity.
+	capacity_ = 0;
 	const size_t n = static_cast<size_t>(capacity);
 	RNB_CUDA(o_.ensure(n * 16));
 	RNB_CUDA(d_.ensure(n * 16));
