@@ -213,6 +213,12 @@ struct Mtl {
 	int r = 0, g = 0, b = 0;
 };
 
+// int(x) as the reference's x86-64 build converts (cvttss2si): truncation, and
+// INT_MIN for NaN and values outside the int range (a C++ cast would be undefined).
+int x86_float_to_int(float x) {
+	return (x >= -2147483648.0f && x < 2147483648.0f) ? static_cast<int>(x) : static_cast<int>(0x80000000u);
+}
+
 bool parse_int_prefix(const std::string &s, int &out) {
 	// std::stoi semantics on the leading integer (leading spaces and sign allowed).
 	const char *p = s.c_str();
@@ -246,9 +252,9 @@ std::map<std::string, Mtl> load_mtl(const std::string &path) {
 			float r = 0, g = 0, b = 0;
 			ss >> r >> g >> b;
 			Mtl m;
-			m.r = static_cast<int>(r * 255);
-			m.g = static_cast<int>(g * 255);
-			m.b = static_cast<int>(b * 255);
+			m.r = x86_float_to_int(r * 255);
+			m.g = x86_float_to_int(g * 255);
+			m.b = x86_float_to_int(b * 255);
 			out[cur] = m;
 		}
 	}
