@@ -7,6 +7,7 @@
 #include "pt_kernels.hpp"
 #include "render_impl.hpp"
 #include "scene_impl.hpp"
+#include "trace_range.hpp"
 
 struct rn_pt_batch {
 	std::vector<rn_pt_job> jobs;
@@ -148,6 +149,7 @@ rn_status autotune_batch(rn_pt_batch *b, int max_spp, long total_pix) {
 extern "C" {
 
 rn_status rn_pt_batch_create(const rn_pt_job *jobs, int n, int integrator, unsigned flags, rn_pt_batch **out) {
+	TraceRange trace_range("rn_pt_batch_create");
 	if (!jobs || n <= 0 || !out) {
 		set_last_error("rn_pt_batch_create: need n > 0 jobs and an output pointer");
 		return RN_ERR_INVALID_ARGUMENT;
@@ -222,6 +224,7 @@ rn_status rn_pt_batch_create(const rn_pt_job *jobs, int n, int integrator, unsig
 
 rn_status rn_pt_batch_render(rn_pt_batch *b, unsigned sample_offset, unsigned flags, void *stream,
                              float *const *out) {
+	TraceRange trace_range("rn_pt_batch_render");
 	if (!b || !out) {
 		set_last_error("rn_pt_batch_render: NULL argument");
 		return RN_ERR_INVALID_ARGUMENT;

@@ -10,6 +10,7 @@
 #include "photon.hpp"
 #include "refmode.hpp"
 #include "scene_impl.hpp"
+#include "trace_range.hpp"
 
 using namespace rnb;
 
@@ -128,6 +129,7 @@ void rn_pt_ref_params_init(rn_pt_ref_params *p, int width, int height, float cam
 
 rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *prm, unsigned flags, void *stream,
                                  uint32_t *argb, float *mean_rgb) {
+	TraceRange trace_range("rn_pt_render_reference");
 	if (!scene || !prm || prm->width <= 0 || prm->height <= 0 || (!argb && !mean_rgb)) {
 		set_last_error("rn_pt_render_reference: invalid argument");
 		return RN_ERR_INVALID_ARGUMENT;
@@ -214,6 +216,7 @@ rn_status rn_pt_render_reference(rn_scene *scene, const rn_pt_ref_params *prm, u
 
 rn_status rn_pt_render_raytraced(rn_scene *scene, const rn_pt_ref_params *prm, int shading, float fog_density,
                                  const float *fog_colour, unsigned flags, void *stream, uint32_t *argb) {
+	TraceRange trace_range("rn_pt_render_raytraced");
 	if (!scene || !prm || prm->width <= 0 || prm->height <= 0 || !argb) {
 		set_last_error("rn_pt_render_raytraced: invalid argument");
 		return RN_ERR_INVALID_ARGUMENT;
@@ -306,6 +309,7 @@ rn_status rn_pt_render_raytraced(rn_scene *scene, const rn_pt_ref_params *prm, i
 
 rn_status rn_pt_render_photon_mapped(rn_scene *scene, const rn_pt_ref_params *prm, int num_photons, int gather_rays,
                                      unsigned flags, void *stream, uint32_t *argb, unsigned *num_stored) {
+	TraceRange trace_range("rn_pt_render_photon_mapped");
 	if (!scene || !prm || prm->width <= 0 || prm->height <= 0 || !argb) {
 		set_last_error("rn_pt_render_photon_mapped: invalid argument");
 		return RN_ERR_INVALID_ARGUMENT;
@@ -399,6 +403,7 @@ rn_status gi_params(const char *fn, rn_scene *scene, const rn_pt_ref_params *prm
 rn_status rn_pt_render_bidirectional(rn_scene *scene, const rn_pt_ref_params *prm, int samples, float exposure, int rng,
                                      unsigned long long seed, unsigned flags, void *stream, uint32_t *argb,
                                      float *rgb) {
+	TraceRange trace_range("rn_pt_render_bidirectional");
 	GiParams p;
 	rn_status st = gi_params("rn_pt_render_bidirectional", scene, prm, exposure, p);
 	if (st != RN_OK)
@@ -443,6 +448,7 @@ rn_status rn_pt_render_bidirectional(rn_scene *scene, const rn_pt_ref_params *pr
 rn_status rn_pt_render_metropolis(rn_scene *scene, const rn_pt_ref_params *prm, long long mutations, float exposure,
                                   int chains, int bootstrap, unsigned long long seed, unsigned flags, void *stream,
                                   uint32_t *argb, float *rgb, double *mean_luminance) {
+	TraceRange trace_range("rn_pt_render_metropolis");
 	GiParams p;
 	rn_status st = gi_params("rn_pt_render_metropolis", scene, prm, exposure, p);
 	if (st != RN_OK)
@@ -497,6 +503,7 @@ rn_status rn_pt_render_metropolis(rn_scene *scene, const rn_pt_ref_params *prm, 
 
 int rn_render(const rn_scene *scene, rn_render_mode mode, int width, int height, float cam_z, int samples,
               unsigned char *rgba) {
+	TraceRange trace_range("rn_render");
 	if (!scene || !rgba || width <= 0 || height <= 0)
 		return 0;
 	if (mode != RN_PATHTRACED && mode != RN_RAYTRACED) {

@@ -32,6 +32,7 @@
 #include "gi.hpp"
 #include "refshade.cuh"
 #include "rng.cuh"
+#include "trace_range.hpp"
 
 namespace rnb {
 
@@ -632,8 +633,12 @@ cudaError_t launch_bdpt(const SceneView &sv, const float4 *ref_shade, const GiPa
 	k_mt_seed_rows<<<static_cast<unsigned>((rows + 127) / 128), 128, 0, st>>>(mt_s, mt_i, p.height);
 	for (int x0 = 0; x0 < p.width; x0 += cw) {
 		const int x1 = std::min(p.width, x0 + cw);
-		k_bdpt_rows<<<static_cast<unsigned>((rows + kRowsPerBlock - 1) / kRowsPerBlock), 32, 0, st>>>(
-		    sv, ref_shade, p, mt_s, mt_i, x0, x1, rec, cnt, status);
+		{
+			TraceRange r("subpaths in row-stream order");
+			k_bdpt_rows<<<static_cast<unsigned>((rows + kRowsPerBlock - 1) / kRowsPerBlock), 32, 0, st>>>(
+			    sv, ref_shade, p, mt_s, mt_i, x0, x1, rec, cnt, status);
+		}
+		TraceRange r("connections");
 		const long n = static_cast<long>(x1 - x0) * p.height;
 		k_bdpt_connect<<<static_cast<unsigned>((n + 127) / 128), 128, 0, st>>>(sv, ref_shade, p, x0, x1, rec, cnt,
 		                                                                       argb, rgb, status);
@@ -664,8 +669,12 @@ cudaError_t launch_mlt(const SceneView &sv, const float4 *ref_shade, const GiPar
 	cudaError_t e = cudaMemsetAsync(image, 0, static_cast<size_t>(npix) * 3 * 4, st);
 	if (e != cudaSuccess)
 		return e;
-	k_mlt_bootstrap<<<static_cast<unsigned>((b + 127) / 128), 128, 0, st>>>(sv, ref_shade, p, lum, len, status);
-	k_mlt_cdf<<<1, 1024, 0, st>>>(lum, p.bootstrap, cdf, total);
+	{
+		TraceRange r("bootstrap");
+		k_mlt_bootstrap<<<static_cast<unsigned>((b + 127) / 128), 128, 0, st>>>(sv, ref_shade, p, lum, len, status);
+		k_mlt_cdf<<<1, 1024, 0, st>>>(lum, p.bootstrap, cdf, total);
+	}
+	TraceRange r("chains");
 	k_mlt_chains<<<static_cast<unsigned>((p.chains + 127) / 128), 128, 0, st>>>(sv, ref_shade, p, cdf, total, len,
 	                                                                          image, status);
 	const long g = std::min<long>((npix + 255) / 256, 148 * 16);

@@ -5,6 +5,7 @@
 #include "adjoint.hpp"
 #include "render_impl.hpp"
 #include "scene_impl.hpp"
+#include "trace_range.hpp"
 
 using namespace rnb;
 
@@ -46,6 +47,7 @@ rn_status rn_pt_scene_set_materials(rn_scene *scene, const float *albedo, const 
 rn_status rn_pt_backward(rn_scene *scene, int n_views, const rn_pt_camera *cameras, const rn_pt_settings *settings,
                          const float *const *d_images, unsigned flags, void *stream, float *d_albedo,
                          float *d_emission) {
+	TraceRange trace_range("rn_pt_backward");
 	if (!scene || n_views <= 0 || !cameras || !settings || !d_images) {
 		set_last_error("rn_pt_backward: invalid argument");
 		return RN_ERR_INVALID_ARGUMENT;

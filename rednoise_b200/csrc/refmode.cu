@@ -20,6 +20,7 @@
 #include <cstdint>
 
 #include "refshade.cuh"
+#include "trace_range.hpp"
 
 namespace rnb {
 
@@ -791,11 +792,19 @@ cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade
 		e = cudaMemsetAsync(dv.bins, 0, sizeof(unsigned) << kShadeKeyBits, st);
 		if (e != cudaSuccess)
 			return e;
-		k_ref_paths<<<std::min(ceil_div(dv.npix, bs), 148 * 8), bs, 0, st>>>(sv, ref_shade, d_params, dv, status);
+		{
+			TraceRange r("paths");
+			k_ref_paths<<<std::min(ceil_div(dv.npix, bs), 148 * 8), bs, 0, st>>>(sv, ref_shade, d_params, dv,
+			                                                                   status);
+		}
 		k_shade_count<<<148 * 8, 256, 0, st>>>(dv);
 		k_shade_scan<<<1, 1024, 0, st>>>(dv);
 		k_shade_scatter<<<148 * 8, 256, 0, st>>>(dv);
-		k_ref_shadow<<<148 * 16, bs, 0, st>>>(sv, d_params, dv, status);
+		{
+			TraceRange r("shadow rays");
+			k_ref_shadow<<<148 * 16, bs, 0, st>>>(sv, d_params, dv, status);
+		}
+		TraceRange r("fold");
 		k_ref_fold<<<ceil_div(dv.npix, bs), bs, 0, st>>>(sv, ref_shade, d_params, dv, argb, mean_rgb, status);
 	}
 	return cudaGetLastError();

@@ -6,6 +6,7 @@
 #include "pt_kernels.hpp"
 #include "render_impl.hpp"
 #include "scene_impl.hpp"
+#include "trace_range.hpp"
 
 namespace rnb {
 
@@ -144,6 +145,7 @@ std::tuple<int, int, int, int> tune_key(const PhysCamera &pc, const PhysSettings
 // a whole frame's paths in one wave, within a memory budget.
 rn_status autotune_scene(rn_scene *s, const PhysScene &ps, const PhysCamera &pc, const PhysSettings &pst,
                          rn_pt_tuning &out) {
+	TraceRange trace_range("autotune");
 	PhysSettings probe = pst;
 	probe.spp = std::clamp(pst.spp, 1, 64);
 	probe.sample_offset = 0x40000000u;
@@ -277,6 +279,7 @@ extern "C" {
 
 rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
                                   unsigned flags, void *stream, float *accum) {
+	TraceRange trace_range("rn_pt_render_accumulate");
 	PhysScene ps;
 	PhysCamera pc;
 	PhysSettings pst;
@@ -304,6 +307,7 @@ rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, c
 
 rn_status rn_pt_autotune(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings, unsigned flags,
                          rn_pt_tuning *out) {
+	TraceRange trace_range("rn_pt_autotune");
 	PhysScene ps;
 	PhysCamera pc;
 	PhysSettings pst;
@@ -342,6 +346,7 @@ rn_status rn_pt_count_traversal(rn_scene *scene, const rn_pt_camera *camera, con
 
 rn_status rn_pt_render(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings, unsigned flags,
                        void *stream, float *rgb) {
+	TraceRange trace_range("rn_pt_render");
 	PhysScene ps;
 	PhysCamera pc;
 	PhysSettings pst;

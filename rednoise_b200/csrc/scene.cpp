@@ -8,6 +8,7 @@
 
 #include "lbvh.hpp"
 #include "scene_impl.hpp"
+#include "trace_range.hpp"
 
 namespace rnb {
 
@@ -62,6 +63,7 @@ rn_status build_host(rn_scene *s) {
 }
 
 rn_status prepare_scene(rn_scene *s) {
+	TraceRange trace_range("scene prepare: BVH build and upload");
 	std::lock_guard<std::mutex> lock(s->mu);
 	if (s->prepared)
 		return RN_OK;
@@ -249,6 +251,7 @@ rn_status check_status_word(int *d_err, cudaStream_t st, const char *what) {
 extern "C" {
 
 rn_scene *rn_scene_load_obj(const char *path, float scale) {
+	TraceRange trace_range("rn_scene_load_obj");
 	if (!path)
 		return nullptr;
 	try {
@@ -325,6 +328,7 @@ rn_status rn_pt_scene_create(const rn_pt_scene_desc *desc, rn_scene **out) {
 }
 
 rn_status rn_pt_scene_prepare(rn_scene *scene) {
+	TraceRange trace_range("rn_pt_scene_prepare");
 	if (!scene) {
 		set_last_error("rn_pt_scene_prepare: NULL scene");
 		return RN_ERR_INVALID_ARGUMENT;
@@ -418,6 +422,7 @@ rn_status rn_pt_scene_dump_bvh(rn_scene *scene, int *order, int *node_count, flo
 }
 
 rn_status rn_pt_scene_build_lbvh(rn_scene *scene, void *stream, double *build_ms) {
+	TraceRange trace_range("rn_pt_scene_build_lbvh");
 	if (!scene) {
 		set_last_error("rn_pt_scene_build_lbvh: NULL scene");
 		return RN_ERR_INVALID_ARGUMENT;
@@ -486,6 +491,7 @@ static rn_status query_view(rn_scene *scene, unsigned flags, const char *what, S
 
 rn_status rn_pt_trace_closest(rn_scene *scene, int n, const float *origins, const float *directions, const int *ignore,
                               unsigned flags, void *stream, int *tri, float *t, float *u, float *v) {
+	TraceRange trace_range("rn_pt_trace_closest");
 	if (!scene || n < 0 || (n > 0 && (!origins || !directions || !tri))) {
 		set_last_error("rn_pt_trace_closest: invalid argument");
 		return RN_ERR_INVALID_ARGUMENT;
@@ -531,6 +537,7 @@ rn_status rn_pt_trace_closest(rn_scene *scene, int n, const float *origins, cons
 
 rn_status rn_pt_trace_any(rn_scene *scene, int n, const float *origins, const float *directions, const float *tmax,
                           const int *ignore, unsigned flags, void *stream, int *occluded) {
+	TraceRange trace_range("rn_pt_trace_any");
 	if (!scene || n < 0 || (n > 0 && (!origins || !directions || !tmax || !occluded))) {
 		set_last_error("rn_pt_trace_any: invalid argument");
 		return RN_ERR_INVALID_ARGUMENT;
