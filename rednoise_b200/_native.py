@@ -10,7 +10,9 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "librednoise_b200.so")
+# RN_B200_LIBRARY selects another build of the library (for instance the
+# bounds-checked librednoise_b200_debug.so); the default is the in-tree release build.
+LIB_PATH = os.environ.get("RN_B200_LIBRARY") or os.path.join(_HERE, "librednoise_b200.so")
 
 RN_OK = 0
 RN_ERR_OUT_OF_MEMORY = 3

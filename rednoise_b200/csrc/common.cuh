@@ -29,6 +29,16 @@ rn_status cuda_fail(cudaError_t e, const char *what);
 			return ::rnb::cuda_fail(e__, #call);                                                                       \
 	} while (0)
 
+// Debug builds (-DRN_BOUNDS_CHECK, `make debug`) check data-dependent indices
+// (tree references, queue slots, sort positions, image pixels) against their
+// buffers; a failed check sets the call's status word and skips the access (no
+// trap), so the call returns an error. Release builds compile the checks away.
+#ifdef RN_BOUNDS_CHECK
+constexpr bool kBoundsCheck = true;
+#else
+constexpr bool kBoundsCheck = false;
+#endif
+
 // A device allocation that frees itself.
 struct DevBuf {
 	void *p = nullptr;

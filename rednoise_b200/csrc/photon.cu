@@ -51,7 +51,7 @@ struct PhotonInput {
 // once, at its end). Reads the engine outputs from draws[p...]; returns the number
 // of draws taken. With out != nullptr the deposits are written there.
 __device__ int trace_photon(const PhotonInput &in, uint32_t p0, float4 *out_pos, float4 *out_pow, float4 *out_dir,
-                            int &deposits, int &err) {
+                            int out_room, int &deposits, int &err) {
 	uint32_t p = p0;
 	auto U = [&]() { return canonical01(in.draws[p++]); };
 	const float z = 1.0f - 2.0f * U();
@@ -109,6 +109,10 @@ __device__ int trace_photon(const PhotonInput &in, uint32_t p0, float4 *out_pos,
 		}
 		// deposit on the diffuse surface, then maybe bounce (roulette by albedo)
 		if (out_pos) {
+			if (kBoundsCheck && deposits >= out_room) {
+				err = 1;
+				break;
+			}
 			out_pos[deposits] = make_float4(point.x, point.y, point.z, 0.0f);
 			out_pow[deposits] = make_float4(power.x, power.y, power.z, 0.0f);
 			out_dir[deposits] = make_float4(direction.x, direction.y, direction.z, 0.0f);
@@ -139,7 +143,7 @@ __global__ void __launch_bounds__(128) k_photon_counts(PhotonInput in, uint32_t 
 	if (p >= n_pos)
 		return;
 	int err = 0, d = 0;
-	const int c = trace_photon(in, p, nullptr, nullptr, nullptr, d, err);
+	const int c = trace_photon(in, p, nullptr, nullptr, nullptr, 0, d, err);
 	next[p] = p + static_cast<uint32_t>(c);
 	deposits[p] = static_cast<uint8_t>(d);
 	if (err)
@@ -173,13 +177,13 @@ __global__ void k_chain_starts(const uint32_t *__restrict__ jumps, uint32_t n_po
 __global__ void __launch_bounds__(128) k_photon_deposit(PhotonInput in, uint32_t n_photons,
                                                         const uint32_t *__restrict__ start,
                                                         const uint32_t *__restrict__ offset, float4 *pos,
-                                                        float4 *pw, float4 *dir, int *status) {
+                                                        float4 *pw, float4 *dir, uint32_t cap, int *status) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n_photons)
 		return;
 	int err = 0, d = 0;
 	const uint32_t o = offset[i];
-	trace_photon(in, start[i], pos + o, pw + o, dir + o, d, err);
+	trace_photon(in, start[i], pos + o, pw + o, dir + o, o < cap ? static_cast<int>(cap - o) : 0, d, err);
 	if (err)
 		atomicOr(status, 1);
 }
@@ -536,7 +540,7 @@ cudaError_t launch_photon_mapped(const SceneView &sv, const float4 *ref_shade, c
 		*deposits_out = n_total;
 	k_photon_deposit<<<ceil_div(static_cast<long>(n_photons), bs), bs, 0, st>>>(in, static_cast<uint32_t>(n_photons),
 	                                                                            d_start, d_off, d_pos, d_pw, d_dir,
-	                                                                            status);
+	                                                                            static_cast<uint32_t>(n_dep), status);
 	// the grid: a stable sort of the deposits by cell key
 	const float radius = 0.25f;
 	PhotonMapView m{};

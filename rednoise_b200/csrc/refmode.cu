@@ -146,6 +146,7 @@ struct DeferView {
 	int taps;
 	long pix0;
 	long npix;
+	long cap; // shading entries the chunk's buffers hold
 };
 
 __device__ __forceinline__ int shading_append(unsigned *count) {
@@ -263,6 +264,10 @@ __device__ void record_path(Ctx &c, V3 origin, V3 direction, Rng &rng, const Def
 		const V3 n = face_viewer(tnormal, direction);
 		const V3 albedo = base_colour(material, rgb, point) / 255.0f;
 		const int entry = shading_append(dv.list_count);
+		if (kBoundsCheck && entry >= dv.cap) {
+			c.err = 1;
+			return;
+		}
 		dv.list[entry] = static_cast<int>(rec_index + level);
 		dv.key[entry] = shade_key(c.sv, point);
 		if (depth <= 0) {
@@ -335,8 +340,12 @@ __global__ void __launch_bounds__(1024) k_shade_scan(DeferView dv) {
 __global__ void k_shade_scatter(DeferView dv) {
 	const long n = *dv.list_count;
 	for (long e = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
-	     e += static_cast<long>(gridDim.x) * blockDim.x)
-		dv.sorted[atomicAdd(dv.bins + dv.key[e], 1u)] = static_cast<int>(e);
+	     e += static_cast<long>(gridDim.x) * blockDim.x) {
+		const unsigned pos = atomicAdd(dv.bins + dv.key[e], 1u);
+		if (kBoundsCheck && pos >= n)
+			continue; // the slot left unwritten reads -1 in k_ref_shadow
+		dv.sorted[pos] = static_cast<int>(e);
+	}
 }
 
 __global__ void __launch_bounds__(128) k_ref_shadow(SceneView sv, const RefParams *__restrict__ params, DeferView dv,
@@ -349,6 +358,10 @@ __global__ void __launch_bounds__(128) k_ref_shadow(SceneView sv, const RefParam
 		const long slot = i / dv.taps;
 		int k = static_cast<int>(i - slot * dv.taps);
 		const long e = dv.sorted[slot];
+		if (kBoundsCheck && (e < 0 || e >= dv.cap)) {
+			c.err = 1;
+			continue;
+		}
 		int l = 0;
 		for (int n = vis_tap_count(p.lights[0]); k >= n; n = vis_tap_count(p.lights[l])) {
 			k -= n;
@@ -782,6 +795,7 @@ cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade
 	dv.occl = reinterpret_cast<uint8_t *>(base);
 	dv.levels = p.max_depth + 1;
 	dv.taps = taps;
+	dv.cap = chunk * static_cast<long>(records);
 	const int bs = 128;
 	for (long p0 = 0; p0 < n; p0 += chunk) {
 		dv.pix0 = p0;
@@ -796,6 +810,12 @@ cudaError_t launch_render_reference(const SceneView &sv, const float4 *ref_shade
 			TraceRange r("paths");
 			k_ref_paths<<<std::min(ceil_div(dv.npix, bs), 148 * 8), bs, 0, st>>>(sv, ref_shade, d_params, dv,
 			                                                                   status);
+		}
+		if (kBoundsCheck) {
+			// unwritten sort slots then read as -1, which k_ref_shadow reports
+			e = cudaMemsetAsync(dv.sorted, 0xFF, static_cast<size_t>(dv.cap) * sizeof(int), st);
+			if (e != cudaSuccess)
+				return e;
 		}
 		k_shade_count<<<148 * 8, 256, 0, st>>>(dv);
 		k_shade_scan<<<1, 1024, 0, st>>>(dv);

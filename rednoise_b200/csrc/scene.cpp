@@ -151,6 +151,8 @@ rn_status prepare_scene(rn_scene *s) {
 	}
 	v.root_ref = lay.root_ref;
 	v.n_tris = n;
+	v.n_nodes = lay.internal_count;
+	v.n_nodes4 = static_cast<int>(lay4.nodes.size() / 8);
 	s->view = v;
 	s->prepared = true;
 	return RN_OK;
@@ -463,6 +465,8 @@ rn_status rn_pt_scene_build_lbvh(rn_scene *scene, void *stream, double *build_ms
 	v.root_ref = res.root_ref;
 	v.root4_ref = 0;
 	v.n_tris = n;
+	v.n_nodes = n > 1 ? n - 1 : 0;
+	v.n_nodes4 = 0;
 	scene->lbvh_view = v;
 	scene->lbvh_depth = res.depth;
 	scene->lbvh_ready = true;

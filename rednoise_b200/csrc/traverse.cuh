@@ -23,6 +23,8 @@
 // reachable leaves depends only on the slab tests against the fixed maxDistance.
 #pragma once
 
+#include "common.cuh"
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -39,6 +41,8 @@ struct SceneView {
 	int root_ref;
 	int root4_ref;
 	int n_tris;
+	int n_nodes;  // internal nodes of the 2-wide layout
+	int n_nodes4; // nodes of the 4-wide layout (0 when absent)
 };
 
 struct RayPre {
@@ -146,6 +150,14 @@ __device__ __forceinline__ bool tri_test(const float4 a, const float4 b, const f
 __device__ __forceinline__ int leaf_start(int ref) { return (~ref) >> 3; }
 __device__ __forceinline__ int leaf_count(int ref) { return (~ref) & 7; }
 
+// Debug-build checks of tree references (compiled away unless RN_BOUNDS_CHECK).
+__device__ __forceinline__ bool bad_node(const SceneView &s, int ref, bool four) {
+	return kBoundsCheck && ref >= (four ? s.n_nodes4 : s.n_nodes);
+}
+__device__ __forceinline__ bool bad_leaf(const SceneView &s, int start, int count) {
+	return kBoundsCheck && (start < 0 || count < 0 || start + count > s.n_tris);
+}
+
 // Closest hit. `ignore` is an original triangle index to skip (-1 = none).
 // `err` is set to 1 if the stack bound would be exceeded (the host rejects
 // trees deeper than the bound, so this only reports corrupted input).
@@ -179,6 +191,10 @@ __device__ __forceinline__ HitRec trace_closest(const SceneView &s, const RayPre
 		}
 		// Descend through internal nodes until a leaf is reached.
 		while (ref >= 0) {
+			if (bad_node(s, ref, false)) {
+				err = 1;
+				return h;
+			}
 			const float4 *nd = s.nodes + 4 * static_cast<size_t>(ref);
 			const float4 n0 = __ldg(nd + 0);
 			const float4 n1 = __ldg(nd + 1);
@@ -241,6 +257,10 @@ __device__ __forceinline__ HitRec trace_closest(const SceneView &s, const RayPre
 		// Leaf: test its triangles in ascending order.
 		const int start = leaf_start(ref);
 		const int count = leaf_count(ref);
+		if (bad_leaf(s, start, count)) {
+			err = 1;
+			return h;
+		}
 		for (int p = start; p < start + count; p++) {
 			const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
 			const float4 a = __ldg(tp + 0);
@@ -288,6 +308,10 @@ __device__ __forceinline__ bool trace_any(const SceneView &s, const RayPre &r, f
 	while (sp > 0) {
 		int ref = st[--sp];
 		while (ref >= 0) {
+			if (bad_node(s, ref, false)) {
+				err = 1;
+				return false;
+			}
 			const float4 *nd = s.nodes + 4 * static_cast<size_t>(ref);
 			const float4 n0 = __ldg(nd + 0);
 			const float4 n1 = __ldg(nd + 1);
@@ -319,6 +343,10 @@ __device__ __forceinline__ bool trace_any(const SceneView &s, const RayPre &r, f
 			continue;
 		const int start = leaf_start(ref);
 		const int count = leaf_count(ref);
+		if (bad_leaf(s, start, count)) {
+			err = 1;
+			return false;
+		}
 		for (int p = start; p < start + count; p++) {
 			const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
 			const float4 a = __ldg(tp + 0);
@@ -462,6 +490,10 @@ __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPr
 		if (!(__int_as_float(static_cast<int>(e >> 32)) < h.t))
 			continue;
 		while (ref >= 0) {
+			if (bad_node(s, ref, true)) {
+				err = 1;
+				return h;
+			}
 			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ref);
 			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
 			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
@@ -494,6 +526,10 @@ __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPr
 			continue;
 		const int start = leaf_start(ref);
 		const int count = leaf_count(ref);
+		if (bad_leaf(s, start, count)) {
+			err = 1;
+			return h;
+		}
 		for (int p = start; p < start + count; p++) {
 			const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
 			const float4 a = __ldg(tp + 0);
@@ -569,6 +605,10 @@ __device__ __forceinline__ HitRec trace_closest4_flat(const SceneView &s, const 
 		if (!(__int_as_float(static_cast<int>(e >> 32)) < h.t))
 			continue;
 		while (ref >= 0) {
+			if (bad_node(s, ref, true)) {
+				err = 1;
+				return h;
+			}
 			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ref);
 			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
 			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
@@ -601,6 +641,10 @@ __device__ __forceinline__ HitRec trace_closest4_flat(const SceneView &s, const 
 			continue;
 		const int start = leaf_start(ref);
 		const int count = leaf_count(ref);
+		if (bad_leaf(s, start, count)) {
+			err = 1;
+			return h;
+		}
 		if (count == 0)
 			continue;
 		float4 ta[4], tb[4], tc[4];
@@ -667,6 +711,10 @@ __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, 
 	while (sp > 0) {
 		int ref = st.get(--sp);
 		while (ref >= 0) {
+			if (bad_node(s, ref, true)) {
+				err = 1;
+				return false;
+			}
 			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ref);
 			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
 			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
@@ -701,6 +749,10 @@ __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, 
 			continue;
 		const int start = leaf_start(ref);
 		const int count = leaf_count(ref);
+		if (bad_leaf(s, start, count)) {
+			err = 1;
+			return false;
+		}
 		for (int p = start; p < start + count; p++) {
 			const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
 			const float4 a = __ldg(tp + 0);
@@ -774,6 +826,10 @@ __device__ __forceinline__ bool trav_step(TravState &ts, const SceneView &s, int
 		ts.cur = static_cast<int>(static_cast<unsigned>(e));
 	}
 	while (ts.cur >= 0) {
+		if (bad_node(s, ts.cur, true)) {
+			err = 1;
+			return false;
+		}
 		const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(ts.cur);
 		const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
 		const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
@@ -805,6 +861,10 @@ __device__ __forceinline__ bool trav_step(TravState &ts, const SceneView &s, int
 	// Leaf.
 	const int start = leaf_start(ts.cur);
 	const int count = leaf_count(ts.cur);
+	if (bad_leaf(s, start, count)) {
+		err = 1;
+		return false;
+	}
 	ts.cur = kPopRef;
 	for (int p = start; p < start + count; p++) {
 		const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
@@ -897,6 +957,10 @@ __device__ bool count_reference_query(const SceneView &s, const RayPre &r, int i
 		if (ref < 0) {
 			const int start = leaf_start(ref);
 			const int count = leaf_count(ref);
+			if (bad_leaf(s, start, count)) {
+				err = 1;
+				return false;
+			}
 			for (int p = start; p < start + count; p++) {
 				const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
 				const float4 a = __ldg(tp + 0);
@@ -921,6 +985,10 @@ __device__ bool count_reference_query(const SceneView &s, const RayPre &r, int i
 			continue;
 		}
 		if (sp + 2 > kStack) {
+			err = 1;
+			return false;
+		}
+		if (bad_node(s, ref, false)) {
 			err = 1;
 			return false;
 		}

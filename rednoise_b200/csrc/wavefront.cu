@@ -143,7 +143,7 @@ __device__ __forceinline__ unsigned ray_bin(const SceneView &sv, const F3 &o, co
 }
 
 __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
-                                                  const int *__restrict__ q, int write_keys) {
+                                                  const int *__restrict__ q, int write_keys, int *status) {
 	const unsigned n = pool.counters[kCntRays + k];
 	int *__restrict__ qn = pool.queue[(k + 1) & 1];
 	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -169,6 +169,10 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 		ShadowReq sr;
 		const bool alive = shade_vertex(job.sc, job.st, ps, h, sr);
 		const unsigned si = warp_append(pool.counters + kCntShadow + k, sr.valid);
+		if (kBoundsCheck && sr.valid && si >= static_cast<unsigned>(pool.capacity)) {
+			atomicOr(status, 1);
+			sr.valid = false;
+		}
 		if (sr.valid) {
 			pool.sh_o[si] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
 			pool.sh_d[si] = make_float4(sr.d.x, sr.d.y, sr.d.z, __int_as_float(sr.ignore));
@@ -176,6 +180,10 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 		}
 		const unsigned ni = warp_append(pool.counters + kCntRays + k + 1, alive);
 		pool.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, L.w);
+		if (kBoundsCheck && alive && ni >= static_cast<unsigned>(pool.capacity)) {
+			atomicOr(status, 1);
+			continue;
+		}
 		if (alive) {
 			qn[ni] = slot;
 			if (write_keys)
@@ -375,7 +383,7 @@ __global__ void __launch_bounds__(kScanThreads) k_wf_bin_scan(WfPool pool) {
 
 // Each block takes a contiguous chunk of the queue, reserves its share of every
 // bin with one atomic per non-empty bin, then places its rays.
-__global__ void __launch_bounds__(1024) k_wf_bin_scatter(WfPool pool, int k) {
+__global__ void __launch_bounds__(1024) k_wf_bin_scatter(WfPool pool, int k, int *status) {
 	extern __shared__ unsigned h[];
 	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
 		h[b] = 0;
@@ -395,6 +403,10 @@ __global__ void __launch_bounds__(1024) k_wf_bin_scatter(WfPool pool, int k) {
 	const int *__restrict__ q = pool.queue[k & 1];
 	for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
 		const unsigned pos = atomicAdd(&h[pool.keys[i] & (kBins - 1)], 1u);
+		if (kBoundsCheck && pos >= n) {
+			atomicOr(status, 1);
+			continue;
+		}
 		pool.sorted[pos] = q[i];
 	}
 }
@@ -441,7 +453,7 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 				return e;
 			k_wf_bin_count<<<lc.grid_bin, 1024, kBins * sizeof(unsigned), st>>>(pool, k);
 			k_wf_bin_scan<<<1, kScanThreads, 0, st>>>(pool);
-			k_wf_bin_scatter<<<lc.grid_bin, 1024, kBins * sizeof(unsigned), st>>>(pool, k);
+			k_wf_bin_scatter<<<lc.grid_bin, 1024, kBins * sizeof(unsigned), st>>>(pool, k, status);
 			q = pool.sorted;
 		}
 		const int oj = wave.only_job;
@@ -451,7 +463,7 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			k_wf_extend<kOrderNearest><<<lc.grid_ext, 128, kWfExtendSmem, st>>>(d_jobs, pool, k, q, oj, status);
 		else
 			k_wf_extend<kOrderReference><<<lc.grid_ext, 128, kWfExtendSmem, st>>>(d_jobs, pool, k, q, oj, status);
-		k_wf_shade<<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, q, sort ? 1 : 0);
+		k_wf_shade<<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, q, sort ? 1 : 0, status);
 		if (use_dyn)
 			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, oj, status);
 		else
