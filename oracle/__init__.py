@@ -98,6 +98,8 @@ def orc() -> ctypes.CDLL:
             "orc_pt_count": (None, [vp, vp, ci, ci, ci, ci, ci, ctypes.c_ulonglong, ctypes.c_uint, vp, ci, vp, vp]),
             "orc_pt_backward": (None, [vp, vp, ci, ci, ci, ci, ci, ctypes.c_ulonglong, ctypes.c_uint, vp, vp, ci,
                                        vp, vp]),
+            "orc_bsdf_eval": (None, [ci, vp, ctypes.c_double, vp, vp, ci, vp, vp, vp, vp]),
+            "orc_bsdf_sample": (None, [ci, vp, ctypes.c_double, vp, vp, ci, vp, vp, vp, vp, vp]),
             "orc_bdpt_render": (None, [vp, vp, vp, ci, ci, ci, ci, cf, vp, vp, ci, cf, ci, ctypes.c_ulonglong, ci,
                                        vp, vp]),
             "orc_mlt_render": (None, [vp, vp, vp, ci, ci, cf, vp, vp, ctypes.c_longlong, ci, ci, ctypes.c_ulonglong,
@@ -291,6 +293,32 @@ class RefModel:
             self.close()
         except Exception:
             pass
+
+
+def bsdf_eval(mat, albedo, param, ng, wo, wi):
+    """The physical estimator's BSDF in double precision for directions wi ((k, 3)):
+    (f cos (k, 3), pdf (k,), ok (k,))."""
+    a, n, o = (np.ascontiguousarray(x, np.float64) for x in (albedo, ng, wo))
+    wi = np.ascontiguousarray(wi, np.float64).reshape(-1, 3)
+    k = wi.shape[0]
+    fc = np.zeros((k, 3))
+    pdf = np.zeros(k)
+    ok = np.zeros(k, np.int32)
+    orc().orc_bsdf_eval(int(mat), P(a), float(param), P(n), P(o), k, P(wi), P(fc), P(pdf), P(ok))
+    return fc, pdf, ok.astype(bool)
+
+
+def bsdf_sample(mat, albedo, param, ng, wo, u):
+    """Continuation samples from uniforms u ((count, 3)): (wi, weight, pdf, ok)."""
+    a, n, o = (np.ascontiguousarray(x, np.float64) for x in (albedo, ng, wo))
+    u = np.ascontiguousarray(u, np.float64).reshape(-1, 3)
+    k = u.shape[0]
+    wi = np.zeros((k, 3))
+    w = np.zeros((k, 3))
+    pdf = np.zeros(k)
+    ok = np.zeros(k, np.int32)
+    orc().orc_bsdf_sample(int(mat), P(a), float(param), P(n), P(o), k, P(u), P(wi), P(w), P(pdf), P(ok))
+    return wi, w, pdf, ok.astype(bool)
 
 
 class OrcBvh:

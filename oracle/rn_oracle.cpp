@@ -736,10 +736,81 @@ template <typename T> X3<T> sdiv(X3<T> a, X3<T> b) {
 	return x3<T>(b.x > 0 ? a.x / b.x : T(0), b.y > 0 ? a.y / b.y : T(0), b.z > 0 ? a.z / b.z : T(0));
 }
 
+// Continuation sampling of the physical estimator: Lambert (cosine), GGX (visible
+// normals, Heitz 2018) or smooth dielectric (Fresnel choice). wi, weight = f cos /
+// pdf, pdf (0 for the delta dielectric) and d log(weight) / d albedo; false when the
+// sample is absorbed (below the surface).
+template <typename T>
+bool sample_t(int mat, X3<T> alb, T param, X3<T> n, X3<T> wo, X3<T> d, T cog, T u1, T u2, T uf, X3<T> &wi,
+              X3<T> &weight, T &pdf, X3<T> &cont_dlog) {
+	const T two_pi = T(6.28318530717958647692);
+	cont_dlog = x3<T>(0, 0, 0);
+	pdf = 0;
+	if (mat == 0) {
+		T r = std::sqrt(u1);
+		T ph = two_pi * u2;
+		X3<T> t, bt;
+		onb_t(n, t, bt);
+		T z = std::sqrt(std::max(T(0), 1 - u1));
+		wi = t * (r * std::cos(ph)) + bt * (r * std::sin(ph)) + n * z;
+		T ci = dt(wi, n);
+		if (ci <= 0)
+			return false;
+		weight = alb;
+		pdf = ci * T(0.318309886183790671537767526745);
+		cont_dlog = dlog_t(0, alb, T(0));
+	} else if (mat == 1) {
+		T alpha = param, a2 = alpha * alpha;
+		X3<T> t, bt;
+		onb_t(n, t, bt);
+		X3<T> wl = x3(dt(wo, t), dt(wo, bt), dt(wo, n));
+		X3<T> vh = nz(x3(alpha * wl.x, alpha * wl.y, wl.z));
+		T lensq = vh.x * vh.x + vh.y * vh.y;
+		X3<T> T1 = lensq > 0 ? x3<T>(-vh.y, vh.x, 0) * (T(1) / std::sqrt(lensq)) : x3<T>(1, 0, 0);
+		X3<T> T2 = cr(vh, T1);
+		T r = std::sqrt(u1);
+		T ph = two_pi * u2;
+		T t1 = r * std::cos(ph), t2 = r * std::sin(ph);
+		T sb = T(0.5) * (1 + vh.z);
+		t2 = (1 - sb) * std::sqrt(std::max(T(0), 1 - t1 * t1)) + sb * t2;
+		X3<T> nh = T1 * t1 + T2 * t2 + vh * std::sqrt(std::max(T(0), 1 - t1 * t1 - t2 * t2));
+		X3<T> ml = nz(x3(alpha * nh.x, alpha * nh.y, std::max(T(0), nh.z)));
+		X3<T> m = t * ml.x + bt * ml.y + n * ml.z;
+		T om = dt(wo, m);
+		wi = m * (2 * om) - wo;
+		T ci = dt(wi, n), co = wl.z;
+		if (ci <= 0 || om <= 0 || co <= 0)
+			return false;
+		T lo_ = ggx_L_t(co, a2), li_ = ggx_L_t(ci, a2);
+		T G1 = 1 / (1 + lo_), G2 = 1 / (1 + lo_ + li_);
+		weight = schlick_t(alb, om) * (G2 / G1);
+		pdf = G1 * ggx_D_t(ml.z, a2) / (4 * co);
+		cont_dlog = dlog_t(1, alb, m5_t(om));
+	} else {
+		T eta = param;
+		bool entering = cog > 0;
+		T ei = entering ? T(1) : eta, et = entering ? eta : T(1);
+		T ci = std::fabs(cog), rel = ei / et;
+		T s2t = rel * rel * std::max(T(0), 1 - ci * ci);
+		T F = 1, ct = 0;
+		if (s2t < 1) {
+			ct = std::sqrt(1 - s2t);
+			T rs = (ei * ci - et * ct) / (ei * ci + et * ct), rp = (et * ci - ei * ct) / (et * ci + ei * ct);
+			F = T(0.5) * (rs * rs + rp * rp);
+		}
+		if (uf < F)
+			wi = n * (2 * ci) - wo;
+		else
+			wi = d * rel + n * (rel * ci - ct);
+		weight = x3<T>(1, 1, 1);
+		pdf = 0;
+	}
+	return true;
+}
+
 template <typename T>
 X3<T> trace_phys(const PhysScene &s, const PhysCam &c, const PhysSet &st, uint32_t pix, uint32_t sample,
                  GradSink<T> *gs = nullptr) {
-	const T two_pi = T(6.28318530717958647692);
 	orc::U4 r0 = prand(st.seed, pix, sample, 0);
 	int px = static_cast<int>(pix % static_cast<uint32_t>(c.w)), py = static_cast<int>(pix / static_cast<uint32_t>(c.w));
 	T sx = ((T(px) + T(orc::u01(r0.x))) / T(c.w)) * 2 - 1;
@@ -825,67 +896,11 @@ X3<T> trace_phys(const PhysScene &s, const PhysCam &c, const PhysSet &st, uint32
 		}
 		if (bounce + 1 >= st.max_depth)
 			break;
-		X3<T> wi, weight, cont_dlog = x3<T>(0, 0, 0);
+		X3<T> wi, weight, cont_dlog;
 		T pdf = 0;
-		if (mat == 0) {
-			T r = std::sqrt(T(orc::u01(rB.x)));
-			T ph = two_pi * T(orc::u01(rB.y));
-			X3<T> t, bt;
-			onb_t(n, t, bt);
-			T z = std::sqrt(std::max(T(0), 1 - T(orc::u01(rB.x))));
-			wi = t * (r * std::cos(ph)) + bt * (r * std::sin(ph)) + n * z;
-			T ci = dt(wi, n);
-			if (ci <= 0)
-				break;
-			weight = alb;
-			pdf = ci * T(0.318309886183790671537767526745);
-			cont_dlog = dlog_t(0, alb, T(0));
-		} else if (mat == 1) {
-			T alpha = param, a2 = alpha * alpha;
-			X3<T> t, bt;
-			onb_t(n, t, bt);
-			X3<T> wl = x3(dt(wo, t), dt(wo, bt), dt(wo, n));
-			X3<T> vh = nz(x3(alpha * wl.x, alpha * wl.y, wl.z));
-			T lensq = vh.x * vh.x + vh.y * vh.y;
-			X3<T> T1 = lensq > 0 ? x3<T>(-vh.y, vh.x, 0) * (T(1) / std::sqrt(lensq)) : x3<T>(1, 0, 0);
-			X3<T> T2 = cr(vh, T1);
-			T r = std::sqrt(T(orc::u01(rB.x)));
-			T ph = two_pi * T(orc::u01(rB.y));
-			T t1 = r * std::cos(ph), t2 = r * std::sin(ph);
-			T sb = T(0.5) * (1 + vh.z);
-			t2 = (1 - sb) * std::sqrt(std::max(T(0), 1 - t1 * t1)) + sb * t2;
-			X3<T> nh = T1 * t1 + T2 * t2 + vh * std::sqrt(std::max(T(0), 1 - t1 * t1 - t2 * t2));
-			X3<T> ml = nz(x3(alpha * nh.x, alpha * nh.y, std::max(T(0), nh.z)));
-			X3<T> m = t * ml.x + bt * ml.y + n * ml.z;
-			T om = dt(wo, m);
-			wi = m * (2 * om) - wo;
-			T ci = dt(wi, n), co = wl.z;
-			if (ci <= 0 || om <= 0 || co <= 0)
-				break;
-			T lo_ = ggx_L_t(co, a2), li_ = ggx_L_t(ci, a2);
-			T G1 = 1 / (1 + lo_), G2 = 1 / (1 + lo_ + li_);
-			weight = schlick_t(alb, om) * (G2 / G1);
-			pdf = G1 * ggx_D_t(ml.z, a2) / (4 * co);
-			cont_dlog = dlog_t(1, alb, m5_t(om));
-		} else {
-			T eta = param;
-			bool entering = cog > 0;
-			T ei = entering ? T(1) : eta, et = entering ? eta : T(1);
-			T ci = std::fabs(cog), rel = ei / et;
-			T s2t = rel * rel * std::max(T(0), 1 - ci * ci);
-			T F = 1, ct = 0;
-			if (s2t < 1) {
-				ct = std::sqrt(1 - s2t);
-				T rs = (ei * ci - et * ct) / (ei * ci + et * ct), rp = (et * ci - ei * ct) / (et * ci + ei * ct);
-				F = T(0.5) * (rs * rs + rp * rp);
-			}
-			if (T(orc::u01(rA.w)) < F)
-				wi = n * (2 * ci) - wo;
-			else
-				wi = d * rel + n * (rel * ci - ct);
-			weight = x3<T>(1, 1, 1);
-			pdf = 0;
-		}
+		if (!sample_t<T>(mat, alb, param, n, wo, d, cog, T(orc::u01(rB.x)), T(orc::u01(rB.y)), T(orc::u01(rA.w)), wi,
+		                 weight, pdf, cont_dlog))
+			break;
 		beta = beta * weight;
 		if (bounce + 1 >= st.rr_depth) {
 			T q = std::min(T(0.95), mx(beta));
@@ -1697,6 +1712,54 @@ void orc_mlt_render(const void *bvh, const float *normal3, const int *rgb, int w
 			V3 v = mk(image[3 * i], image[3 * i + 1], image[3 * i + 2]) * scale * exposure;
 			argb[i] = gi_pack(v);
 		}
+	}
+}
+
+} // extern "C"
+
+extern "C" {
+
+// The physical estimator's BSDFs in double precision, for analytic checks
+// (tests/test_oracle.py): material 0 Lambert, 1 GGX (param = alpha, albedo = F0),
+// 2 smooth dielectric (param = IOR). ng: the geometric normal; wo: towards the
+// viewer. eval: f cos and the sampling pdf of each wi (ok = 0 below either side).
+void orc_bsdf_eval(int mat, const double *alb3, double param, const double *ng3, const double *wo3, int count,
+                   const double *wi3, double *fc3, double *pdf, int *ok) {
+	X3<double> alb = x3(alb3[0], alb3[1], alb3[2]), ng = x3(ng3[0], ng3[1], ng3[2]);
+	X3<double> wo = x3(wo3[0], wo3[1], wo3[2]);
+	X3<double> n = dt(ng, wo) >= 0 ? ng : -ng;
+	for (int i = 0; i < count; i++) {
+		X3<double> wi = x3(wi3[3 * i], wi3[3 * i + 1], wi3[3 * i + 2]), fc = x3(0.0, 0.0, 0.0);
+		double p = 0;
+		ok[i] = eval_t<double>(mat, alb, param, n, wo, wi, fc, p) ? 1 : 0;
+		fc3[3 * i] = fc.x;
+		fc3[3 * i + 1] = fc.y;
+		fc3[3 * i + 2] = fc.z;
+		pdf[i] = p;
+	}
+}
+
+// count samples from uniforms u (3 per sample: the two direction uniforms and the
+// Fresnel choice): wi, weight = f cos / pdf, pdf, ok (0: absorbed).
+void orc_bsdf_sample(int mat, const double *alb3, double param, const double *ng3, const double *wo3, int count,
+                     const double *u3, double *wi3, double *weight3, double *pdf, int *ok) {
+	X3<double> alb = x3(alb3[0], alb3[1], alb3[2]), ng = x3(ng3[0], ng3[1], ng3[2]);
+	X3<double> wo = x3(wo3[0], wo3[1], wo3[2]);
+	const double cog = dt(ng, wo);
+	X3<double> n = cog >= 0 ? ng : -ng;
+	for (int i = 0; i < count; i++) {
+		X3<double> wi = x3(0.0, 0.0, 0.0), w = x3(0.0, 0.0, 0.0), dl;
+		double p = 0;
+		const bool good = sample_t<double>(mat, alb, param, n, wo, -wo, cog, u3[3 * i], u3[3 * i + 1],
+		                                   u3[3 * i + 2], wi, w, p, dl);
+		ok[i] = good ? 1 : 0;
+		wi3[3 * i] = wi.x;
+		wi3[3 * i + 1] = wi.y;
+		wi3[3 * i + 2] = wi.z;
+		weight3[3 * i] = w.x;
+		weight3[3 * i + 1] = w.y;
+		weight3[3 * i + 2] = w.z;
+		pdf[i] = p;
 	}
 }
 
