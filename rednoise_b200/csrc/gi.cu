@@ -14,7 +14,8 @@
 // device memory between chunks.
 //
 // Bidirectional, counter stream: the same estimator with each (pixel, sample)
-// drawing from Philox-4x32-10 under the seed, one thread per pixel.
+// drawing from Philox-4x32-10 under the seed; the subpaths are traced one thread
+// per sample, then the same per-pixel connection pass sums them in order.
 //
 // Metropolis: many chains run in parallel, one thread each. A bootstrap of
 // independent paths estimates the normalisation b as the reference does; chain
@@ -242,6 +243,24 @@ __global__ void k_mt_seed_rows(uint32_t *s, int *idx, int rows) {
 	idx[y] = 624;
 }
 
+// Traces one sample's subpaths and records them: camera vertices in slots 0-3,
+// the emitter point in slot 4, light vertices in slots 5-8 (16 B each: position
+// and 2 * triangle + normal flip), and the two lengths in cnt.
+template <bool kAlone, class D>
+__device__ __forceinline__ void record_sample(Ctx &c, const GiParams &p, const GiCam &cam, int x, int y, D &draw,
+                                              float4 *__restrict__ rec, uint8_t *__restrict__ cnt, size_t sample) {
+	GV cv[kGiMaxDepth], lv[kGiMaxDepth + 1];
+	int cc[kGiMaxDepth], lc[kGiMaxDepth], nc, nl;
+	bdpt_subpaths<kAlone>(c, p, cam, x, y, draw, cv, cc, nc, lv, lc, nl);
+	float4 *r = rec + sample * kBdptRecordSlots;
+	for (int i = 0; i < nc; i++)
+		r[i] = make_float4(cv[i].p.x, cv[i].p.y, cv[i].p.z, __int_as_float(cc[i]));
+	r[kGiMaxDepth] = make_float4(lv[0].p.x, lv[0].p.y, lv[0].p.z, 0.0f);
+	for (int j = 1; j < nl; j++)
+		r[kGiMaxDepth + j] = make_float4(lv[j].p.x, lv[j].p.y, lv[j].p.z, __int_as_float(lc[j - 1]));
+	cnt[sample] = static_cast<uint8_t>(nc | ((nl - 1) << 4));
+}
+
 // Stream-order pass over columns [x0, x1): one thread per row.
 __global__ void __launch_bounds__(32) k_bdpt_rows(SceneView sv, const float4 *__restrict__ ref_shade, GiParams p,
                                                   uint32_t *mt_s, int *mt_i, int x0, int x1,
@@ -258,19 +277,32 @@ __global__ void __launch_bounds__(32) k_bdpt_rows(SceneView sv, const float4 *__
 	for (int x = x0; x < x1; x++) {
 		for (int s = 0; s < p.samples; s++) {
 			const size_t sample = (static_cast<size_t>(y) * cw + (x - x0)) * p.samples + s;
-			GV cv[kGiMaxDepth], lv[kGiMaxDepth + 1];
-			int cc[kGiMaxDepth], lc[kGiMaxDepth], nc, nl;
-			bdpt_subpaths<true>(c, p, cam, x, y, rng, cv, cc, nc, lv, lc, nl);
-			float4 *r = rec + sample * kBdptRecordSlots;
-			for (int i = 0; i < nc; i++)
-				r[i] = make_float4(cv[i].p.x, cv[i].p.y, cv[i].p.z, __int_as_float(cc[i]));
-			r[kGiMaxDepth] = make_float4(lv[0].p.x, lv[0].p.y, lv[0].p.z, 0.0f);
-			for (int j = 1; j < nl; j++)
-				r[kGiMaxDepth + j] = make_float4(lv[j].p.x, lv[j].p.y, lv[j].p.z, __int_as_float(lc[j - 1]));
-			cnt[sample] = static_cast<uint8_t>(nc | ((nl - 1) << 4));
+			record_sample<true>(c, p, cam, x, y, rng, rec, cnt, sample);
 		}
 	}
 	mt_i[y] = rng.i;
+	if (c.err)
+		atomicOr(status, 1);
+}
+
+// Counter streams: every sample is independent, so the subpaths of columns
+// [x0, x1) are traced one thread per (pixel, sample) and recorded for k_bdpt_connect.
+__global__ void __launch_bounds__(128) k_bdpt_counter_paths(SceneView sv, const float4 *__restrict__ ref_shade,
+                                                            GiParams p, int x0, int x1, float4 *__restrict__ rec,
+                                                            uint8_t *__restrict__ cnt, int *status) {
+	const int cw = x1 - x0;
+	const long total = static_cast<long>(cw) * p.height * p.samples;
+	const long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (i >= total)
+		return;
+	const long pix_local = i / p.samples;
+	const int s = static_cast<int>(i - pix_local * p.samples);
+	const int y = static_cast<int>(pix_local / cw), x = x0 + static_cast<int>(pix_local % cw);
+	const long pix = static_cast<long>(y) * p.width + x;
+	Ctx c{sv, ref_shade, nullptr, 0};
+	CtrDraw d{static_cast<uint32_t>(pix), static_cast<uint32_t>(s), 0u, static_cast<uint32_t>(p.seed),
+	          static_cast<uint32_t>(p.seed >> 32), 0, U4{0u, 0u, 0u, 0u}};
+	record_sample<false>(c, p, gi_cam(p), x, y, d, rec, cnt, static_cast<size_t>(i));
 	if (c.err)
 		atomicOr(status, 1);
 }
@@ -320,30 +352,6 @@ __global__ void __launch_bounds__(128) k_bdpt_connect(SceneView sv, const float4
 	}
 	const V3 col = acc * (p.exposure / static_cast<float>(p.samples));
 	gi_store(p, static_cast<long>(y) * p.width + x, col, argb, rgb);
-	if (c.err)
-		atomicOr(status, 1);
-}
-
-// Counter-stream bidirectional estimator: one thread per pixel.
-__global__ void __launch_bounds__(128) k_bdpt_counter(SceneView sv, const float4 *__restrict__ ref_shade, GiParams p,
-                                                      uint32_t *argb, float *rgb, int *status) {
-	const long pix = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-	if (pix >= static_cast<long>(p.width) * p.height)
-		return;
-	const int x = static_cast<int>(pix % p.width), y = static_cast<int>(pix / p.width);
-	Ctx c{sv, ref_shade, nullptr, 0};
-	const GiCam cam = gi_cam(p);
-	V3 acc = mk(0.0f, 0.0f, 0.0f);
-	for (int s = 0; s < p.samples; s++) {
-		CtrDraw d{static_cast<uint32_t>(pix), static_cast<uint32_t>(s), 0u, static_cast<uint32_t>(p.seed),
-		          static_cast<uint32_t>(p.seed >> 32), 0, U4{0u, 0u, 0u, 0u}};
-		GV cv[kGiMaxDepth], lv[kGiMaxDepth + 1];
-		int nc, nl;
-		bdpt_subpaths<false>(c, p, cam, x, y, d, cv, static_cast<int *>(nullptr), nc, lv, static_cast<int *>(nullptr),
-		                     nl);
-		bdpt_connect(c, cv, nc, lv, nl, acc);
-	}
-	gi_store(p, pix, acc * (p.exposure / static_cast<float>(p.samples)), argb, rgb);
 	if (c.err)
 		atomicOr(status, 1);
 }
@@ -604,8 +612,7 @@ int bdpt_chunk_width(const GiParams &p, size_t budget) {
 } // namespace
 
 size_t bdpt_scratch_bytes(const GiParams &p, bool reference_stream, size_t chunk_budget) {
-	if (!reference_stream)
-		return 0;
+	(void)reference_stream; // both streams record subpaths; the row streams' state is small
 	const size_t rows = static_cast<size_t>(p.height);
 	const size_t samples = static_cast<size_t>(bdpt_chunk_width(p, chunk_budget)) * rows * p.samples;
 	return align256(624 * 4 * rows) + align256(4 * rows) + align256(samples * kBdptRecordSlots * 16) +
@@ -614,11 +621,6 @@ size_t bdpt_scratch_bytes(const GiParams &p, bool reference_stream, size_t chunk
 
 cudaError_t launch_bdpt(const SceneView &sv, const float4 *ref_shade, const GiParams &p, bool reference_stream,
                         size_t chunk_budget, void *scratch, uint32_t *argb, float *rgb, int *status, cudaStream_t st) {
-	const long npix = static_cast<long>(p.width) * p.height;
-	if (!reference_stream) {
-		k_bdpt_counter<<<static_cast<unsigned>((npix + 127) / 128), 128, 0, st>>>(sv, ref_shade, p, argb, rgb, status);
-		return cudaGetLastError();
-	}
 	const size_t rows = static_cast<size_t>(p.height);
 	const int cw = bdpt_chunk_width(p, chunk_budget);
 	const size_t samples = static_cast<size_t>(cw) * rows * p.samples;
@@ -630,13 +632,19 @@ cudaError_t launch_bdpt(const SceneView &sv, const float4 *ref_shade, const GiPa
 	float4 *rec = reinterpret_cast<float4 *>(base);
 	base += align256(samples * kBdptRecordSlots * 16);
 	uint8_t *cnt = reinterpret_cast<uint8_t *>(base);
-	k_mt_seed_rows<<<static_cast<unsigned>((rows + 127) / 128), 128, 0, st>>>(mt_s, mt_i, p.height);
+	if (reference_stream)
+		k_mt_seed_rows<<<static_cast<unsigned>((rows + 127) / 128), 128, 0, st>>>(mt_s, mt_i, p.height);
 	for (int x0 = 0; x0 < p.width; x0 += cw) {
 		const int x1 = std::min(p.width, x0 + cw);
-		{
+		if (reference_stream) {
 			TraceRange r("subpaths in row-stream order");
 			k_bdpt_rows<<<static_cast<unsigned>((rows + kRowsPerBlock - 1) / kRowsPerBlock), 32, 0, st>>>(
 			    sv, ref_shade, p, mt_s, mt_i, x0, x1, rec, cnt, status);
+		} else {
+			TraceRange r("subpaths, one thread per sample");
+			const long n = static_cast<long>(x1 - x0) * p.height * p.samples;
+			k_bdpt_counter_paths<<<static_cast<unsigned>((n + 127) / 128), 128, 0, st>>>(sv, ref_shade, p, x0, x1,
+			                                                                            rec, cnt, status);
 		}
 		TraceRange r("connections");
 		const long n = static_cast<long>(x1 - x0) * p.height;

@@ -29,7 +29,7 @@ constexpr int kMltMaxBootstrap = 1 << 24;
 // Bidirectional path tracing. reference_stream: the reference's std::mt19937 per image
 // row (exact canvas; rows trace subpaths in stream order, pixels connect them in
 // parallel, in column chunks of at most chunk_budget bytes of subpath records);
-// otherwise Philox counter-based random numbers, one thread per pixel.
+// otherwise Philox counter-based random numbers, subpaths one thread per sample.
 size_t bdpt_scratch_bytes(const GiParams &p, bool reference_stream, size_t chunk_budget);
 cudaError_t launch_bdpt(const SceneView &sv, const float4 *ref_shade, const GiParams &p, bool reference_stream,
                         size_t chunk_budget, void *scratch, uint32_t *argb, float *rgb, int *status, cudaStream_t st);
