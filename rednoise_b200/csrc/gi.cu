@@ -8,14 +8,14 @@
 // reference's. The number of draws a sample takes depends on its subpath lengths,
 // so a row's samples are found in stream order: one thread per row traces the
 // camera and light subpaths (the closest-hit chain) and records their vertices;
-// then one thread per pixel makes every connection (the shadow rays, most of the
-// work) and sums them in the reference's order. Columns are processed in chunks so
+// then the connections (the shadow rays, most of the work) run one thread per
+// connection and are summed per pixel in the reference's order. Columns are processed in chunks so
 // the vertex records stay within a fixed budget; the row streams persist in
 // device memory between chunks.
 //
 // Bidirectional, counter stream: the same estimator with each (pixel, sample)
 // drawing from Philox-4x32-10 under the seed; the subpaths are traced one thread
-// per sample, then the same per-pixel connection pass sums them in order.
+// per sample, then the same connection passes.
 //
 // Metropolis: many chains run in parallel, one thread each. A bootstrap of
 // independent paths estimates the normalisation b as the reference does; chain
@@ -184,34 +184,6 @@ __device__ void bdpt_subpaths(Ctx &c, const GiParams &p, const GiCam &cam, int x
 	nl = 1 + gi_subpath<kAlone>(c, lp + kGiEps * ldir, ldir, le, lv + 1, lcode, draw);
 }
 
-// Every camera vertex to every light vertex with the uniform MIS weight
-// (src/BDPT.cpp:110-134), added to acc in the reference's order.
-__device__ void bdpt_connect(Ctx &c, const GV *cam, int nc, const GV *lv, int nl, V3 &acc) {
-	for (int i = 0; i < nc; i++) {
-		const GV cv = cam[i];
-		for (int j = 0; j < nl; j++) {
-			const GV l = lv[j];
-			V3 d = l.p - cv.p;
-			const float dist2 = dot(d, d);
-			const float dist = sqrtf(dist2);
-			d = d / dist;
-			const float cosC = dot(cv.n, d);
-			const float cosL = dot(l.n, -d);
-			if (cosC <= 0.0f || cosL <= 0.0f)
-				continue;
-			if (occluded(c, cv.p + cv.n * kGiEps, d, dist - 2.0f * kGiEps, -1))
-				continue;
-			const float G = cosC * cosL / dist2;
-			const V3 fC = cv.albedo / kGiPi;
-			V3 contrib = cv.beta * fC * G * l.beta;
-			if (j > 0)
-				contrib = contrib * (l.albedo / kGiPi);
-			const float w = 1.0f / static_cast<float>(i + j + 2);
-			acc = acc + contrib * w;
-		}
-	}
-}
-
 // Reinhard and the 8-bit pack (src/BDPT.cpp:137-141, src/Metropolis.cpp:185-189).
 __device__ __forceinline__ uint32_t gi_pack(V3 c) {
 	c = 255.0f * mk(c.x / (c.x + 1.0f), c.y / (c.y + 1.0f), c.z / (c.z + 1.0f));
@@ -286,7 +258,7 @@ __global__ void __launch_bounds__(32) k_bdpt_rows(SceneView sv, const float4 *__
 }
 
 // Counter streams: every sample is independent, so the subpaths of columns
-// [x0, x1) are traced one thread per (pixel, sample) and recorded for k_bdpt_connect.
+// [x0, x1) are traced one thread per (pixel, sample) and recorded for the connections.
 __global__ void __launch_bounds__(128) k_bdpt_counter_paths(SceneView sv, const float4 *__restrict__ ref_shade,
                                                             GiParams p, int x0, int x1, float4 *__restrict__ rec,
                                                             uint8_t *__restrict__ cnt, int *status) {
@@ -325,35 +297,160 @@ __device__ __forceinline__ V3 replay(const float4 *ref_shade, const float4 *r, i
 	return beta;
 }
 
-// Connection pass over columns [x0, x1): one thread per pixel.
-__global__ void __launch_bounds__(128) k_bdpt_connect(SceneView sv, const float4 *__restrict__ ref_shade, GiParams p,
-                                                      int x0, int x1, const float4 *__restrict__ rec,
-                                                      const uint8_t *__restrict__ cnt, uint32_t *argb, float *rgb,
-                                                      int *status) {
+// ---- connections ----
+// Every camera vertex is joined to every light vertex (src/BDPT.cpp:110-134) in
+// three passes: k_bdpt_pairs lists the pairs that pass the two cosine tests (each
+// sample's in one block, in the reference's (i, j) order), k_bdpt_shadow traces
+// one shadow ray per listed pair, k_bdpt_fold sums the contributions per pixel in
+// the reference's order from the recorded occlusions. A list entry is
+// (sample << 5) | (i * 5 + j).
+constexpr int kBdptPairs = kGiMaxDepth * (kGiMaxDepth + 1); // 20 per sample at most
+
+struct ConnView {
+	int *pair_base;     // per sample: its first list entry
+	uint32_t *pair;     // list entries
+	uint8_t *occ;       // per entry: 1 if the shadow ray is blocked
+	unsigned *count;    // entries listed
+};
+
+__device__ __forceinline__ void replay_sample(const float4 *ref_shade, const float4 *r, int nc, int nls, GV *cv,
+                                              GV *lv) {
+	const V3 le = mk(30.0f, 30.0f, 30.0f) * gi_light_area();
+	replay(ref_shade, r, nc, mk(1.0f, 1.0f, 1.0f), cv);
+	const float4 l0 = r[kGiMaxDepth];
+	lv[0] = GV{mk(l0.x, l0.y, l0.z), mk(0.0f, -1.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), le};
+	replay(ref_shade, r + kGiMaxDepth + 1, nls, le, lv + 1);
+}
+
+// The direction, distance and the two cosines of one connection, with the
+// reference's operations; false where a cosine test rejects it.
+__device__ __forceinline__ bool connection(const GV &cv, const GV &l, V3 &d, float &dist, float &dist2, float &cosC,
+                                           float &cosL) {
+	d = l.p - cv.p;
+	dist2 = dot(d, d);
+	dist = sqrtf(dist2);
+	d = d / dist;
+	cosC = dot(cv.n, d);
+	cosL = dot(l.n, -d);
+	return !(cosC <= 0.0f || cosL <= 0.0f);
+}
+
+__global__ void __launch_bounds__(128) k_bdpt_pairs(const float4 *__restrict__ ref_shade, long samples,
+                                                    const float4 *__restrict__ rec, const uint8_t *__restrict__ cnt,
+                                                    ConnView cv_) {
+	// Every lane of the warp takes part in the prefix sum below (lanes past the last
+	// sample list nothing), so no early return.
+	const long sample = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+	const bool live = sample < samples;
+	uint32_t ok = 0; // bit i * 5 + j
+	if (live) {
+		const int k = cnt[sample];
+		const int nc = k & 15, nls = k >> 4;
+		GV cv[kGiMaxDepth], lv[kGiMaxDepth + 1];
+		replay_sample(ref_shade, rec + static_cast<size_t>(sample) * kBdptRecordSlots, nc, nls, cv, lv);
+		for (int i = 0; i < nc; i++)
+			for (int j = 0; j <= nls; j++) {
+				V3 d;
+				float dist, dist2, cosC, cosL;
+				if (connection(cv[i], lv[j], d, dist, dist2, cosC, cosL))
+					ok |= 1u << (i * 5 + j);
+			}
+	}
+	// one atomic per warp: the lanes' counts are prefix-summed with shuffles
+	const int lane = static_cast<int>(threadIdx.x & 31);
+	const int mine = __popc(ok);
+	int incl = mine;
+	for (int off = 1; off < 32; off <<= 1) {
+		const int v = __shfl_up_sync(0xffffffffu, incl, off);
+		if (lane >= off)
+			incl += v;
+	}
+	unsigned base = 0;
+	if (lane == 31 && incl > 0)
+		base = atomicAdd(cv_.count, static_cast<unsigned>(incl));
+	base = __shfl_sync(0xffffffffu, base, 31);
+	if (!live)
+		return;
+	const unsigned first = base + static_cast<unsigned>(incl - mine);
+	cv_.pair_base[sample] = static_cast<int>(first);
+	unsigned e = first;
+	for (uint32_t bits = ok; bits; bits &= bits - 1)
+		cv_.pair[e++] = (static_cast<uint32_t>(sample) << 5) | static_cast<uint32_t>(__ffs(bits) - 1);
+}
+
+__global__ void __launch_bounds__(128) k_bdpt_shadow(SceneView sv, const float4 *__restrict__ ref_shade,
+                                                     const float4 *__restrict__ rec, ConnView cv_, int *status) {
+	Ctx c{sv, ref_shade, nullptr, 0};
+	const unsigned n = *cv_.count;
+	for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+		const uint32_t w = cv_.pair[e];
+		const size_t sample = w >> 5;
+		const int code = static_cast<int>(w & 31u), i = code / 5, j = code % 5;
+		const float4 *r = rec + sample * kBdptRecordSlots;
+		const float4 a = r[i];
+		const int ca = __float_as_int(a.w);
+		const V3 tn = tri_normal(ref_shade, ca >> 1);
+		GV cvx, lx;
+		cvx.p = mk(a.x, a.y, a.z);
+		cvx.n = (ca & 1) ? -tn : tn;
+		const float4 b = r[kGiMaxDepth + j];
+		lx.p = mk(b.x, b.y, b.z);
+		if (j == 0) {
+			lx.n = mk(0.0f, -1.0f, 0.0f);
+		} else {
+			const int cb = __float_as_int(b.w);
+			const V3 tl = tri_normal(ref_shade, cb >> 1);
+			lx.n = (cb & 1) ? -tl : tl;
+		}
+		V3 d;
+		float dist, dist2, cosC, cosL;
+		connection(cvx, lx, d, dist, dist2, cosC, cosL);
+		cv_.occ[e] = occluded(c, cvx.p + cvx.n * kGiEps, d, dist - 2.0f * kGiEps, -1) ? 1 : 0;
+	}
+	if (c.err)
+		atomicOr(status, 1);
+}
+
+// Sums one pixel's connections over its samples in the reference's order: for each
+// sample, camera vertex i, light vertex j, contribution x uniform MIS weight.
+__global__ void __launch_bounds__(128) k_bdpt_fold(const float4 *__restrict__ ref_shade, GiParams p, int x0, int x1,
+                                                   const float4 *__restrict__ rec, const uint8_t *__restrict__ cnt,
+                                                   ConnView cv_, uint32_t *argb, float *rgb) {
 	const int cw = x1 - x0;
 	const long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
 	if (idx >= static_cast<long>(cw) * p.height)
 		return;
 	const int y = static_cast<int>(idx / cw), x = x0 + static_cast<int>(idx % cw);
-	Ctx c{sv, ref_shade, nullptr, 0};
-	const V3 le = mk(30.0f, 30.0f, 30.0f) * gi_light_area();
 	V3 acc = mk(0.0f, 0.0f, 0.0f);
 	for (int s = 0; s < p.samples; s++) {
 		const size_t sample = static_cast<size_t>(idx) * p.samples + s;
 		const int k = cnt[sample];
 		const int nc = k & 15, nls = k >> 4;
-		const float4 *r = rec + sample * kBdptRecordSlots;
 		GV cv[kGiMaxDepth], lv[kGiMaxDepth + 1];
-		replay(ref_shade, r, nc, mk(1.0f, 1.0f, 1.0f), cv);
-		const float4 l0 = r[kGiMaxDepth];
-		lv[0] = GV{mk(l0.x, l0.y, l0.z), mk(0.0f, -1.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), le};
-		replay(ref_shade, r + kGiMaxDepth + 1, nls, le, lv + 1);
-		bdpt_connect(c, cv, nc, lv, 1 + nls, acc);
+		replay_sample(ref_shade, rec + sample * kBdptRecordSlots, nc, nls, cv, lv);
+		unsigned e = static_cast<unsigned>(cv_.pair_base[sample]);
+		for (int i = 0; i < nc; i++) {
+			const GV c0 = cv[i];
+			for (int j = 0; j <= nls; j++) {
+				const GV l = lv[j];
+				V3 d;
+				float dist, dist2, cosC, cosL;
+				if (!connection(c0, l, d, dist, dist2, cosC, cosL))
+					continue;
+				if (cv_.occ[e++])
+					continue;
+				const float G = cosC * cosL / dist2;
+				const V3 fC = c0.albedo / kGiPi;
+				V3 contrib = c0.beta * fC * G * l.beta;
+				if (j > 0)
+					contrib = contrib * (l.albedo / kGiPi);
+				const float w = 1.0f / static_cast<float>(i + j + 2);
+				acc = acc + contrib * w;
+			}
+		}
 	}
 	const V3 col = acc * (p.exposure / static_cast<float>(p.samples));
 	gi_store(p, static_cast<long>(y) * p.width + x, col, argb, rgb);
-	if (c.err)
-		atomicOr(status, 1);
 }
 
 // ---- Metropolis ----
@@ -602,9 +699,16 @@ __global__ void k_mlt_resolve(GiParams p, const float *__restrict__ image, const
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// Bytes per sample of a chunk: its subpath record, its first list entry, and up to
+// 20 list entries with their occlusion bytes.
+constexpr size_t kBdptSampleBytes = kBdptRecordBytes + 4 + kBdptPairs * 5;
+
 int bdpt_chunk_width(const GiParams &p, size_t budget) {
-	const size_t per_col = static_cast<size_t>(p.height) * static_cast<size_t>(p.samples) * kBdptRecordBytes;
-	size_t cw = per_col ? budget / per_col : 1;
+	const size_t per_col = static_cast<size_t>(p.height) * static_cast<size_t>(p.samples);
+	size_t cw = per_col ? budget / (per_col * kBdptSampleBytes) : 1;
+	// list entries hold the sample index in 27 bits
+	if (per_col)
+		cw = std::min(cw, (size_t(1) << 27) / per_col);
 	cw = std::max<size_t>(1, std::min<size_t>(cw, static_cast<size_t>(p.width)));
 	return static_cast<int>(cw);
 }
@@ -616,7 +720,8 @@ size_t bdpt_scratch_bytes(const GiParams &p, bool reference_stream, size_t chunk
 	const size_t rows = static_cast<size_t>(p.height);
 	const size_t samples = static_cast<size_t>(bdpt_chunk_width(p, chunk_budget)) * rows * p.samples;
 	return align256(624 * 4 * rows) + align256(4 * rows) + align256(samples * kBdptRecordSlots * 16) +
-	       align256(samples);
+	       align256(samples) + align256(samples * 4) + align256(samples * kBdptPairs * 4) +
+	       align256(samples * kBdptPairs) + 256;
 }
 
 cudaError_t launch_bdpt(const SceneView &sv, const float4 *ref_shade, const GiParams &p, bool reference_stream,
@@ -632,6 +737,15 @@ cudaError_t launch_bdpt(const SceneView &sv, const float4 *ref_shade, const GiPa
 	float4 *rec = reinterpret_cast<float4 *>(base);
 	base += align256(samples * kBdptRecordSlots * 16);
 	uint8_t *cnt = reinterpret_cast<uint8_t *>(base);
+	base += align256(samples);
+	ConnView cv;
+	cv.pair_base = reinterpret_cast<int *>(base);
+	base += align256(samples * 4);
+	cv.pair = reinterpret_cast<uint32_t *>(base);
+	base += align256(samples * kBdptPairs * 4);
+	cv.occ = reinterpret_cast<uint8_t *>(base);
+	base += align256(samples * kBdptPairs);
+	cv.count = reinterpret_cast<unsigned *>(base);
 	if (reference_stream)
 		k_mt_seed_rows<<<static_cast<unsigned>((rows + 127) / 128), 128, 0, st>>>(mt_s, mt_i, p.height);
 	for (int x0 = 0; x0 < p.width; x0 += cw) {
@@ -647,9 +761,15 @@ cudaError_t launch_bdpt(const SceneView &sv, const float4 *ref_shade, const GiPa
 			                                                                            rec, cnt, status);
 		}
 		TraceRange r("connections");
-		const long n = static_cast<long>(x1 - x0) * p.height;
-		k_bdpt_connect<<<static_cast<unsigned>((n + 127) / 128), 128, 0, st>>>(sv, ref_shade, p, x0, x1, rec, cnt,
-		                                                                       argb, rgb, status);
+		const long ns = static_cast<long>(x1 - x0) * p.height * p.samples;
+		const long npx = static_cast<long>(x1 - x0) * p.height;
+		cudaError_t e = cudaMemsetAsync(cv.count, 0, sizeof(unsigned), st);
+		if (e != cudaSuccess)
+			return e;
+		k_bdpt_pairs<<<static_cast<unsigned>((ns + 127) / 128), 128, 0, st>>>(ref_shade, ns, rec, cnt, cv);
+		k_bdpt_shadow<<<148 * 16, 128, 0, st>>>(sv, ref_shade, rec, cv, status);
+		k_bdpt_fold<<<static_cast<unsigned>((npx + 127) / 128), 128, 0, st>>>(ref_shade, p, x0, x1, rec, cnt, cv, argb,
+		                                                                      rgb);
 	}
 	return cudaGetLastError();
 }
