@@ -124,6 +124,20 @@ __device__ __forceinline__ unsigned cell_of(float x, float lo, float hi) {
 	constexpr float kCells = static_cast<float>(1 << kBinCellBits);
 	return quantize((x - lo) * __fdividef(1.0f, hi - lo), kCells);
 }
+// 15-bit Morton cell (5 bits per axis over the scene's box) of a shadow ray's origin.
+__device__ __forceinline__ unsigned point_bin(const SceneView &sv, const F3 &o) {
+	const float q[3] = {o.x, o.y, o.z};
+	unsigned m = 0;
+#pragma unroll
+	for (int a = 0; a < 3; a++) {
+		const unsigned c = quantize((q[a] - sv.root_lo[a]) * __fdividef(1.0f, sv.root_hi[a] - sv.root_lo[a]), 32.0f);
+#pragma unroll
+		for (int b = 0; b < 5; b++)
+			m |= ((c >> b) & 1u) << (3 * b + a);
+	}
+	return m;
+}
+
 __device__ __forceinline__ unsigned ray_bin(const SceneView &sv, const F3 &o, const F3 &d) {
 	const float inv_l1 = __fdividef(1.0f, fabsf(d.x) + fabsf(d.y) + fabsf(d.z));
 	float px = d.x * inv_l1, py = d.y * inv_l1;
@@ -174,6 +188,8 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 			sr.valid = false;
 		}
 		if (sr.valid) {
+			if (write_keys)
+				pool.sh_keys[si] = static_cast<uint16_t>(point_bin(job.sc.sv, sr.o));
 			pool.sh_o[si] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
 			pool.sh_d[si] = make_float4(sr.d.x, sr.d.y, sr.d.z, __int_as_float(sr.ignore));
 			pool.sh_c[si] = make_float4(sr.contrib.x, sr.contrib.y, sr.contrib.z, __int_as_float(slot));
@@ -196,7 +212,7 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 }
 
 __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ jobs, WfPool pool, int k, int only_job,
-                                                   int *status) {
+                                                   const int *__restrict__ order, int *status) {
 	const unsigned n = pool.counters[kCntShadow + k];
 	const int lane = threadIdx.x & 31;
 	int err = 0;
@@ -207,8 +223,9 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 		base = __shfl_sync(0xffffffffu, base, 0);
 		if (base >= n)
 			break;
-		const unsigned i = base + lane;
-		if (i < n) {
+		const unsigned q = base + lane;
+		if (q < n) {
+			const unsigned i = order ? static_cast<unsigned>(order[q]) : q;
 			const float4 so = pool.sh_o[i], sd = pool.sh_d[i];
 			const float4 sc = pool.sh_c[i];
 			const int slot = __float_as_int(sc.w);
@@ -328,28 +345,37 @@ __global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ 
 // the shade stage wrote): histogram, exclusive scan, scatter. Blocks of 1024
 // threads with a kBins-word histogram in dynamic shared memory; keys are masked
 // to kBins so every shared-memory index is in range.
-__global__ void __launch_bounds__(1024) k_wf_bin_count(WfPool pool, int k) {
+// A counting sort of `*count` items by 15-bit key: out[position] = items[i], or i
+// when items is null.
+struct BinSrc {
+	const uint16_t *keys;
+	const unsigned *count;
+	const int *items;
+	int *out;
+};
+
+__global__ void __launch_bounds__(1024) k_wf_bin_count(BinSrc src, unsigned *bins) {
 	extern __shared__ unsigned h[];
 	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
 		h[b] = 0;
 	__syncthreads();
-	const unsigned n = pool.counters[kCntRays + k];
+	const unsigned n = *src.count;
 	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-		atomicAdd(&h[pool.keys[i] & (kBins - 1)], 1u);
+		atomicAdd(&h[src.keys[i] & (kBins - 1)], 1u);
 	__syncthreads();
 	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
 		if (h[b])
-			atomicAdd(&pool.bins[b], h[b]);
+			atomicAdd(&bins[b], h[b]);
 }
 
 // One block of 1024 threads, kBins / 1024 consecutive bins each: counts -> exclusive offsets.
 constexpr int kScanThreads = 1024;
 constexpr int kBinsPerThread = kBins / kScanThreads;
 static_assert(kBins % kScanThreads == 0, "k_wf_bin_scan splits the bins evenly");
-__global__ void __launch_bounds__(kScanThreads) k_wf_bin_scan(WfPool pool) {
+__global__ void __launch_bounds__(kScanThreads) k_wf_bin_scan(unsigned *bins) {
 	__shared__ unsigned warp_sum[kScanThreads / 32];
 	const int t = threadIdx.x;
-	unsigned *mine = pool.bins + t * kBinsPerThread;
+	unsigned *mine = bins + t * kBinsPerThread;
 	unsigned own = 0;
 	for (int i = 0; i < kBinsPerThread; i++)
 		own += mine[i];
@@ -381,34 +407,43 @@ __global__ void __launch_bounds__(kScanThreads) k_wf_bin_scan(WfPool pool) {
 	}
 }
 
-// Each block takes a contiguous chunk of the queue, reserves its share of every
-// bin with one atomic per non-empty bin, then places its rays.
-__global__ void __launch_bounds__(1024) k_wf_bin_scatter(WfPool pool, int k, int *status) {
+// Each block takes a contiguous chunk of the items, reserves its share of every
+// bin with one atomic per non-empty bin, then places its items.
+__global__ void __launch_bounds__(1024) k_wf_bin_scatter(BinSrc src, unsigned *bins, int *status) {
 	extern __shared__ unsigned h[];
 	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
 		h[b] = 0;
 	__syncthreads();
-	const unsigned n = pool.counters[kCntRays + k];
+	const unsigned n = *src.count;
 	const unsigned per = (n + gridDim.x - 1) / gridDim.x;
 	const unsigned c0 = min(n, blockIdx.x * per);
 	const unsigned c1 = min(n, c0 + per);
 	for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x)
-		atomicAdd(&h[pool.keys[i] & (kBins - 1)], 1u);
+		atomicAdd(&h[src.keys[i] & (kBins - 1)], 1u);
 	__syncthreads();
 	for (int b = threadIdx.x; b < kBins; b += blockDim.x) {
 		const unsigned c = h[b];
-		h[b] = c ? atomicAdd(&pool.bins[b], c) : 0u;
+		h[b] = c ? atomicAdd(&bins[b], c) : 0u;
 	}
 	__syncthreads();
-	const int *__restrict__ q = pool.queue[k & 1];
 	for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-		const unsigned pos = atomicAdd(&h[pool.keys[i] & (kBins - 1)], 1u);
+		const unsigned pos = atomicAdd(&h[src.keys[i] & (kBins - 1)], 1u);
 		if (kBoundsCheck && pos >= n) {
 			atomicOr(status, 1);
 			continue;
 		}
-		pool.sorted[pos] = q[i];
+		src.out[pos] = src.items ? src.items[i] : static_cast<int>(i);
 	}
+}
+
+cudaError_t bin_sort(const BinSrc &src, unsigned *bins, int grid, int *status, cudaStream_t st) {
+	cudaError_t e = cudaMemsetAsync(bins, 0, kBins * sizeof(unsigned), st);
+	if (e != cudaSuccess)
+		return e;
+	k_wf_bin_count<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, bins);
+	k_wf_bin_scan<<<1, kScanThreads, 0, st>>>(bins);
+	k_wf_bin_scatter<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, bins, status);
+	return cudaGetLastError();
 }
 
 // Adds each pixel's samples of this wave to its sum, in sample order.
@@ -448,12 +483,10 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 	for (int k = 0; k < max_depth; k++) {
 		const int *q = pool.queue[k & 1];
 		if (sort && k > 0) {
-			e = cudaMemsetAsync(pool.bins, 0, kBins * sizeof(unsigned), st);
+			e = bin_sort(BinSrc{pool.keys, pool.counters + kCntRays + k, q, pool.sorted}, pool.bins, lc.grid_bin,
+			             status, st);
 			if (e != cudaSuccess)
 				return e;
-			k_wf_bin_count<<<lc.grid_bin, 1024, kBins * sizeof(unsigned), st>>>(pool, k);
-			k_wf_bin_scan<<<1, kScanThreads, 0, st>>>(pool);
-			k_wf_bin_scatter<<<lc.grid_bin, 1024, kBins * sizeof(unsigned), st>>>(pool, k, status);
 			q = pool.sorted;
 		}
 		const int oj = wave.only_job;
@@ -466,8 +499,18 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 		k_wf_shade<<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, q, sort ? 1 : 0, status);
 		if (use_dyn)
 			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, oj, status);
-		else
-			k_wf_shadow<<<lc.grid_sh, 128, kWfShadowSmem, st>>>(d_jobs, pool, k, oj, status);
+		else {
+			// with binning, the shadow records are traced in the order of their origins' cells
+			const bool sort_sh = sort && pool.sh_keys && pool.sh_sorted;
+			if (sort_sh) {
+				e = bin_sort(BinSrc{pool.sh_keys, pool.counters + kCntShadow + k, nullptr, pool.sh_sorted}, pool.bins,
+				             lc.grid_bin, status, st);
+				if (e != cudaSuccess)
+					return e;
+			}
+			k_wf_shadow<<<lc.grid_sh, 128, kWfShadowSmem, st>>>(d_jobs, pool, k, oj, sort_sh ? pool.sh_sorted : nullptr,
+			                                                    status);
+		}
 	}
 	const int gacc = (wave.n_pix + 255) / 256 < 148 * 8 ? (wave.n_pix + 255) / 256 : 148 * 8;
 	k_wf_accumulate<<<gacc, 256, 0, st>>>(d_jobs, pool, wave);

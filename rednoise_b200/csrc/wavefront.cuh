@@ -57,6 +57,10 @@ struct WfPool {
 	uint16_t *keys;
 	int *sorted;
 	unsigned *bins; // kBins counters, then offsets
+	// With binning on, each shadow record's key (the 15-bit Morton cell of its
+	// origin, the shading point) and the shadow stage's order sorted by it.
+	uint16_t *sh_keys;
+	int *sh_sorted;
 	int capacity;
 };
 
