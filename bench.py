@@ -410,7 +410,12 @@ def run_ours(args):
     else:
         spw = tuned["samples_per_wave"] if integ == 0 else max(1, min(spp, (1 << 20) // (W * H)))
         waves = (spp + spw - 1) // spw
-        launches_per_step = waves * (2 + 3 * args.depth) + 1  # camera, 3 stages per bounce, accumulate; resolve
+        per_wave = 2 + 3 * args.depth  # camera, 3 stages per bounce, accumulate
+        if tuned["ray_sort"] and not tuned["dynamic_fetch"]:
+            # counting sorts (count, scan, scatter) of the ray queue before bounces 1.. and
+            # of the shadow queue at every bounce
+            per_wave += 3 * (args.depth - 1) + 3 * args.depth
+        launches_per_step = waves * per_wave + 1  # + resolve
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -544,7 +549,7 @@ def run_ours(args):
                      "algorithmic": "24 B per node-box test + 36 B per triangle test of the reference-order "
                                     "traversal, counted on the GPU for 1 spp of the same frame",
                      "kernel_ms": kernel_ms,
-                     "scope": "whole frame: the closest-hit and shadow traversal kernels are 81 % of its device "
+                     "scope": "whole frame: the closest-hit and shadow traversal kernels are 77 % of its device "
                               "time (ncu launch list); traffic scaled from a 480x270 capture"},
         "clocks": clk,
         "rmse_vs_fp64_64spp": rmse,
