@@ -103,9 +103,11 @@ __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ job
 		atomicOr(status, 1);
 }
 
-// Bin of a ray for the binning sort: an octahedral cell of its direction
-// (8 x 8 over the unit octahedron unfolded onto a square) above a Morton code of
-// the cell that holds its origin (8 x 8 x 8 over the scene's bounding box).
+// Bin of a ray for the binning sort: a Morton code of the cell that holds its
+// origin (8 x 8 x 8 over the scene's bounding box) above an octahedral cell of its
+// direction (8 x 8 over the unit octahedron unfolded onto a square). Origin-major
+// order measured 2.5-3 % faster on the 1.31M-triangle frame than direction-major,
+// and both beat keys that give either part fewer bits.
 constexpr int kBinDirBits = 6;
 constexpr int kBinCellBits = 3;
 static_assert(kBinDirBits + 3 * kBinCellBits == kBinBits, "bin key width");
@@ -153,7 +155,7 @@ __device__ __forceinline__ unsigned ray_bin(const SceneView &sv, const F3 &o, co
 	const unsigned m = spread_bits(cell_of(o.x, sv.root_lo[0], sv.root_hi[0])) |
 	                   (spread_bits(cell_of(o.y, sv.root_lo[1], sv.root_hi[1])) << 1) |
 	                   (spread_bits(cell_of(o.z, sv.root_lo[2], sv.root_hi[2])) << 2);
-	return (dir << (3 * kBinCellBits)) | m;
+	return (m << kBinDirBits) | dir;
 }
 
 __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
@@ -496,7 +498,11 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			k_wf_extend<kOrderNearest><<<lc.grid_ext, 128, kWfExtendSmem, st>>>(d_jobs, pool, k, q, oj, status);
 		else
 			k_wf_extend<kOrderReference><<<lc.grid_ext, 128, kWfExtendSmem, st>>>(d_jobs, pool, k, q, oj, status);
-		k_wf_shade<<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, q, sort ? 1 : 0, status);
+		// Shading takes the queue in its append order, not the binned order: the previous
+		// bounce appended each warp's surviving slots in increasing order, so the path
+		// state reads and writes of neighbouring lanes fall on neighbouring slots. The
+		// results do not depend on the order in which paths are shaded.
+		k_wf_shade<<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, pool.queue[k & 1], sort ? 1 : 0, status);
 		if (use_dyn)
 			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, oj, status);
 		else {
