@@ -103,30 +103,21 @@ __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ job
 		atomicOr(status, 1);
 }
 
-// Bin of a ray for the binning sort: a Morton code of the cell that holds its
-// origin (8 x 8 x 8 over the scene's bounding box) above an octahedral cell of its
-// direction (8 x 8 over the unit octahedron unfolded onto a square). Origin-major
-// order measured 2.5-3 % faster on the 1.31M-triangle frame than direction-major,
-// and both beat keys that give either part fewer bits.
-constexpr int kBinDirBits = 6;
-constexpr int kBinCellBits = 3;
-static_assert(kBinDirBits + 3 * kBinCellBits == kBinBits, "bin key width");
-__device__ __forceinline__ unsigned spread_bits(unsigned x) {
-	unsigned r = 0;
-#pragma unroll
-	for (int b = 0; b < kBinCellBits; b++)
-		r |= ((x >> b) & 1u) << (3 * b);
-	return r;
-}
+// Bins of the binning sorts. A continuation ray's bin is the Morton cell of its
+// origin (point_bin, 5 bits per axis over the scene's box) refined by a 16 x 16
+// octahedral cell of its direction (dir_cell); a shadow record's bin is the cell of
+// its origin alone (its direction points at the light). On the 1.31M-triangle
+// 1080p frame this 23-bit order, sorted in two counting passes, took the frame from
+// 208 to 191 ms against a single 15-bit key (an 8 x 8 x 8 origin cell above an
+// 8 x 8 direction cell); a 30-bit key (64 x 64 x 64 origin cells, 64 x 64
+// direction cells) left too few rays per bin to fill a warp and gained a third as
+// much. Of the single 15-bit splits, origin-major beat direction-major, and keys that
+// gave either part fewer bits were slower still.
 // fmaxf maps a NaN (a flat extent: 0 * inf) to cell 0
 __device__ __forceinline__ unsigned quantize(float x, float cells) {
 	return static_cast<unsigned>(fminf(fmaxf(x * cells, 0.0f), cells - 1.0f));
 }
-__device__ __forceinline__ unsigned cell_of(float x, float lo, float hi) {
-	constexpr float kCells = static_cast<float>(1 << kBinCellBits);
-	return quantize((x - lo) * __fdividef(1.0f, hi - lo), kCells);
-}
-// 15-bit Morton cell (5 bits per axis over the scene's box) of a shadow ray's origin.
+// 15-bit Morton cell (5 bits per axis over the scene's box) of a ray's origin.
 __device__ __forceinline__ unsigned point_bin(const SceneView &sv, const F3 &o) {
 	const float q[3] = {o.x, o.y, o.z};
 	unsigned m = 0;
@@ -139,8 +130,10 @@ __device__ __forceinline__ unsigned point_bin(const SceneView &sv, const F3 &o) 
 	}
 	return m;
 }
+static_assert(kBinBits == 15, "point_bin writes 15-bit keys");
 
-__device__ __forceinline__ unsigned ray_bin(const SceneView &sv, const F3 &o, const F3 &d) {
+// 8-bit cell of a direction: 16 x 16 over the unit octahedron unfolded onto a square.
+__device__ __forceinline__ unsigned dir_cell(const F3 &d) {
 	const float inv_l1 = __fdividef(1.0f, fabsf(d.x) + fabsf(d.y) + fabsf(d.z));
 	float px = d.x * inv_l1, py = d.y * inv_l1;
 	if (d.z < 0.0f) { // fold the lower hemisphere onto the corners
@@ -149,13 +142,7 @@ __device__ __forceinline__ unsigned ray_bin(const SceneView &sv, const F3 &o, co
 		px = qx;
 		py = qy;
 	}
-	constexpr float kDirCells = static_cast<float>(1 << (kBinDirBits / 2));
-	const unsigned dir = (quantize(0.5f * (py + 1.0f), kDirCells) << (kBinDirBits / 2)) |
-	                     quantize(0.5f * (px + 1.0f), kDirCells);
-	const unsigned m = spread_bits(cell_of(o.x, sv.root_lo[0], sv.root_hi[0])) |
-	                   (spread_bits(cell_of(o.y, sv.root_lo[1], sv.root_hi[1])) << 1) |
-	                   (spread_bits(cell_of(o.z, sv.root_lo[2], sv.root_hi[2])) << 2);
-	return (m << kBinDirBits) | dir;
+	return (quantize(0.5f * (py + 1.0f), 16.0f) << 4) | quantize(0.5f * (px + 1.0f), 16.0f);
 }
 
 __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
@@ -204,8 +191,10 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 		}
 		if (alive) {
 			qn[ni] = slot;
-			if (write_keys)
-				pool.keys[ni] = static_cast<uint16_t>(ray_bin(job.sc.sv, ps.o, ps.d));
+			if (write_keys) {
+				pool.keys[ni] = static_cast<uint16_t>(point_bin(job.sc.sv, ps.o));
+				pool.fine[ni] = static_cast<uint8_t>(dir_cell(ps.d));
+			}
 			pool.o[slot] = make_float4(ps.o.x, ps.o.y, ps.o.z, __int_as_float(ps.ignore));
 			pool.d[slot] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.prev_pdf);
 			pool.beta[slot] = make_float4(ps.beta.x, ps.beta.y, ps.beta.z, __int_as_float(ps.bounce));
@@ -343,17 +332,19 @@ __global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ 
 		atomicOr(status, 1);
 }
 
-// Binning sort of the closest-hit queue of bounce k (counting sort on the keys
-// the shade stage wrote): histogram, exclusive scan, scatter. Blocks of 1024
+// Binning sorts of the closest-hit and shadow queues of bounce k (counting sorts on
+// the keys the shade stage wrote): histogram, exclusive scan, scatter. Blocks of 1024
 // threads with a kBins-word histogram in dynamic shared memory; keys are masked
 // to kBins so every shared-memory index is in range.
 // A counting sort of `*count` items by 15-bit key: out[position] = items[i], or i
-// when items is null.
+// when items is null; with fine set, fine_out[position] = fine[i] as well.
 struct BinSrc {
 	const uint16_t *keys;
 	const unsigned *count;
 	const int *items;
 	int *out;
+	const uint8_t *fine;
+	uint8_t *fine_out;
 };
 
 __global__ void __launch_bounds__(1024) k_wf_bin_count(BinSrc src, unsigned *bins) {
@@ -435,6 +426,68 @@ __global__ void __launch_bounds__(1024) k_wf_bin_scatter(BinSrc src, unsigned *b
 			continue;
 		}
 		src.out[pos] = src.items ? src.items[i] : static_cast<int>(i);
+		if (src.fine)
+			src.fine_out[pos] = src.fine[i];
+	}
+}
+
+// Second level of the ray sort: block b takes origin cell b's entries of the first
+// level's output (after the scatter bins[b] holds the end of cell b, so the cell
+// spans [bins[b-1], bins[b])) and places them by their 8-bit direction cell with a
+// shared-memory counting sort. The queue ends up ordered by (origin cell,
+// direction cell); entries of one bin keep no particular order.
+constexpr int kFineBins = 256;
+__global__ void __launch_bounds__(kFineBins) k_wf_bin_refine(const unsigned *bins, const int *in, const uint8_t *fine,
+                                                             int *out, unsigned n_max, int *status) {
+	__shared__ unsigned h[kFineBins];
+	__shared__ unsigned wsum[kFineBins / 32];
+	const unsigned s = blockIdx.x ? bins[blockIdx.x - 1] : 0u;
+	const unsigned e = bins[blockIdx.x];
+	if (e <= s) // the same for every thread of the block
+		return;
+	if (kBoundsCheck && e > n_max) {
+		if (threadIdx.x == 0)
+			atomicOr(status, 1);
+		return;
+	}
+	const int t = threadIdx.x;
+	h[t] = 0;
+	__syncthreads();
+	for (unsigned i = s + t; i < e; i += kFineBins)
+		atomicAdd(&h[fine[i]], 1u);
+	__syncthreads();
+	// exclusive scan of the kFineBins counts, one per thread
+	const unsigned c = h[t];
+	unsigned x = c;
+	for (int o = 1; o < 32; o <<= 1) {
+		const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+		if ((t & 31) >= o)
+			x += y;
+	}
+	if ((t & 31) == 31)
+		wsum[t >> 5] = x;
+	__syncthreads();
+	if (t < 32) {
+		const unsigned w = t < kFineBins / 32 ? wsum[t] : 0u;
+		unsigned z = w;
+		for (int o = 1; o < 32; o <<= 1) {
+			const unsigned y = __shfl_up_sync(0xffffffffu, z, o);
+			if (t >= o)
+				z += y;
+		}
+		if (t < kFineBins / 32)
+			wsum[t] = z - w;
+	}
+	__syncthreads();
+	h[t] = s + wsum[t >> 5] + x - c;
+	__syncthreads();
+	for (unsigned i = s + t; i < e; i += kFineBins) {
+		const unsigned pos = atomicAdd(&h[fine[i]], 1u);
+		if (kBoundsCheck && pos >= e) {
+			atomicOr(status, 1);
+			continue;
+		}
+		out[pos] = in[i];
 	}
 }
 
@@ -481,14 +534,18 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 	const int gcam = (wave.n_slots + 255) / 256 < 148 * 8 ? (wave.n_slots + 255) / 256 : 148 * 8;
 	k_wf_camera<<<gcam, 256, 0, st>>>(d_jobs, pool, wave);
 	const bool use_dyn = lc.dyn && order == kOrderReference;
-	const bool sort = lc.sort && pool.keys && pool.sorted && pool.bins;
+	const bool sort = lc.sort && pool.keys && pool.fine && pool.sorted_coarse && pool.sorted_fine && pool.sorted &&
+	                  pool.bins;
 	for (int k = 0; k < max_depth; k++) {
 		const int *q = pool.queue[k & 1];
 		if (sort && k > 0) {
-			e = bin_sort(BinSrc{pool.keys, pool.counters + kCntRays + k, q, pool.sorted}, pool.bins, lc.grid_bin,
-			             status, st);
+			e = bin_sort(BinSrc{pool.keys, pool.counters + kCntRays + k, q, pool.sorted_coarse, pool.fine,
+			                    pool.sorted_fine},
+			             pool.bins, lc.grid_bin, status, st);
 			if (e != cudaSuccess)
 				return e;
+			k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.sorted_coarse, pool.sorted_fine, pool.sorted,
+			                                            static_cast<unsigned>(pool.capacity), status);
 			q = pool.sorted;
 		}
 		const int oj = wave.only_job;
@@ -509,8 +566,9 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			// with binning, the shadow records are traced in the order of their origins' cells
 			const bool sort_sh = sort && pool.sh_keys && pool.sh_sorted;
 			if (sort_sh) {
-				e = bin_sort(BinSrc{pool.sh_keys, pool.counters + kCntShadow + k, nullptr, pool.sh_sorted}, pool.bins,
-				             lc.grid_bin, status, st);
+				e = bin_sort(BinSrc{pool.sh_keys, pool.counters + kCntShadow + k, nullptr, pool.sh_sorted, nullptr,
+				                    nullptr},
+				             pool.bins, lc.grid_bin, status, st);
 				if (e != cudaSuccess)
 					return e;
 			}

@@ -49,12 +49,18 @@ struct WfPool {
 	// counters: [0, kWfMaxDepth] ray-queue lengths per bounce, [kWfMaxDepth+1 ...] shadow
 	// lengths per bounce, then per-bounce fetch counters of extend and shadow.
 	unsigned *counters;
-	// Ray binning (optional): the shade stage writes each continuation ray's bin
-	// (coarse cell of its direction, coarse cell of its origin) to keys; before the next
-	// closest-hit stage a counting sort by bin rewrites the queue into sorted, so
-	// the lanes of a warp trace rays that start close together in similar
-	// directions and visit the same nodes.
+	// Ray binning (optional): the shade stage writes each continuation ray's bin in
+	// two parts, keys (the 15-bit Morton cell of its origin, 5 bits per axis over the
+	// scene's box) and fine (a 16 x 16 octahedral cell of its direction). Before the
+	// next closest-hit stage a counting sort by origin cell writes the queue to
+	// sorted_coarse (carrying each entry's direction cell to sorted_fine), and a
+	// counting sort of every origin cell's entries by direction cell writes it to
+	// sorted: the lanes of a warp then trace rays that start close together in
+	// similar directions and visit the same nodes.
 	uint16_t *keys;
+	uint8_t *fine;
+	int *sorted_coarse;
+	uint8_t *sorted_fine;
 	int *sorted;
 	unsigned *bins; // kBins counters, then offsets
 	// With binning on, each shadow record's key (the 15-bit Morton cell of its

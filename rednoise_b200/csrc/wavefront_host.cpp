@@ -41,6 +41,9 @@ rn_status WfContext::ensure_pool(int capacity) {
 	RNB_CUDA(sh_c_.ensure(n * 16));
 	RNB_CUDA(counters_.ensure(kCntTotal * sizeof(unsigned)));
 	RNB_CUDA(keys_.ensure(n * sizeof(uint16_t)));
+	RNB_CUDA(fine_.ensure(n));
+	RNB_CUDA(sorted_coarse_.ensure(n * 4));
+	RNB_CUDA(sorted_fine_.ensure(n));
 	RNB_CUDA(sorted_.ensure(n * 4));
 	RNB_CUDA(bins_.ensure(kBins * sizeof(unsigned)));
 	RNB_CUDA(sh_keys_.ensure(n * sizeof(uint16_t)));
@@ -61,6 +64,9 @@ rn_status WfContext::ensure_pool(int capacity) {
 	pool_.sh_c = sh_c_.as<float4>();
 	pool_.counters = counters_.as<unsigned>();
 	pool_.keys = keys_.as<uint16_t>();
+	pool_.fine = fine_.as<uint8_t>();
+	pool_.sorted_coarse = sorted_coarse_.as<int>();
+	pool_.sorted_fine = sorted_fine_.as<uint8_t>();
 	pool_.sorted = sorted_.as<int>();
 	pool_.bins = bins_.as<unsigned>();
 	pool_.sh_keys = sh_keys_.as<uint16_t>();
