@@ -131,6 +131,17 @@ __device__ __forceinline__ unsigned point_bin(const SceneView &sv, const F3 &o) 
 	return m;
 }
 static_assert(kBinBits == 15, "point_bin writes 15-bit keys");
+// 6-bit Morton sub-cell of a point inside its point_bin cell (the next 2 bits per axis).
+__device__ __forceinline__ unsigned point_sub_cell(const SceneView &sv, const F3 &o) {
+	const float q[3] = {o.x, o.y, o.z};
+	unsigned m = 0;
+#pragma unroll
+	for (int a = 0; a < 3; a++) {
+		const unsigned c = quantize((q[a] - sv.root_lo[a]) * __fdividef(1.0f, sv.root_hi[a] - sv.root_lo[a]), 128.0f);
+		m |= ((c & 1u) << a) | (((c >> 1) & 1u) << (3 + a));
+	}
+	return m;
+}
 
 // 8-bit cell of a direction: 16 x 16 over the unit octahedron unfolded onto a square.
 __device__ __forceinline__ unsigned dir_cell(const F3 &d) {
@@ -177,8 +188,10 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 			sr.valid = false;
 		}
 		if (sr.valid) {
-			if (write_keys)
+			if (write_keys) {
 				pool.sh_keys[si] = static_cast<uint16_t>(point_bin(job.sc.sv, sr.o));
+				pool.sh_fine[si] = static_cast<uint8_t>(point_sub_cell(job.sc.sv, sr.o));
+			}
 			pool.sh_o[si] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
 			pool.sh_d[si] = make_float4(sr.d.x, sr.d.y, sr.d.z, __int_as_float(sr.ignore));
 			pool.sh_c[si] = make_float4(sr.contrib.x, sr.contrib.y, sr.contrib.z, __int_as_float(slot));
@@ -564,13 +577,17 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, oj, status);
 		else {
 			// with binning, the shadow records are traced in the order of their origins' cells
-			const bool sort_sh = sort && pool.sh_keys && pool.sh_sorted;
+			// and sub-cells; the ray sort's first-level buffers are free until the next bounce
+			const bool sort_sh = sort && pool.sh_keys && pool.sh_fine && pool.sh_sorted;
 			if (sort_sh) {
-				e = bin_sort(BinSrc{pool.sh_keys, pool.counters + kCntShadow + k, nullptr, pool.sh_sorted, nullptr,
-				                    nullptr},
+				e = bin_sort(BinSrc{pool.sh_keys, pool.counters + kCntShadow + k, nullptr, pool.sorted_coarse,
+				                    pool.sh_fine, pool.sorted_fine},
 				             pool.bins, lc.grid_bin, status, st);
 				if (e != cudaSuccess)
 					return e;
+				k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.sorted_coarse, pool.sorted_fine,
+				                                            pool.sh_sorted, static_cast<unsigned>(pool.capacity),
+				                                            status);
 			}
 			k_wf_shadow<<<lc.grid_sh, 128, kWfShadowSmem, st>>>(d_jobs, pool, k, oj, sort_sh ? pool.sh_sorted : nullptr,
 			                                                    status);

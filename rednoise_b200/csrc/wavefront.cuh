@@ -63,9 +63,12 @@ struct WfPool {
 	uint8_t *sorted_fine;
 	int *sorted;
 	unsigned *bins; // kBins counters, then offsets
-	// With binning on, each shadow record's key (the 15-bit Morton cell of its
-	// origin, the shading point) and the shadow stage's order sorted by it.
+	// With binning on, each shadow record's key in two parts (the 15-bit Morton cell
+	// of its origin, the shading point, and the 6-bit Morton sub-cell of the origin
+	// inside it) and the shadow stage's order sorted by them (the same two counting
+	// sorts, with sorted_coarse and sorted_fine as scratch).
 	uint16_t *sh_keys;
+	uint8_t *sh_fine;
 	int *sh_sorted;
 	int capacity;
 };

@@ -47,6 +47,7 @@ rn_status WfContext::ensure_pool(int capacity) {
 	RNB_CUDA(sorted_.ensure(n * 4));
 	RNB_CUDA(bins_.ensure(kBins * sizeof(unsigned)));
 	RNB_CUDA(sh_keys_.ensure(n * sizeof(uint16_t)));
+	RNB_CUDA(sh_fine_.ensure(n));
 	RNB_CUDA(sh_sorted_.ensure(n * 4));
 	pool_.o = o_.as<float4>();
 	pool_.d = d_.as<float4>();
@@ -70,6 +71,7 @@ rn_status WfContext::ensure_pool(int capacity) {
 	pool_.sorted = sorted_.as<int>();
 	pool_.bins = bins_.as<unsigned>();
 	pool_.sh_keys = sh_keys_.as<uint16_t>();
+	pool_.sh_fine = sh_fine_.as<uint8_t>();
 	pool_.sh_sorted = sh_sorted_.as<int>();
 	pool_.capacity = capacity;
 	capacity_ = capacity;

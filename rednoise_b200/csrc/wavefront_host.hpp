@@ -25,9 +25,9 @@ inline int default_samples_per_wave(long n_pix, int spp) {
 
 // Device bytes per wavefront path slot: origin, direction, throughput, radiance,
 // pixel, sample, hit record, two queues and the sorted queue, the two parts of the bin
-// key, the first-level sorted queue with its fine keys, shadow record with its key and
-// sorted position.
-constexpr size_t kWfBytesPerPath = 4 * 16 + 4 * 4 + 3 * 4 + 2 + 1 + 4 + 1 + 3 * 16 + 2 + 4;
+// key, the first-level sorted queue with its fine keys, shadow record with the two
+// parts of its key and its sorted position.
+constexpr size_t kWfBytesPerPath = 4 * 16 + 4 * 4 + 3 * 4 + 2 + 1 + 4 + 1 + 3 * 16 + 2 + 1 + 4;
 
 // Memory the autotuners let a path pool take: half the free device memory, at most 32 GiB.
 inline cudaError_t wf_pool_budget(size_t &budget) {
@@ -78,7 +78,7 @@ private:
 	void release_graph();
 
 	DevBuf o_, d_, beta_, L_, pixel_, sample_, hit_idx_, hit_t_, q0_, q1_, sh_o_, sh_d_, sh_c_, counters_;
-	DevBuf keys_, fine_, sorted_coarse_, sorted_fine_, sorted_, bins_, sh_keys_, sh_sorted_;
+	DevBuf keys_, fine_, sorted_coarse_, sorted_fine_, sorted_, bins_, sh_keys_, sh_fine_, sh_sorted_;
 	DevBuf d_jobs_, d_wave_tab_;
 	WfPool pool_{};
 	int capacity_ = 0;
