@@ -354,8 +354,12 @@ rn_status rn_pt_scene_set_materials(rn_scene *scene, const float *albedo, const 
  * d_albedo = dL/d(albedo) and d_emission = dL/d(emitted radiance), 3 floats per
  * triangle each (overwritten; either may be NULL). Each view's settings give its
  * adjoint samples (spp, seed, sample_offset, depth, roulette). Every path is
- * regenerated from its RNG key and traced twice, so memory stays O(pixels).
- * Roulette probabilities are treated as constants. */
+ * regenerated from its RNG key and traced again. settings->integrator picks the
+ * schedule: RN_PT_MEGAKERNEL (one thread per path, memory O(pixels)),
+ * RN_PT_WAVEFRONT (waves of paths binned like rn_pt_render's wavefront; each path
+ * in flight keeps its continuation vertices, 32 bytes per vertex), RN_PT_AUTO
+ * (waves for scenes above 4096 triangles). Roulette probabilities are treated as
+ * constants. */
 rn_status rn_pt_backward(rn_scene *scene, int n_views, const rn_pt_camera *cameras, const rn_pt_settings *settings,
                          const float *const *d_images, unsigned flags, void *stream, float *d_albedo,
                          float *d_emission);

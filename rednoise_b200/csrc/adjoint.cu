@@ -42,17 +42,7 @@ __device__ __forceinline__ int find_view(const AdjView *v, int n, unsigned item)
 
 template <bool kShared>
 __device__ __forceinline__ void add3(float *gbuf, float *sbuf, int tri, F3 v) {
-	float *p = kShared ? sbuf + 3 * tri : gbuf + 3 * static_cast<size_t>(tri);
-	if (v.x != 0.0f)
-		atomicAdd(p, v.x);
-	if (v.y != 0.0f)
-		atomicAdd(p + 1, v.y);
-	if (v.z != 0.0f)
-		atomicAdd(p + 2, v.z);
-}
-
-__device__ __forceinline__ F3 safe_div(F3 a, F3 b) {
-	return f3(b.x > 0.0f ? a.x / b.x : 0.0f, b.y > 0.0f ? a.y / b.y : 0.0f, b.z > 0.0f ? a.z / b.z : 0.0f);
+	add_grad3(kShared ? sbuf + 3 * tri : gbuf + 3 * static_cast<size_t>(tri), v);
 }
 
 struct AdjEntry {
@@ -77,6 +67,8 @@ __device__ __forceinline__ int adjoint_path(const PhysScene &sc, const PhysSetti
 		ShadowReq sr;
 		VertexGrad vg;
 		const bool alive = shade_vertex_t<true>(sc, st, ps, h, sr, &vg);
+		if (h.idx < 0) // an escaping ray gathers the environment (shade_vertex_t's miss term)
+			P = P + ps.beta * f3(st.env[0], st.env[1], st.env[2]);
 		if (vg.hit_emitter >= 0) {
 			P = P + vg.emit;
 			add3<kShared>(d_em, s_em, vg.hit_emitter, g * safe_div(vg.emit, vg.Le));
@@ -111,6 +103,8 @@ __device__ __forceinline__ void adjoint_replay_tail(const PhysScene &sc, const P
 		ShadowReq sr;
 		VertexGrad vg;
 		const bool alive = shade_vertex_t<true>(sc, st, ps, h, sr, &vg);
+		if (h.idx < 0)
+			P = P + ps.beta * f3(st.env[0], st.env[1], st.env[2]);
 		if (vg.hit_emitter >= 0)
 			P = P + vg.emit;
 		if (sr.valid) {

@@ -1,4 +1,5 @@
 // Differentiable-rendering entry points: material updates and the adjoint.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -6,8 +7,56 @@
 #include "render_impl.hpp"
 #include "scene_impl.hpp"
 #include "trace_range.hpp"
+#include "wavefront_host.hpp"
 
 using namespace rnb;
+
+namespace {
+
+// The adjoint as wavefront waves (one job per view): the paths are regenerated and
+// traced once, in waves sorted like rn_pt_render's wavefront, each path keeping its
+// continuation vertices in the pool until its radiance is final.
+rn_status backward_wavefront(rn_scene *scene, const PhysScene &ps, const std::vector<AdjView> &views, float *g_alb,
+                             float *g_em, cudaStream_t cs) {
+	std::vector<WfJob> jobs(views.size());
+	int max_depth = 1, max_spp = 0;
+	long pix = 0;
+	for (size_t v = 0; v < views.size(); v++) {
+		WfJob &j = jobs[v];
+		j.sc = ps;
+		j.cam = views[v].cam;
+		j.st = views[v].st;
+		j.accum = nullptr;
+		j.n_pix = views[v].n_pix;
+		j.spp = views[v].st.spp > 0 ? views[v].st.spp : 0;
+		j.dimg = views[v].dimg;
+		max_depth = std::max(max_depth, j.st.max_depth);
+		max_spp = std::max(max_spp, j.spp);
+		if (j.spp > 0)
+			pix += j.n_pix;
+	}
+	if (max_spp == 0 || pix == 0)
+		return RN_OK;
+	const int entries = std::max(1, max_depth - 1);
+	size_t budget = 0;
+	RNB_CUDA(wf_pool_budget(budget));
+	long spw = static_cast<long>(budget / (wf_adjoint_bytes_per_path(entries) * static_cast<size_t>(pix)));
+	spw = std::min<long>(spw, (1L << 30) / pix);
+	spw = std::max<long>(1, std::min<long>(spw, max_spp));
+	if (!scene->wf_adj)
+		scene->wf_adj.reset(new WfContext());
+	WfContext &wf = *scene->wf_adj;
+	wf.set_frame_io(nullptr, 0, {});
+	wf.set_dynamic(0);
+	wf.set_sort(1);
+	wf.set_adjoint(entries, g_alb, g_em);
+	rn_status r = wf.configure(jobs, max_depth, kOrderReference, static_cast<int>(spw), cs);
+	if (r != RN_OK)
+		return r;
+	return wf.enqueue(scene->d_status.as<int>(), cs);
+}
+
+} // namespace
 
 extern "C" {
 
@@ -109,9 +158,25 @@ rn_status rn_pt_backward(rn_scene *scene, int n_views, const rn_pt_camera *camer
 	RNB_CUDA(cudaMemcpyAsync(d_views, views.data(), views.size() * sizeof(AdjView), cudaMemcpyHostToDevice, cs));
 	RNB_CUDA(cudaMemsetAsync(g_alb, 0, gbytes, cs));
 	RNB_CUDA(cudaMemsetAsync(g_em, 0, gbytes, cs));
-	RNB_CUDA(scene->d_adj_counter.ensure(256));
-	RNB_CUDA(launch_adjoint(ps, d_views, n_views, static_cast<unsigned>(items), g_alb, g_em, n,
-	                        scene->d_adj_counter.as<unsigned>(), scene->d_status.as<int>(), cs));
+	// Integrator: RN_PT_MEGAKERNEL in any view's settings keeps one thread per path,
+	// RN_PT_WAVEFRONT in any view asks for waves; RN_PT_AUTO takes waves above the
+	// triangle count whose gradients the per-path kernel keeps in shared memory.
+	bool want_mk = false, want_wf = false, depth_ok = true;
+	for (int v = 0; v < n_views; v++) {
+		want_mk = want_mk || settings[v].integrator == RN_PT_MEGAKERNEL;
+		want_wf = want_wf || settings[v].integrator == RN_PT_WAVEFRONT;
+		depth_ok = depth_ok && views[v].st.max_depth <= kWfMaxDepth;
+	}
+	const bool use_wf = depth_ok && !want_mk && (want_wf || n > kAdjointSharedTris);
+	if (use_wf) {
+		rn_status r = backward_wavefront(scene, ps, views, g_alb, g_em, cs);
+		if (r != RN_OK)
+			return r;
+	} else {
+		RNB_CUDA(scene->d_adj_counter.ensure(256));
+		RNB_CUDA(launch_adjoint(ps, d_views, n_views, static_cast<unsigned>(items), g_alb, g_em, n,
+		                        scene->d_adj_counter.as<unsigned>(), scene->d_status.as<int>(), cs));
+	}
 	if (dev)
 		return RN_OK;
 	if (d_albedo)

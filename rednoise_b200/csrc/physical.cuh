@@ -199,6 +199,21 @@ struct VertexGrad {
 	F3 cont_dlog;     // d log(continuation weight) / d albedo
 };
 
+// Adjoint helpers shared by the per-path and the wavefront adjoint: a / b per channel
+// where b > 0 (else 0), and a gradient 3-vector added to one triangle's three floats
+// (zero components skipped).
+__device__ __forceinline__ F3 safe_div(F3 a, F3 b) {
+	return f3(b.x > 0.0f ? a.x / b.x : 0.0f, b.y > 0.0f ? a.y / b.y : 0.0f, b.z > 0.0f ? a.z / b.z : 0.0f);
+}
+__device__ __forceinline__ void add_grad3(float *p, F3 v) {
+	if (v.x != 0.0f)
+		atomicAdd(p, v.x);
+	if (v.y != 0.0f)
+		atomicAdd(p + 1, v.y);
+	if (v.z != 0.0f)
+		atomicAdd(p + 2, v.z);
+}
+
 __device__ __forceinline__ float power_mis(float a, float b) {
 	const float a2 = a * a, b2 = b * b;
 	return a2 / (a2 + b2);

@@ -52,6 +52,7 @@ struct rn_scene {
 	rnb::DevBuf d_adj_counter; // work counter of the adjoint kernel
 	// Wavefront pools and the captured frame graph of single-scene renders.
 	std::unique_ptr<rnb::WfContext> wf;
+	std::unique_ptr<rnb::WfContext> wf_adj; // the wavefront adjoint's pools and schedule
 	// Autotuner choices per (width, height, max_depth, order):
 	// (integrator, samples per wave, per-lane ray replacement).
 	std::map<std::tuple<int, int, int, int>, std::tuple<int, int, int, int>> tuned;

@@ -156,6 +156,48 @@ __device__ __forceinline__ unsigned dir_cell(const F3 &d) {
 	return (quantize(0.5f * (py + 1.0f), 16.0f) << 4) | quantize(0.5f * (px + 1.0f), 16.0f);
 }
 
+// Gradient adds of one warp merged per triangle: every lane of `mask` calls this;
+// lanes with `on` set add v to base[3 tri .. 3 tri + 2]. Lanes that share a triangle
+// pass their values through this warp's 96 floats of shared memory (scratch) to the
+// lowest of them, which adds the sum: few emitter and wall triangles take most of the
+// adjoint's terms, and one atomic per triangle and warp keeps them from queueing.
+__device__ __forceinline__ void add_grad3_warp(float *base, int tri, F3 v, bool on, unsigned mask, float *scratch) {
+	const int lane = threadIdx.x & 31;
+	const unsigned act = __ballot_sync(mask, on);
+	if (on) {
+		const unsigned peers = __match_any_sync(act, tri);
+		scratch[lane] = v.x;
+		scratch[32 + lane] = v.y;
+		scratch[64 + lane] = v.z;
+		__syncwarp(act);
+		if (lane == __ffs(peers) - 1) {
+			F3 sum = f3(0.0f, 0.0f, 0.0f);
+			for (unsigned m = peers; m; m &= m - 1) {
+				const int l = __ffs(m) - 1;
+				sum.x += scratch[l];
+				sum.y += scratch[32 + l];
+				sum.z += scratch[64 + l];
+			}
+			add_grad3(base + 3 * static_cast<size_t>(tri), sum);
+		}
+		__syncwarp(act);
+	}
+}
+
+// dL/d(sample radiance) of a path of job `job` through `pixel`: the mean image's
+// gradient over the job's samples per pixel.
+__device__ __forceinline__ F3 adj_weight(const WfJob &job, uint32_t pixel) {
+	const float inv = 1.0f / static_cast<float>(job.st.spp);
+	const float *gi = job.dimg + 3 * static_cast<size_t>(pixel);
+	return f3(gi[0] * inv, gi[1] * inv, gi[2] * inv);
+}
+
+// kAdj: the adjoint wave's shade stage (path replay backpropagation, the same terms
+// in the same arithmetic as the per-path adjoint): the previous vertex's gathered
+// radiance is complete when this stage starts (its next-event term was added by the
+// shadow stage), emission terms go to d_em here, next-event terms are handed to the
+// shadow stage with the record, and a continuing vertex joins the slot's list.
+template <bool kAdj>
 __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
                                                   const int *__restrict__ q, int write_keys, int *status) {
 	const unsigned n = pool.counters[kCntRays + k];
@@ -181,7 +223,22 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 		h.u = h.v = 0.0f;
 		h.rank = 0;
 		ShadowReq sr;
-		const bool alive = shade_vertex(job.sc, job.st, ps, h, sr);
+		VertexGrad vg;
+		F3 g = f3(0.0f, 0.0f, 0.0f);
+		int n_list = 0;
+		if constexpr (kAdj) {
+			g = adj_weight(job, ps.pixel);
+			n_list = pool.adj_n[slot];
+			if (n_list > 0)
+				pool.adj_pt[static_cast<size_t>(n_list - 1) * pool.capacity + slot] = make_float4(L.x, L.y, L.z, 0.0f);
+		}
+		const bool alive = shade_vertex_t<kAdj>(job.sc, job.st, ps, h, sr, kAdj ? &vg : nullptr);
+		if constexpr (kAdj) {
+			__shared__ float agg[4 * 96];
+			const bool em = vg.hit_emitter >= 0;
+			add_grad3_warp(pool.d_em, em ? vg.hit_emitter : 0, em ? g * safe_div(vg.emit, vg.Le) : f3(0.0f, 0.0f, 0.0f),
+			               em, __activemask(), agg + (threadIdx.x >> 5) * 96);
+		}
 		const unsigned si = warp_append(pool.counters + kCntShadow + k, sr.valid);
 		if (kBoundsCheck && sr.valid && si >= static_cast<unsigned>(pool.capacity)) {
 			atomicOr(status, 1);
@@ -195,6 +252,21 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 			pool.sh_o[si] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
 			pool.sh_d[si] = make_float4(sr.d.x, sr.d.y, sr.d.z, __int_as_float(sr.ignore));
 			pool.sh_c[si] = make_float4(sr.contrib.x, sr.contrib.y, sr.contrib.z, __int_as_float(slot));
+			if constexpr (kAdj) {
+				pool.sh_gdlog[si] = make_float4(vg.nee_dlog.x, vg.nee_dlog.y, vg.nee_dlog.z, __int_as_float(vg.tri));
+				pool.sh_gle[si] = make_float4(vg.nee_Le.x, vg.nee_Le.y, vg.nee_Le.z, __int_as_float(vg.nee_emitter));
+			}
+		}
+		if constexpr (kAdj) {
+			if (alive) {
+				if (kBoundsCheck && n_list >= pool.adj_entries) {
+					atomicOr(status, 1);
+				} else {
+					pool.adj_dlog[static_cast<size_t>(n_list) * pool.capacity + slot] =
+					    make_float4(vg.cont_dlog.x, vg.cont_dlog.y, vg.cont_dlog.z, __int_as_float(vg.tri));
+					pool.adj_n[slot] = n_list + 1;
+				}
+			}
 		}
 		const unsigned ni = warp_append(pool.counters + kCntRays + k + 1, alive);
 		pool.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, L.w);
@@ -215,6 +287,8 @@ __global__ void __launch_bounds__(128) k_wf_shade(const WfJob *__restrict__ jobs
 	}
 }
 
+// kAdj: an unoccluded record also adds its next-event terms to d_alb and d_em.
+template <bool kAdj>
 __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ jobs, WfPool pool, int k, int only_job,
                                                    const int *__restrict__ order, int *status) {
 	const unsigned n = pool.counters[kCntShadow + k];
@@ -228,6 +302,10 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 		if (base >= n)
 			break;
 		const unsigned q = base + lane;
+		// kAdj: this lane's next-event gradient terms, added by the whole warp below
+		bool g_on = false;
+		int g_tri = 0, g_em = 0;
+		F3 g_alb_v = f3(0.0f, 0.0f, 0.0f), g_em_v = f3(0.0f, 0.0f, 0.0f);
 		if (q < n) {
 			const unsigned i = order ? static_cast<unsigned>(order[q]) : q;
 			const float4 so = pool.sh_o[i], sd = pool.sh_d[i];
@@ -249,7 +327,23 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 				L.y += sc.y;
 				L.z += sc.z;
 				pool.L[slot] = L;
+				if constexpr (kAdj) {
+					const F3 g = adj_weight(jobs[j], pool.pixel[slot]);
+					const float4 gd = pool.sh_gdlog[i], gl = pool.sh_gle[i];
+					const F3 c = f3(sc.x, sc.y, sc.z);
+					g_on = true;
+					g_tri = __float_as_int(gd.w);
+					g_em = __float_as_int(gl.w);
+					g_alb_v = g * c * f3(gd.x, gd.y, gd.z);
+					g_em_v = g * safe_div(c, f3(gl.x, gl.y, gl.z));
+				}
 			}
+		}
+		if constexpr (kAdj) {
+			__shared__ float agg[4 * 96];
+			float *scratch = agg + (threadIdx.x >> 5) * 96;
+			add_grad3_warp(pool.d_alb, g_tri, g_alb_v, g_on, 0xffffffffu, scratch);
+			add_grad3_warp(pool.d_em, g_em, g_em_v, g_on, 0xffffffffu, scratch);
 		}
 	}
 	if (err)
@@ -514,6 +608,39 @@ cudaError_t bin_sort(const BinSrc &src, unsigned *bins, int grid, int *status, c
 	return cudaGetLastError();
 }
 
+// End of an adjoint wave: each path's radiance C is final, so every listed
+// continuation vertex adds g (C - P) d log w / d albedo to its triangle.
+__global__ void __launch_bounds__(256) k_wf_adj_flush(const WfJob *__restrict__ jobs, WfPool pool, WfWave wave) {
+	__shared__ float agg[8 * 96];
+	float *scratch = agg + (threadIdx.x >> 5) * 96;
+	const int stride = gridDim.x * blockDim.x;
+	// the loop bound is a multiple of the block size, so whole warps run each iteration
+	const int end = (wave.n_slots + blockDim.x - 1) / blockDim.x * blockDim.x;
+	for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < end; slot += stride) {
+		const bool in = slot < wave.n_slots;
+		const int n = in ? pool.adj_n[slot] : 0;
+		F3 C = f3(0.0f, 0.0f, 0.0f), g = C;
+		if (n > 0) {
+			const float4 L = pool.L[slot];
+			C = f3(L.x, L.y, L.z);
+			g = adj_weight(jobs[__float_as_int(L.w)], pool.pixel[slot]);
+		}
+		const int n_warp = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(n));
+		for (int e = 0; e < n_warp; e++) {
+			const bool on = e < n;
+			int tri = 0;
+			F3 v = f3(0.0f, 0.0f, 0.0f);
+			if (on) {
+				const size_t at = static_cast<size_t>(e) * pool.capacity + slot;
+				const float4 P = pool.adj_pt[at], dl = pool.adj_dlog[at];
+				tri = __float_as_int(dl.w);
+				v = g * (C - f3(P.x, P.y, P.z)) * f3(dl.x, dl.y, dl.z);
+			}
+			add_grad3_warp(pool.d_alb, tri, v, on, 0xffffffffu, scratch);
+		}
+	}
+}
+
 // Adds each pixel's samples of this wave to its sum, in sample order.
 __global__ void __launch_bounds__(256) k_wf_accumulate(const WfJob *__restrict__ jobs, WfPool pool, WfWave wave) {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < wave.n_pix; i += gridDim.x * blockDim.x) {
@@ -544,9 +671,17 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 	cudaError_t e = cudaMemsetAsync(pool.counters, 0, kCntTotal * sizeof(unsigned), st);
 	if (e != cudaSuccess)
 		return e;
+	// adjoint waves: every slot's continuation list starts empty; their traversal stages
+	// are the one-ray-per-lane kernels, whose shadow stage adds the next-event terms
+	const bool adj = pool.adj_n != nullptr;
+	if (adj) {
+		e = cudaMemsetAsync(pool.adj_n, 0, static_cast<size_t>(wave.n_slots) * sizeof(int), st);
+		if (e != cudaSuccess)
+			return e;
+	}
 	const int gcam = (wave.n_slots + 255) / 256 < 148 * 8 ? (wave.n_slots + 255) / 256 : 148 * 8;
 	k_wf_camera<<<gcam, 256, 0, st>>>(d_jobs, pool, wave);
-	const bool use_dyn = lc.dyn && order == kOrderReference;
+	const bool use_dyn = lc.dyn && order == kOrderReference && !adj;
 	const bool sort = lc.sort && pool.keys && pool.fine && pool.sorted_coarse && pool.sorted_fine && pool.sorted &&
 	                  pool.bins;
 	for (int k = 0; k < max_depth; k++) {
@@ -572,7 +707,11 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 		// bounce appended each warp's surviving slots in increasing order, so the path
 		// state reads and writes of neighbouring lanes fall on neighbouring slots. The
 		// results do not depend on the order in which paths are shaded.
-		k_wf_shade<<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, pool.queue[k & 1], sort ? 1 : 0, status);
+		if (adj)
+			k_wf_shade<true><<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, pool.queue[k & 1], sort ? 1 : 0, status);
+		else
+			k_wf_shade<false><<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, pool.queue[k & 1], sort ? 1 : 0,
+			                                                 status);
 		if (use_dyn)
 			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, oj, status);
 		else {
@@ -589,9 +728,16 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 				                                            pool.sh_sorted, static_cast<unsigned>(pool.capacity),
 				                                            status);
 			}
-			k_wf_shadow<<<lc.grid_sh, 128, kWfShadowSmem, st>>>(d_jobs, pool, k, oj, sort_sh ? pool.sh_sorted : nullptr,
-			                                                    status);
+			const int *order_sh = sort_sh ? pool.sh_sorted : nullptr;
+			if (adj)
+				k_wf_shadow<true><<<lc.grid_sh, 128, kWfShadowSmem, st>>>(d_jobs, pool, k, oj, order_sh, status);
+			else
+				k_wf_shadow<false><<<lc.grid_sh, 128, kWfShadowSmem, st>>>(d_jobs, pool, k, oj, order_sh, status);
 		}
+	}
+	if (adj) {
+		k_wf_adj_flush<<<gcam, 256, 0, st>>>(d_jobs, pool, wave);
+		return cudaGetLastError();
 	}
 	const int gacc = (wave.n_pix + 255) / 256 < 148 * 8 ? (wave.n_pix + 255) / 256 : 148 * 8;
 	k_wf_accumulate<<<gacc, 256, 0, st>>>(d_jobs, pool, wave);
@@ -605,8 +751,8 @@ void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn, 
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	int a = 0, b = 0, c = 0, d0 = 0, d1 = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_wf_extend<kOrderReference>, 128, kWfExtendSmem);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_wf_shade, 128, 0);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_wf_shadow, 128, kWfShadowSmem);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_wf_shade<false>, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_wf_shadow<false>, 128, kWfShadowSmem);
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d0, k_wf_trace_dyn<false>, 128, 0);
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d1, k_wf_trace_dyn<true>, 128, 0);
 	grid_ext = sms * (a > 0 ? a : 1);

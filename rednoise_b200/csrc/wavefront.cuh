@@ -26,9 +26,10 @@ struct WfJob {
 	PhysScene sc;
 	PhysCamera cam;
 	PhysSettings st;
-	float *accum; // 3 floats per pixel (sums)
+	float *accum; // 3 floats per pixel (sums); unused by adjoint waves
 	int n_pix;
 	int spp;
+	const float *dimg = nullptr; // adjoint waves: dL/d(mean image), 3 floats per pixel
 };
 
 // Pools of `capacity` path slots.
@@ -70,6 +71,22 @@ struct WfPool {
 	uint16_t *sh_keys;
 	uint8_t *sh_fine;
 	int *sh_sorted;
+	// Adjoint waves only (null otherwise; path replay backpropagation). Per slot, the
+	// list of its continuation vertices, entry e of slot s at e * capacity + s:
+	// adj_pt = radiance gathered up to and including the vertex (written by the
+	// next shade stage, when the vertex's next-event term is in), adj_dlog = d log
+	// (continuation weight) / d albedo .xyz and the vertex's triangle (int bits);
+	// adj_n = entries per slot. Per shadow record, sh_gdlog = d log f(light) / d albedo
+	// .xyz and the scattering triangle, sh_gle = the sampled emitter's radiance .xyz
+	// and the emitter triangle. d_alb / d_em: the gradients (3 floats per triangle).
+	float4 *adj_pt;
+	float4 *adj_dlog;
+	int *adj_n;
+	float4 *sh_gdlog;
+	float4 *sh_gle;
+	float *d_alb;
+	float *d_em;
+	int adj_entries; // list entries per slot (>= max_depth - 1)
 	int capacity;
 };
 

@@ -78,6 +78,31 @@ rn_status WfContext::ensure_pool(int capacity) {
 	return RN_OK;
 }
 
+rn_status WfContext::ensure_adjoint() {
+	pool_.adj_pt = pool_.adj_dlog = pool_.sh_gdlog = pool_.sh_gle = nullptr;
+	pool_.adj_n = nullptr;
+	pool_.adj_entries = 0;
+	pool_.d_alb = pool_.d_em = nullptr;
+	if (adj_entries_ <= 0)
+		return RN_OK;
+	const size_t n = static_cast<size_t>(capacity_);
+	const size_t m = n * static_cast<size_t>(adj_entries_);
+	RNB_CUDA(adj_pt_.ensure(m * 16));
+	RNB_CUDA(adj_dlog_.ensure(m * 16));
+	RNB_CUDA(adj_n_.ensure(n * 4));
+	RNB_CUDA(sh_gdlog_.ensure(n * 16));
+	RNB_CUDA(sh_gle_.ensure(n * 16));
+	pool_.adj_pt = adj_pt_.as<float4>();
+	pool_.adj_dlog = adj_dlog_.as<float4>();
+	pool_.adj_n = adj_n_.as<int>();
+	pool_.sh_gdlog = sh_gdlog_.as<float4>();
+	pool_.sh_gle = sh_gle_.as<float4>();
+	pool_.adj_entries = adj_entries_;
+	pool_.d_alb = d_alb_;
+	pool_.d_em = d_em_;
+	return RN_OK;
+}
+
 rn_status WfContext::configure(const std::vector<WfJob> &jobs, int max_depth, int order, int spw,
                                cudaStream_t st) {
 	if (jobs.empty() || max_depth < 1 || max_depth > kWfMaxDepth || spw < 1) {
@@ -137,6 +162,9 @@ rn_status WfContext::configure(const std::vector<WfJob> &jobs, int max_depth, in
 		capacity = std::max(capacity, base);
 	}
 	rn_status r = ensure_pool(static_cast<int>(capacity));
+	if (r != RN_OK)
+		return r;
+	r = ensure_adjoint();
 	if (r != RN_OK)
 		return r;
 	if (grid_ext_ == 0)

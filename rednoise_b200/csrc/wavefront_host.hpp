@@ -28,6 +28,11 @@ inline int default_samples_per_wave(long n_pix, int spp) {
 // key, the first-level sorted queue with its fine keys, shadow record with the two
 // parts of its key and its sorted position.
 constexpr size_t kWfBytesPerPath = 4 * 16 + 4 * 4 + 3 * 4 + 2 + 1 + 4 + 1 + 3 * 16 + 2 + 1 + 4;
+// Adjoint waves add per slot: the list (32 B per entry), its length and the shadow
+// record's two gradient float4s.
+inline size_t wf_adjoint_bytes_per_path(int list_entries) {
+	return kWfBytesPerPath + 32 * static_cast<size_t>(list_entries) + 4 + 32;
+}
 
 // Memory the autotuners let a path pool take: half the free device memory, at most 32 GiB.
 inline cudaError_t wf_pool_budget(size_t &budget) {
@@ -72,15 +77,28 @@ public:
 		sort_ = sort;
 	}
 	int sort() const { return sort_; }
+	// Adjoint waves (path replay backpropagation): list_entries continuation vertices
+	// per path (max_depth - 1 suffice), gradients added to d_alb / d_em (device, 3 floats
+	// per triangle). Takes effect at the next configure; run them with enqueue.
+	void set_adjoint(int list_entries, float *d_alb, float *d_em) {
+		release_graph();
+		adj_entries_ = list_entries;
+		d_alb_ = d_alb;
+		d_em_ = d_em;
+	}
 
 private:
 	rn_status ensure_pool(int capacity);
+	rn_status ensure_adjoint();
 	void release_graph();
 
 	DevBuf o_, d_, beta_, L_, pixel_, sample_, hit_idx_, hit_t_, q0_, q1_, sh_o_, sh_d_, sh_c_, counters_;
 	DevBuf keys_, fine_, sorted_coarse_, sorted_fine_, sorted_, bins_, sh_keys_, sh_fine_, sh_sorted_;
+	DevBuf adj_pt_, adj_dlog_, adj_n_, sh_gdlog_, sh_gle_;
 	DevBuf d_jobs_, d_wave_tab_;
 	WfPool pool_{};
+	int adj_entries_ = 0;
+	float *d_alb_ = nullptr, *d_em_ = nullptr;
 	int capacity_ = 0;
 	int max_depth_ = 0;
 	int order_ = 0;

@@ -177,3 +177,86 @@ def test_inverse_rendering_recovers_albedo():
     err1 = np.abs(alb[moved] - truth[moved]).mean()
     assert err1 < 0.8 * err0, (err0, err1)
     assert np.mean(losses[-10:]) < np.mean(losses[:5])
+
+
+def _with_integrator(v, integrator, **kw):
+    st = v[1]
+    fields = dict(spp=st.spp, max_depth=st.max_depth, rr_depth=st.rr_depth, seed=st.seed,
+                  sample_offset=st.sample_offset, env=tuple(st.env))
+    fields.update(kw)
+    return v[0], rn.Settings.make(integrator=integrator, **fields)
+
+
+def _grads_agree(a, b):
+    """The two schedules add the same terms in different orders (float atomics)."""
+    tol = 1e-4 * np.abs(b).max() + 1e-3 * np.abs(b)
+    bad = np.abs(a - b) > tol
+    assert bad.mean() < 1e-3 and np.abs(a - b).max() <= 1e-3 * np.abs(b).max() + 1e-12, (bad.sum(), np.abs(a - b).max())
+
+
+@pytest.mark.parametrize("env", [(0.0, 0.0, 0.0), (0.3, 0.5, 0.8)])
+def test_wavefront_adjoint_matches_per_path_adjoint(setup, env):
+    """Waves of binned paths (RN_PT_WAVEFRONT) and one thread per path
+    (RN_PT_MEGAKERNEL) replay the same paths and add the same terms: albedo and
+    emission gradients agree up to the order of the float additions. With an
+    environment, escaping rays' radiance enters the continuation terms of both."""
+    sc, target, v = setup
+    s = make_scene(sc)
+    rng = np.random.default_rng(4)
+    dI = rng.normal(size=(36, 48, 3)).astype(np.float32)
+    a_mk, e_mk = s.backward([_with_integrator(v, 1, env=env, rr_depth=3)], [dI])
+    a_wf, e_wf = s.backward([_with_integrator(v, 2, env=env, rr_depth=3)], [dI])
+    assert np.abs(a_mk).max() > 0 and np.abs(e_mk).max() > 0
+    _grads_agree(a_wf, a_mk)
+    _grads_agree(e_wf, e_mk)
+
+
+def test_environment_gradient_matches_central_differences(setup):
+    """Escaping rays gather the environment: the albedo gradient of both schedules
+    follows central differences of the same fixed-sample estimator."""
+    sc, target, v = setup
+    env = (0.3, 0.5, 0.8)
+    s = make_scene(sc)
+    views = {k: _with_integrator(v, k, env=env) for k in (1, 2)}
+    img0 = s.render_physical(views[1][0], views[1][1]).astype(np.float64)
+    dI = (2 * (img0 - target)).astype(np.float32)
+    grads = {k: s.backward([views[k]], [dI])[0] for k in (1, 2)}
+    rng = np.random.default_rng(6)
+    eps = 1e-3
+    errs = {1: [], 2: []}
+    for _ in range(16):
+        tri, ch = int(rng.integers(0, 34)), int(rng.integers(0, 3))
+        alb = sc["albedo"].copy()
+        alb[tri, ch] += eps
+        s.set_materials(albedo=alb)
+        Lp = ((s.render_physical(views[1][0], views[1][1]).astype(np.float64) - target) ** 2).sum()
+        alb[tri, ch] -= 2 * eps
+        s.set_materials(albedo=alb)
+        Lm = ((s.render_physical(views[1][0], views[1][1]).astype(np.float64) - target) ** 2).sum()
+        s.set_materials(albedo=sc["albedo"])
+        fd = (Lp - Lm) / (2 * eps)
+        if abs(fd) > 1e-7:
+            for k in (1, 2):
+                errs[k].append(abs(fd - grads[k][tri, ch]) / abs(fd))
+    for k in (1, 2):
+        assert len(errs[k]) >= 6
+        assert np.median(errs[k]) < 0.02 and max(errs[k]) < 0.1, (k, errs[k])
+
+
+def test_wavefront_adjoint_multi_view_and_large_scene():
+    """Two views of different sizes and sample counts in one wave schedule, on a
+    scene above the shared-memory limit (RN_PT_AUTO takes waves there): the same
+    gradients as the per-path adjoint."""
+    sc = scenes.icosphere_scene(level=4)
+    assert len(sc["vertices"]) > 4096
+    s = make_scene(sc)
+    va = view(40, 30, seed=5, spp=8, depth=6)
+    vb = view(24, 20, seed=7, spp=12, depth=5)
+    rng = np.random.default_rng(8)
+    ga = rng.normal(size=(30, 40, 3)).astype(np.float32)
+    gb = rng.normal(size=(20, 24, 3)).astype(np.float32)
+    a_mk, e_mk = s.backward([_with_integrator(va, 1, rr_depth=3), _with_integrator(vb, 1, rr_depth=3)], [ga, gb])
+    a_auto, e_auto = s.backward([_with_integrator(va, 0, rr_depth=3), _with_integrator(vb, 0, rr_depth=3)], [ga, gb])
+    assert np.abs(a_mk).max() > 0
+    _grads_agree(a_auto, a_mk)
+    _grads_agree(e_auto, e_mk)
