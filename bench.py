@@ -552,7 +552,7 @@ def run_ours(args):
                      "algorithmic": "24 B per node-box test + 36 B per triangle test of the reference-order "
                                     "traversal, counted on the GPU for 1 spp of the same frame",
                      "kernel_ms": kernel_ms,
-                     "scope": "whole frame: the closest-hit and shadow traversal kernels are 83 % of its device "
+                     "scope": "whole frame: the closest-hit and shadow traversal kernels are 84 % of its device "
                               "time (ncu launch list); traffic scaled from a 480x270 capture"},
         "clocks": clk,
         "rmse_vs_fp64_64spp": rmse,
