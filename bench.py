@@ -284,6 +284,73 @@ def gradient_timing(scene, lib, stream, sptr, l2, size=512, spp=32, depth=6) -> 
             "grad_nonzero": int((g_alb != 0).sum().item())}
 
 
+def time_to_rmse(scene, lib, stream, sptr, cam, args, fp64, W, H, target=0.5, frame_spp=64, max_frames=32):
+    """Time for each integrator to bring the frame's relative RMSE against the FP64
+    65536-spp reference (its seeded 512-pixel subset) below `target`: 64-spp frames of
+    consecutive sample indices are accumulated (rn_pt_render_accumulate) until the
+    running mean reaches the target. Both integrators render the same samples to the
+    same floats, so they need the same number of frames; the time is the sum of the
+    frames' device times (CUDA events; the RMSE check between frames is not timed).
+    Also the relative RMSE of single 64-spp frames over 8 sample blocks: a few
+    subset pixels see rare, bright caustic paths (light reaching the emitter-lit
+    surfaces through the dielectric triangles), so one 64-spp block's error depends
+    on whether such a path was drawn."""
+    import torch
+
+    import rednoise_b200 as rn
+    from rednoise_b200 import _native
+
+    px = torch.as_tensor(fp64["c2_pixels"].astype(np.int64), device="cuda")
+    mref = torch.as_tensor(fp64["c2_mean"], device="cuda", dtype=torch.float64)
+    ref_norm = float(torch.sqrt((mref ** 2).mean()))
+    acc = torch.zeros(H * W * 3, dtype=torch.float32, device="cuda")
+    base = 1 << 24  # sample indices not used by the timed frames
+
+    def rel_rmse(mean_flat):
+        m = mean_flat.view(-1, 3)[px].to(torch.float64)
+        return float(torch.sqrt(((m - mref) ** 2).mean())) / ref_norm
+
+    def frame(code, k):
+        st = rn.Settings.make(spp=frame_spp, max_depth=args.depth, rr_depth=args.rr, integrator=code, seed=1,
+                              sample_offset=base + k * frame_spp)
+        _native.check(lib.rn_pt_render_accumulate(scene.handle, ctypes.byref(cam), ctypes.byref(st),
+                                                  _native.RN_PT_DEVICE_POINTERS, sptr,
+                                                  ctypes.c_void_p(acc.data_ptr())), "rn_pt_render_accumulate")
+
+    out = {"target_relative_rmse": target, "frame_spp": frame_spp,
+           "reference": "FP64 oracle estimator, 65536 spp, 512 seeded pixels (tests/golden/fp64_ref.npz)"}
+    with torch.cuda.stream(stream):
+        blocks = []
+        for b in range(8):
+            acc.zero_()
+            frame(_native.RN_PT_AUTO, 1000 + b)
+            torch.cuda.synchronize()
+            blocks.append(rel_rmse(acc / frame_spp))
+        out["single_64spp_frame_relative_rmse"] = {"min": min(blocks), "median": float(np.median(blocks)),
+                                                   "max": max(blocks)}
+        for name, code in (("wavefront", _native.RN_PT_AUTO), ("megakernel", _native.RN_PT_MEGAKERNEL)):
+            acc.zero_()
+            frame(code, 999)  # warm-up (graph capture of the accumulate path), not counted
+            acc.zero_()
+            ms, err, k = 0.0, None, 0
+            while k < max_frames:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                frame(code, k)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
+                k += 1
+                err = rel_rmse(acc / (k * frame_spp))
+                if err < target:
+                    break
+            out[name] = {"frames": k, "spp": k * frame_spp, "seconds": ms / 1e3, "relative_rmse": err,
+                         "reached": err < target,
+                         "samples_per_s_at_target": W * H * k * frame_spp / (ms / 1e3)}
+    out["wavefront_speedup_at_target"] = out["megakernel"]["seconds"] / out["wavefront"]["seconds"]
+    return out
+
+
 def run_reference_arm(args):
     rank, _, world = dist_env()
     if rank != 0:
@@ -320,6 +387,51 @@ def measured_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def read_peaks(lib, stream, sptr) -> dict:
+    """Read bandwidths measured on this GPU in this run (rn_pt_probe_read, CUDA events):
+    an L2-resident read (16-64 MB buffers, loads that bypass L1; the best size) and an
+    HBM read (a 2 GB buffer)."""
+    import torch
+
+    from rednoise_b200 import _native
+
+    out = {}
+    best = 0.0
+    for mb in (16, 32, 64):
+        buf = torch.empty(mb << 20, dtype=torch.uint8, device="cuda")
+        buf.zero_()
+        torch.cuda.synchronize()
+        ms = ctypes.c_float(0.0)
+        n = 200
+        _native.check(lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr()), buf.numel(), n, 1, sptr,
+                                           ctypes.byref(ms)), "rn_pt_probe_read")
+        gbs = buf.numel() * n / (ms.value / 1e3) / 1e9
+        out[f"l2_read_{mb}MB_gbs"] = gbs
+        best = max(best, gbs)
+        del buf
+    out["l2_read_gbs"] = best
+    big = torch.empty(2 << 30, dtype=torch.uint8, device="cuda")
+    big.zero_()
+    torch.cuda.synchronize()
+    ms = ctypes.c_float(0.0)
+    _native.check(lib.rn_pt_probe_read(ctypes.c_void_p(big.data_ptr()), big.numel(), 5, 1, sptr, ctypes.byref(ms)),
+                  "rn_pt_probe_read")
+    out["hbm_read_gbs"] = big.numel() * 5 / (ms.value / 1e3) / 1e9
+    del big
+    torch.cuda.empty_cache()
+    return out
+
+
+def kernel_profile():
+    """ncu figures of the traversal kernels (instructions, lanes per instruction, issue
+    activity, DRAM bytes per sample of the frame), committed under profiles/."""
+    path = os.path.join(ROOT, "profiles", "traversal_kernels.json")
+    if not os.path.isfile(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
 
 
 def profiled_traffic():
@@ -523,6 +635,19 @@ def run_ours(args):
                                                                 for k in rmse_by},
                    "wavefront_speedup_at_equal_rmse": compare["wavefront"] / compare["megakernel"]}
 
+    # Per-stage device times of the same frame, launched kernel by kernel with CUDA
+    # events between the stages (the timed frames above replay the captured graph).
+    st_prof = rn.Settings.make(spp=spp, max_depth=args.depth, rr_depth=args.rr, integrator=integ, seed=1,
+                               sample_offset=same.sample_offset)
+    with torch.cuda.stream(stream):
+        l2.zero_()
+        torch.cuda.synchronize()
+        _, stages = scene.profile_wavefront(cam, st_prof)
+    peaks = read_peaks(lib, stream, sptr)
+    t_rmse = None
+    if fp64 is not None:
+        t_rmse = time_to_rmse(scene, lib, stream, sptr, cam, args, fp64, W, H)
+
     grad = None
     if not args.no_grad:
         grad = gradient_timing(scene, lib, stream, sptr, l2)
@@ -535,6 +660,27 @@ def run_ours(args):
     traffic = None
     if tr and tr.get("bytes_per_sample"):
         traffic = tr["bytes_per_sample"] * samples_per_step
+    # Traversal kernels against the level that holds their working set (the 4-wide tree
+    # and the triangles, ~150 MB, mostly L1/L2-resident): algorithmic bytes of the
+    # reference traversal per stage over the stage's device time.
+    ext_bps = (24.0 * counts["closest_boxes"] + 36.0 * counts["closest_tris"]) / counts["samples"]
+    sh_bps = (24.0 * counts["any_boxes"] + 36.0 * counts["any_tris"]) / counts["samples"]
+    kp = kernel_profile() or {}
+    per_kernel = {}
+    for name, bps, ms_key in (("k_wf_extend", ext_bps, "extend_ms"), ("k_wf_shadow", sh_bps, "shadow_ms")):
+        ms = stages[ms_key]
+        gbs = bps * samples_per_step / (ms / 1e3) / 1e9 if ms > 0 else None
+        ent = {"ms_per_frame": ms, "launches_per_frame": args.depth, "share_of_frame": ms / stages["total_ms"],
+               "algorithmic_bytes_per_sample": bps, "achieved_gbs": gbs,
+               "frac_of_l2_read": gbs / peaks["l2_read_gbs"] if gbs else None,
+               "frac_of_hbm": gbs / peak if gbs else None}
+        if name in kp:
+            ent["ncu"] = kp[name]
+        per_kernel[name] = ent
+    top = per_kernel["k_wf_extend"]
+    top_traffic = None
+    if "k_wf_extend" in kp and kp["k_wf_extend"].get("dram_bytes_per_sample"):
+        top_traffic = kp["k_wf_extend"]["dram_bytes_per_sample"] * samples_per_step / args.depth
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -546,14 +692,22 @@ def run_ours(args):
         "gpu_launches": launches_per_step * args.steps,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ctypes.sizeof(cam) + ctypes.sizeof(st),
                 "d2h_bytes_per_step": H * W * 3 * 4, "api": "rn_pt_render with host output buffer"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": traffic,
-                     "bytes_per_sample": bytes_per_sample,
+        "roofline": {"bound": "l2", "kernel": "k_wf_extend", "achieved": top["achieved_gbs"],
+                     "peak": peaks["l2_read_gbs"], "unit": "GB/s", "frac": top["frac_of_l2_read"],
+                     "peak_kind": "measured in this run: L2-resident read (rn_pt_probe_read, loads bypassing L1)",
+                     "traffic": top_traffic,
                      "algorithmic": "24 B per node-box test + 36 B per triangle test of the reference-order "
-                                    "traversal, counted on the GPU for 1 spp of the same frame",
-                     "kernel_ms": kernel_ms,
-                     "scope": "whole frame: the closest-hit and shadow traversal kernels are 84 % of its device "
-                              "time (ncu launch list); traffic scaled from a 480x270 capture"},
+                                    "closest-hit traversal, counted on the GPU for 1 spp of the same frame",
+                     "kernel_ms_per_launch": top["ms_per_frame"] / args.depth,
+                     "hbm": {"peak": peak, "peak_kind": peak_kind, "frac": top["frac_of_hbm"],
+                             "read_probe_gbs": peaks["hbm_read_gbs"]},
+                     "per_kernel": per_kernel,
+                     "stages_ms": stages,
+                     "frame": {"achieved": achieved, "bytes_per_sample": bytes_per_sample, "kernel_ms": kernel_ms,
+                               "frac_of_l2_read": achieved / peaks["l2_read_gbs"], "frac_of_hbm": achieved / peak,
+                               "dram_traffic": traffic},
+                     "probes": peaks},
+        "time_to_rmse": t_rmse,
         "clocks": clk,
         "rmse_vs_fp64_64spp": rmse,
         "at_equal_rmse": at_rmse,
@@ -563,9 +717,22 @@ def run_ours(args):
         "integrators_samples_per_s": compare,
         "scene_build_ms": info["build_ms"],
     }
+    line["config"]["reference_semantics"] = (
+        "the reference arm (bench.py --impl reference) and cpu_baseline time the reference's renderPathTraced, "
+        "which runs the reference's estimator (depth 4, the default disk light with 9 shadow rays per diffuse "
+        "vertex, 8-bit canvas) on this geometry and camera; this line's value runs the physical estimator "
+        "(depth 8, emitter next-event estimation, Russian roulette). Like for like: reference_semantics_gpu "
+        "(the drop-in rn_render path tracer on the same frame) against cpu_baseline, in like_for_like")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sc)
         line["cpu_physical_fp32"] = cpu_physical_baseline(sc, c, args)
+        line["like_for_like"] = {
+            "reference_semantics": {"gpu_samples_per_s": like_for_like["value"],
+                                    "reference_cpu_samples_per_s": line["cpu_baseline"]["value"],
+                                    "speedup": like_for_like["value"] / line["cpu_baseline"]["value"]},
+            "physical_estimator": {"gpu_samples_per_s": value,
+                                   "oracle_fp32_cpu_samples_per_s": line["cpu_physical_fp32"]["value"],
+                                   "speedup": value / line["cpu_physical_fp32"]["value"]}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -313,10 +313,13 @@ rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, c
  * each GPU) and writes the mean radiance to rgb, a DEVICE pointer of
  * width*height*3 floats, asynchronously on stream (NULL: the scene's stream).
  * The scene must be prepared (rn_pt_scene_prepare) and its device current.
- * Larger images return RN_ERR_CAPACITY. The first call on a device looks up the
- * array's address; make it before any stream capture. All calls share the array:
- * calls whose GPU work overlaps race and must be serialised by the caller. A
- * traversal error is reported by the scene's next synchronising call. */
+ * Larger images return RN_ERR_CAPACITY; an rgb that is not device or managed
+ * memory of the scene's GPU returns RN_ERR_INVALID_ARGUMENT, both before any GPU
+ * work. The first call on a device looks up the array's address and keeps it;
+ * make it before any stream capture, and do not call this after cudaDeviceReset
+ * of that device. All calls share the array: calls whose GPU work overlaps race
+ * and must be serialised by the caller. A traversal error is reported by the
+ * scene's next synchronising call. */
 rn_status rn_pt_render_static(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
                               unsigned flags, void *stream, float *rgb);
 
@@ -340,6 +343,46 @@ typedef struct {
  * image size. `out` may be NULL. */
 rn_status rn_pt_autotune(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings, unsigned flags,
                          rn_pt_tuning *out);
+
+/* ---- profiling ---- */
+
+/* Device time of each stage kind of one wavefront frame, summed over the frame's
+ * bounces and waves (milliseconds), from CUDA events recorded between the stages. */
+typedef struct {
+	double camera_ms;      /* camera rays */
+	double ray_sort_ms;    /* counting sorts of the closest-hit queues */
+	double extend_ms;      /* closest hits */
+	double shade_ms;       /* shading, next-event records, continuations */
+	double shadow_sort_ms; /* counting sorts of the shadow records */
+	double shadow_ms;      /* any hits of the shadow records */
+	double accumulate_ms;  /* per-pixel sums and the resolve to the mean image */
+	double total_ms;       /* the whole frame */
+	int launches;          /* kernels launched */
+	int waves;             /* waves of the frame */
+	int samples_per_wave;  /* the wavefront configuration that ran */
+	int dynamic_fetch;
+	int ray_sort;
+} rn_pt_stage_times;
+
+/* One frame of rn_pt_render through the wavefront integrator, with the
+ * configuration an RN_PT_AUTO render of these settings would use when its tuned
+ * choice is the wavefront (else the wavefront's defaults; RN_PT_RAY_SORT /
+ * RN_PT_NO_RAY_SORT / RN_PT_WAVEFRONT_STATIC in flags apply as for rn_pt_render),
+ * launched kernel by kernel instead of from the captured frame graph with an
+ * event after every stage, so each stage's device time can be measured. rgb
+ * receives the mean image (a device pointer when flags has RN_PT_DEVICE_POINTERS,
+ * else host memory); it equals rn_pt_render's. Synchronises the stream. A
+ * profiling aid with no counterpart in the reference. */
+rn_status rn_pt_profile_wavefront(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
+                                  unsigned flags, void *stream, float *rgb, rn_pt_stage_times *out);
+
+/* Read the device buffer buf (bytes, 16-byte aligned) once per launch, `launches`
+ * times, with 16-byte loads from a persistent grid, after one untimed launch, and
+ * write the device time of the timed launches to *ms (bandwidth = bytes * launches
+ * / ms). l2_only: the loads bypass L1, so a buffer well under the L2's size gives
+ * the L2 read bandwidth and one far above it the HBM read bandwidth. Synchronises
+ * the stream. A roofline probe with no counterpart in the reference. */
+rn_status rn_pt_probe_read(const void *buf, size_t bytes, int launches, int l2_only, void *stream, float *ms);
 
 /* ---- differentiable rendering ---- */
 

@@ -100,6 +100,7 @@ def orc() -> ctypes.CDLL:
                                        vp, vp]),
             "orc_bsdf_eval": (None, [ci, vp, ctypes.c_double, vp, vp, ci, vp, vp, vp, vp]),
             "orc_bsdf_sample": (None, [ci, vp, ctypes.c_double, vp, vp, ci, vp, vp, vp, vp, vp]),
+            "orc_sincos_turn": (None, [ci, vp, vp, vp]),
             "orc_bdpt_render": (None, [vp, vp, vp, ci, ci, ci, ci, cf, vp, vp, ci, cf, ci, ctypes.c_ulonglong, ci,
                                        vp, vp]),
             "orc_mlt_render": (None, [vp, vp, vp, ci, ci, cf, vp, vp, ctypes.c_longlong, ci, ci, ctypes.c_ulonglong,
@@ -319,6 +320,15 @@ def bsdf_sample(mat, albedo, param, ng, wo, u):
     ok = np.zeros(k, np.int32)
     orc().orc_bsdf_sample(int(mat), P(a), float(param), P(n), P(o), k, P(u), P(wi), P(w), P(pdf), P(ok))
     return wi, w, pdf, ok.astype(bool)
+
+
+def sincos_turn(u):
+    """The FP32 estimator's (sin(2 pi u), cos(2 pi u)) for float32 u in [0, 1)."""
+    u = np.ascontiguousarray(u, np.float32).reshape(-1)
+    s = np.zeros_like(u)
+    c = np.zeros_like(u)
+    orc().orc_sincos_turn(u.size, P(u), P(s), P(c))
+    return s, c
 
 
 class OrcBvh:

@@ -736,6 +736,37 @@ template <typename T> X3<T> sdiv(X3<T> a, X3<T> b) {
 	return x3<T>(b.x > 0 ? a.x / b.x : T(0), b.y > 0 ? a.y / b.y : T(0), b.z > 0 ? a.z / b.z : T(0));
 }
 
+// sin(2 pi u), cos(2 pi u). In double: the C library's. In float: the product's
+// quarter-turn reduction and Taylor polynomials (rednoise_b200/csrc/physical.cuh,
+// sincos_turn), restated operation by operation so that the FP32 estimator draws the
+// same directions bit for bit: u * 4 and the removal of its integer part are exact,
+// x = f * pi/2 with |x| <= pi/4, sin to x^11 and cos to x^12 by Horner's rule.
+inline void sincos_turn_t(double u, double &s, double &c) {
+	const double a = 6.28318530717958647692 * u;
+	s = std::sin(a);
+	c = std::cos(a);
+}
+inline void sincos_turn_t(float u, float &s, float &c) {
+	const float t = u * 4.0f;
+	int q = static_cast<int>(t);
+	float f = t - static_cast<float>(q);
+	if (f > 0.5f) {
+		f = f - 1.0f;
+		q = q + 1;
+	}
+	const float x = f * 1.57079632679489662f;
+	const float x2 = x * x;
+	const float c11 = -2.50521083854417188e-8f, c9 = 2.75573192239858907e-6f, c7 = -1.98412698412698413e-4f;
+	const float c5 = 8.33333333333333333e-3f, c3 = -1.66666666666666667e-1f;
+	const float sp = x + x * x2 * (c3 + x2 * (c5 + x2 * (c7 + x2 * (c9 + x2 * c11))));
+	const float d12 = 2.08767569878680990e-9f, d10 = -2.75573192239858907e-7f, d8 = 2.48015873015873016e-5f;
+	const float d6 = -1.38888888888888889e-3f, d4 = 4.16666666666666667e-2f, d2 = -0.5f;
+	const float cp = 1.0f + x2 * (d2 + x2 * (d4 + x2 * (d6 + x2 * (d8 + x2 * (d10 + x2 * d12)))));
+	const int k = q & 3;
+	s = k == 0 ? sp : k == 1 ? cp : k == 2 ? -sp : -cp;
+	c = k == 0 ? cp : k == 1 ? -sp : k == 2 ? -cp : sp;
+}
+
 // Continuation sampling of the physical estimator: Lambert (cosine), GGX (visible
 // normals, Heitz 2018) or smooth dielectric (Fresnel choice). wi, weight = f cos /
 // pdf, pdf (0 for the delta dielectric) and d log(weight) / d albedo; false when the
@@ -743,16 +774,16 @@ template <typename T> X3<T> sdiv(X3<T> a, X3<T> b) {
 template <typename T>
 bool sample_t(int mat, X3<T> alb, T param, X3<T> n, X3<T> wo, X3<T> d, T cog, T u1, T u2, T uf, X3<T> &wi,
               X3<T> &weight, T &pdf, X3<T> &cont_dlog) {
-	const T two_pi = T(6.28318530717958647692);
 	cont_dlog = x3<T>(0, 0, 0);
 	pdf = 0;
 	if (mat == 0) {
 		T r = std::sqrt(u1);
-		T ph = two_pi * u2;
+		T sn, cs;
+		sincos_turn_t(u2, sn, cs);
 		X3<T> t, bt;
 		onb_t(n, t, bt);
 		T z = std::sqrt(std::max(T(0), 1 - u1));
-		wi = t * (r * std::cos(ph)) + bt * (r * std::sin(ph)) + n * z;
+		wi = t * (r * cs) + bt * (r * sn) + n * z;
 		T ci = dt(wi, n);
 		if (ci <= 0)
 			return false;
@@ -769,8 +800,9 @@ bool sample_t(int mat, X3<T> alb, T param, X3<T> n, X3<T> wo, X3<T> d, T cog, T 
 		X3<T> T1 = lensq > 0 ? x3<T>(-vh.y, vh.x, 0) * (T(1) / std::sqrt(lensq)) : x3<T>(1, 0, 0);
 		X3<T> T2 = cr(vh, T1);
 		T r = std::sqrt(u1);
-		T ph = two_pi * u2;
-		T t1 = r * std::cos(ph), t2 = r * std::sin(ph);
+		T sn, cs;
+		sincos_turn_t(u2, sn, cs);
+		T t1 = r * cs, t2 = r * sn;
 		T sb = T(0.5) * (1 + vh.z);
 		t2 = (1 - sb) * std::sqrt(std::max(T(0), 1 - t1 * t1)) + sb * t2;
 		X3<T> nh = T1 * t1 + T2 * t2 + vh * std::sqrt(std::max(T(0), 1 - t1 * t1 - t2 * t2));
@@ -1737,6 +1769,12 @@ void orc_bsdf_eval(int mat, const double *alb3, double param, const double *ng3,
 		fc3[3 * i + 2] = fc.z;
 		pdf[i] = p;
 	}
+}
+
+// The FP32 estimator's sin(2 pi u), cos(2 pi u) on count uniforms (accuracy checks).
+void orc_sincos_turn(int count, const float *u, float *s, float *c) {
+	for (int i = 0; i < count; i++)
+		sincos_turn_t(u[i], s[i], c[i]);
 }
 
 // count samples from uniforms u (3 per sample: the two direction uniforms and the

@@ -532,6 +532,20 @@ class Scene:
                       "rn_pt_render_accumulate")
         return accum
 
+    def profile_wavefront(self, camera: "Camera", settings: "Settings", ray_sort: Optional[bool] = None,
+                          wavefront_static: bool = False) -> Tuple[np.ndarray, dict]:
+        """One wavefront frame launched stage by stage with CUDA events between the
+        stages (the configuration an RN_PT_AUTO render would use): (mean image as
+        (height, width, 3) float32, per-stage device milliseconds and counts)."""
+        self._check_open()
+        rgb = np.empty((camera.height, camera.width, 3), np.float32)
+        t = _native.StageTimes()
+        flags = _sort_flag(ray_sort) | (_native.RN_PT_WAVEFRONT_STATIC if wavefront_static else 0)
+        _native.check(_native.load().rn_pt_profile_wavefront(self._handle, ctypes.byref(camera),
+                                                             ctypes.byref(settings), flags, None, _ptr(rgb),
+                                                             ctypes.byref(t)), "rn_pt_profile_wavefront")
+        return rgb, {k: getattr(t, k) for k, _ in t._fields_}
+
     def autotune(self, camera: "Camera", settings: "Settings", nearest_first: bool = False) -> dict:
         """Measure megakernel vs wavefront (and wavefront queue capacities) for this
         camera / settings; RN_PT_AUTO renders then use the fastest."""

@@ -15,7 +15,13 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("RN_B200_LIBRARY") or os.path.join(_HERE, "librednoise_b200.so")
 
 RN_OK = 0
+RN_ERR_INVALID_ARGUMENT = 1
+RN_ERR_CUDA = 2
 RN_ERR_OUT_OF_MEMORY = 3
+RN_ERR_UNSUPPORTED = 4
+RN_ERR_DEVICE_TIMEOUT = 5
+RN_ERR_CAPACITY = 6
+RN_ERR_INTERNAL = 7
 RN_PT_DEVICE_POINTERS = 1
 RN_PT_ORDER_NEAREST = 2
 RN_PT_WIDTH2 = 4
@@ -194,6 +200,14 @@ class Settings(ctypes.Structure):
         return s
 
 
+class StageTimes(ctypes.Structure):
+    """rn_pt_stage_times."""
+
+    _fields_ = [(k, ctypes.c_double) for k in ("camera_ms", "ray_sort_ms", "extend_ms", "shade_ms", "shadow_sort_ms",
+                                               "shadow_ms", "accumulate_ms", "total_ms")] + [
+        (k, ctypes.c_int) for k in ("launches", "waves", "samples_per_wave", "dynamic_fetch", "ray_sort")]
+
+
 class Tuning(ctypes.Structure):
     """rn_pt_tuning."""
 
@@ -258,6 +272,10 @@ SIGNATURES = {
     "rn_pt_render_static": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint, vp,
                                            vp]),
     "rn_pt_count_traversal": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), vp]),
+    "rn_pt_profile_wavefront": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
+                                               vp, vp, ctypes.POINTER(StageTimes)]),
+    "rn_pt_probe_read": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, vp,
+                                        ctypes.POINTER(ctypes.c_float)]),
     "rn_pt_autotune": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                       ctypes.POINTER(Tuning)]),
     "rn_pt_scene_set_materials": (ctypes.c_int, [vp, vp, vp, ctypes.c_uint, vp]),

@@ -14,6 +14,12 @@
 //   * uniforms of vertex b: blocks 2 + 2b (light select, light u, light v, lobe)
 //     and 3 + 2b (direction u, direction v, roulette, -).
 // Triangles whose emission is positive are lights: they are hit but absorb.
+//
+// Arithmetic contract: the translation units that include this file are compiled
+// without multiply-add contraction (-fmad=false), divisions and square roots are
+// IEEE, and sin/cos are sincos_turn's plain float operations, so every path's
+// radiance is the bit pattern the CPU restatement (compiled without contraction)
+// computes for the same uniforms.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -66,9 +72,58 @@ __device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y
 __device__ __forceinline__ F3 cross3(F3 a, F3 b) {
 	return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
-__device__ __forceinline__ F3 norm3(F3 a) { return a * rsqrtf(dot3(a, a)); }
+// 1 / sqrt with IEEE division and square root (not the approximate rsqrtf), so a
+// unit vector carries the same bits as the CPU restatement's a * (1 / std::sqrt(a.a)).
+__device__ __forceinline__ F3 norm3(F3 a) { return a * (1.0f / sqrtf(dot3(a, a))); }
 __device__ __forceinline__ float maxc(F3 a) { return fmaxf(a.x, fmaxf(a.y, a.z)); }
 __device__ __forceinline__ F3 ld3(const float4 v) { return {v.x, v.y, v.z}; }
+
+// sin(2 pi u) and cos(2 pi u) for u in [0, 1): the angle is reduced exactly to a
+// quarter turn q and a remainder f in [-1/2, 1/2] quarter turns (scaling by 4 and
+// removing the integer part are exact in float), x = f pi / 2 with |x| <= pi / 4,
+// then the Taylor series of sin to x^11 and of cos to x^12 (the omitted terms are
+// below 7e-12 there) and the quadrant's rotation. Written with plain IEEE float
+// operations only, so a CPU compiled without contraction computes the same bits;
+// about one ulp from the exact values.
+__device__ __forceinline__ void sincos_turn(float u, float &s, float &c) {
+	const float t = u * 4.0f;
+	int q = static_cast<int>(t);
+	float f = t - static_cast<float>(q);
+	if (f > 0.5f) {
+		f = f - 1.0f;
+		q = q + 1;
+	}
+	const float x = f * 1.57079632679489662f;
+	const float x2 = x * x;
+	const float sp =
+	    x + x * x2 *
+	            (-1.66666666666666667e-1f +
+	             x2 * (8.33333333333333333e-3f +
+	                   x2 * (-1.98412698412698413e-4f + x2 * (2.75573192239858907e-6f + x2 * -2.50521083854417188e-8f))));
+	const float cp =
+	    1.0f + x2 * (-0.5f + x2 * (4.16666666666666667e-2f +
+	                               x2 * (-1.38888888888888889e-3f +
+	                                     x2 * (2.48015873015873016e-5f +
+	                                           x2 * (-2.75573192239858907e-7f + x2 * 2.08767569878680990e-9f)))));
+	switch (q & 3) {
+	case 0:
+		s = sp;
+		c = cp;
+		break;
+	case 1:
+		s = cp;
+		c = -sp;
+		break;
+	case 2:
+		s = -sp;
+		c = -cp;
+		break;
+	default:
+		s = -cp;
+		c = sp;
+		break;
+	}
+}
 
 // Orthonormal basis around n (Duff et al., "Building an Orthonormal Basis, Revisited", 2017).
 __device__ __forceinline__ void onb(F3 n, F3 &t, F3 &b) {
@@ -330,7 +385,7 @@ __device__ __forceinline__ bool shade_vertex_t(const PhysScene &sc, const PhysSe
 	if (mat == 0) {
 		const float r = sqrtf(u01(rB.x));
 		float sn, cs;
-		sincosf(6.28318530717959f * u01(rB.y), &sn, &cs);
+		sincos_turn(u01(rB.y), sn, cs);
 		F3 t, bt;
 		onb(n, t, bt);
 		const float z = sqrtf(fmaxf(0.0f, 1.0f - u01(rB.x)));
@@ -350,11 +405,11 @@ __device__ __forceinline__ bool shade_vertex_t(const PhysScene &sc, const PhysSe
 		// Visible-normal sampling (Heitz 2018).
 		const F3 vh = norm3(f3(alpha * wl.x, alpha * wl.y, wl.z));
 		const float lensq = vh.x * vh.x + vh.y * vh.y;
-		const F3 T1 = lensq > 0.0f ? f3(-vh.y, vh.x, 0.0f) * rsqrtf(lensq) : f3(1.0f, 0.0f, 0.0f);
+		const F3 T1 = lensq > 0.0f ? f3(-vh.y, vh.x, 0.0f) * (1.0f / sqrtf(lensq)) : f3(1.0f, 0.0f, 0.0f);
 		const F3 T2 = cross3(vh, T1);
 		const float r = sqrtf(u01(rB.x));
 		float sn, cs;
-		sincosf(6.28318530717959f * u01(rB.y), &sn, &cs);
+		sincos_turn(u01(rB.y), sn, cs);
 		const float t1 = r * cs;
 		float t2 = r * sn;
 		const float sblend = 0.5f * (1.0f + vh.z);

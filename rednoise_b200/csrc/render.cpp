@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 
 #include "pt_kernels.hpp"
 #include "render_impl.hpp"
@@ -104,7 +105,8 @@ namespace {
 // default samples per wave; dyn selects the wavefront's per-lane ray replacement
 // and sort its binning of each bounce's rays.
 rn_status run_fixed(rn_scene *s, int integrator, int spw, int dyn, int sort, const PhysScene &ps,
-                    const PhysCamera &pc, const PhysSettings &pst, float *d_accum, cudaStream_t cs) {
+                    const PhysCamera &pc, const PhysSettings &pst, float *d_accum, cudaStream_t cs,
+                    WfStageClock *clock = nullptr) {
 	if (integrator == RN_PT_WAVEFRONT) {
 		if (pst.max_depth > kWfMaxDepth) {
 			set_last_error("render: the wavefront integrator supports max_depth <= 64");
@@ -127,6 +129,8 @@ rn_status run_fixed(rn_scene *s, int integrator, int spw, int dyn, int sort, con
 		rn_status r = s->wf->configure({job}, pst.max_depth, pst.order, spw, cs);
 		if (r != RN_OK)
 			return r;
+		if (clock) // profiled frame: the same launches, made directly with stage events
+			return s->wf->enqueue(s->d_status.as<int>(), cs, clock);
 		return s->wf->launch_graph(s->d_status.as<int>(), cs);
 	}
 	RNB_CUDA(s->d_counter.ensure(256));
@@ -261,6 +265,21 @@ rn_status run_integrator(rn_scene *s, const rn_pt_settings *st, unsigned flags, 
 	return run_fixed(s, integ, spw, dyn, pick_sort(sort), ps, pc, pst, d_accum, cs);
 }
 
+// The wavefront configuration an RN_PT_AUTO render would use when its tuned choice
+// is the wavefront, else the explicit wavefront's: (samples per wave, dyn, sort).
+std::tuple<int, int, int> wavefront_choice(rn_scene *s, unsigned flags, const PhysCamera &pc,
+                                           const PhysSettings &pst) {
+	auto pick_sort = [flags](int tuned) {
+		return (flags & RN_PT_RAY_SORT) ? 1 : ((flags & RN_PT_NO_RAY_SORT) ? 0 : tuned);
+	};
+	const bool static_lanes = (flags & RN_PT_WAVEFRONT_STATIC) != 0;
+	auto it = s->tuned.find(tune_key(pc, pst));
+	if (it != s->tuned.end() && std::get<0>(it->second) == RN_PT_WAVEFRONT)
+		return {std::get<1>(it->second), static_lanes ? 0 : std::get<2>(it->second),
+		        pick_sort(std::get<3>(it->second))};
+	return {0, static_lanes ? 0 : 1, pick_sort(0)};
+}
+
 rn_status finish_sync(rn_scene *s, cudaStream_t cs, const char *what) {
 	int h = 0;
 	RNB_CUDA(cudaMemcpyAsync(&h, s->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, cs));
@@ -276,6 +295,72 @@ rn_status finish_sync(rn_scene *s, cudaStream_t cs, const char *what) {
 } // namespace
 
 extern "C" {
+
+rn_status rn_pt_profile_wavefront(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
+                                  unsigned flags, void *stream, float *rgb, rn_pt_stage_times *out) {
+	TraceRange trace_range("rn_pt_profile_wavefront");
+	PhysScene ps;
+	PhysCamera pc;
+	PhysSettings pst;
+	rn_status r = make_phys_inputs(scene, camera, settings, flags, ps, pc, pst);
+	if (r != RN_OK)
+		return r;
+	if (!rgb || !out) {
+		set_last_error("rn_pt_profile_wavefront: NULL rgb or out");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	cudaStream_t cs = pick_stream(scene, stream);
+	const long nf = static_cast<long>(camera->width) * camera->height * 3;
+	const size_t bytes = static_cast<size_t>(nf) * sizeof(float);
+	const float inv = settings->spp > 0 ? 1.0f / static_cast<float>(settings->spp) : 0.0f;
+	std::lock_guard<std::mutex> lock(scene->scratch_mu);
+	RNB_CUDA(scene->scratch.ensure(2 * bytes + 256));
+	float *acc = scene->scratch.as<float>();
+	float *mean = (flags & RN_PT_DEVICE_POINTERS) ? rgb : acc + nf + 64;
+	const auto [spw, dyn, sort] = wavefront_choice(scene, flags, pc, pst);
+	std::unique_ptr<WfStageClock> clock(new WfStageClock());
+	RNB_CUDA(cudaMemsetAsync(acc, 0, bytes, cs));
+	r = run_fixed(scene, RN_PT_WAVEFRONT, spw, dyn, sort, ps, pc, pst, acc, cs, clock.get());
+	if (r != RN_OK)
+		return r;
+	RNB_CUDA(launch_resolve(acc, mean, nf, inv, cs));
+	RNB_CUDA(clock->mark(kStAccumulate, 1, cs));
+	if (!(flags & RN_PT_DEVICE_POINTERS))
+		RNB_CUDA(cudaMemcpyAsync(rgb, mean, bytes, cudaMemcpyDeviceToHost, cs));
+	r = finish_sync(scene, cs, "rn_pt_profile_wavefront");
+	if (r != RN_OK)
+		return r;
+	if (clock->overflow) {
+		set_last_error("rn_pt_profile_wavefront: more stages than the profiler records");
+		return RN_ERR_CAPACITY;
+	}
+	double ms[kStCount] = {};
+	cudaEvent_t prev = clock->start;
+	for (int i = 0; i < clock->n; i++) {
+		float t = 0.0f;
+		RNB_CUDA(cudaEventElapsedTime(&t, prev, clock->ev[i]));
+		ms[clock->kind[i]] += t;
+		prev = clock->ev[i];
+	}
+	float total = 0.0f;
+	if (clock->n > 0)
+		RNB_CUDA(cudaEventElapsedTime(&total, clock->start, clock->ev[clock->n - 1]));
+	out->camera_ms = ms[kStCamera];
+	out->ray_sort_ms = ms[kStRaySort];
+	out->extend_ms = ms[kStExtend];
+	out->shade_ms = ms[kStShade];
+	out->shadow_sort_ms = ms[kStShadowSort];
+	out->shadow_ms = ms[kStShadow];
+	out->accumulate_ms = ms[kStAccumulate];
+	out->total_ms = total;
+	out->launches = clock->launches;
+	const int used_spw = spw > 0 ? spw : default_samples_per_wave(pc.width * static_cast<long>(pc.height), pst.spp);
+	out->waves = pst.spp > 0 ? (pst.spp + used_spw - 1) / used_spw : 0;
+	out->samples_per_wave = used_spw;
+	out->dynamic_fetch = dyn;
+	out->ray_sort = sort;
+	return RN_OK;
+}
 
 rn_status rn_pt_render_accumulate(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
                                   unsigned flags, void *stream, float *accum) {

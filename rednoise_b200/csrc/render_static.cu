@@ -15,7 +15,12 @@
 // images are rejected. All calls share it and it keeps the previous call's
 // contents, so each call clears the parts that must start at zero; calls whose GPU
 // work overlaps (two streams, two threads) race on it and must be serialised by
-// the caller.
+// the caller. The output must be device (or managed) memory of the scene's GPU:
+// the pointer is checked with cudaPointerGetAttributes, which allocates nothing,
+// before any GPU work, so a host buffer is refused instead of being written by a
+// kernel. The array's device address is looked up once per device and kept for
+// the life of the process; cudaDeviceReset unloads the module that holds the
+// array, so calling this entry point after a reset of the device is unsupported.
 #include <mutex>
 
 #include "pt_kernels.hpp"
@@ -72,7 +77,12 @@ rn_status rn_pt_render_static(rn_scene *scene, const rn_pt_camera *camera, const
 		set_last_error("rn_pt_render_static: NULL argument");
 		return RN_ERR_INVALID_ARGUMENT;
 	}
-	if (!scene->prepared) {
+	bool prepared;
+	{
+		std::lock_guard<std::mutex> lock(scene->mu); // prepare_scene sets the flag under this lock
+		prepared = scene->prepared;
+	}
+	if (!prepared) {
 		set_last_error("rn_pt_render_static: prepare the scene first (rn_pt_scene_prepare allocates)");
 		return RN_ERR_INVALID_ARGUMENT;
 	}
@@ -92,6 +102,20 @@ rn_status rn_pt_render_static(rn_scene *scene, const rn_pt_camera *camera, const
 	RNB_CUDA(cudaGetDevice(&dev));
 	if (dev != scene->device) {
 		set_last_error("rn_pt_render_static: make the scene's device current first");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	// The output must be memory a kernel on this device may write: a host buffer
+	// (pageable or pinned) is refused here, before any GPU work.
+	cudaPointerAttributes pa{};
+	const cudaError_t pe = cudaPointerGetAttributes(&pa, rgb);
+	if (pe != cudaSuccess) {
+		(void)cudaGetLastError(); // an unknown pointer also sets the thread's last CUDA error; clear it
+		set_last_error("rn_pt_render_static: rgb is not a CUDA device pointer");
+		return RN_ERR_INVALID_ARGUMENT;
+	}
+	if (!((pa.type == cudaMemoryTypeDevice && pa.device == dev) || pa.type == cudaMemoryTypeManaged)) {
+		set_last_error("rn_pt_render_static: rgb must be device memory of the scene's GPU (or managed memory); "
+		               "host buffers are not accepted");
 		return RN_ERR_INVALID_ARGUMENT;
 	}
 	void *base = nullptr;

@@ -683,8 +683,14 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 		if (e != cudaSuccess)
 			return e;
 	}
+	// profiled frames: an event after every stage (no effect on the work)
+	auto mark = [&](int stage, int kernels) -> cudaError_t {
+		return lc.clock ? lc.clock->mark(stage, kernels, st) : cudaSuccess;
+	};
 	const int gcam = (wave.n_slots + 255) / 256 < 148 * 8 ? (wave.n_slots + 255) / 256 : 148 * 8;
 	k_wf_camera<<<gcam, 256, 0, st>>>(d_jobs, pool, wave);
+	if ((e = mark(kStCamera, 1)) != cudaSuccess)
+		return e;
 	const bool use_dyn = lc.dyn && order == kOrderReference && !adj;
 	const bool sort = lc.sort && pool.keys && pool.fine && pool.sorted_coarse && pool.sorted_fine && pool.sorted &&
 	                  pool.bins;
@@ -699,6 +705,8 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.sorted_coarse, pool.sorted_fine, pool.sorted,
 			                                            static_cast<unsigned>(pool.capacity), status);
 			q = pool.sorted;
+			if ((e = mark(kStRaySort, 4)) != cudaSuccess)
+				return e;
 		}
 		const int oj = wave.only_job;
 		if (use_dyn)
@@ -707,6 +715,8 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			k_wf_extend<kOrderNearest><<<lc.grid_ext, 128, kWfExtendSmem, st>>>(d_jobs, pool, k, q, oj, status);
 		else
 			k_wf_extend<kOrderReference><<<lc.grid_ext, 128, kWfExtendSmem, st>>>(d_jobs, pool, k, q, oj, status);
+		if ((e = mark(kStExtend, 1)) != cudaSuccess)
+			return e;
 		// Shading takes the queue in its append order, not the binned order: the previous
 		// bounce appended each warp's surviving slots in increasing order, so the path
 		// state reads and writes of neighbouring lanes fall on neighbouring slots. The
@@ -716,6 +726,8 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 		else
 			k_wf_shade<false><<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, pool.queue[k & 1], sort ? 1 : 0,
 			                                                 status);
+		if ((e = mark(kStShade, 1)) != cudaSuccess)
+			return e;
 		if (use_dyn)
 			k_wf_trace_dyn<true><<<lc.grid_dyn, 128, 0, st>>>(d_jobs, pool, k, nullptr, oj, status);
 		else {
@@ -731,6 +743,8 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 				k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.sorted_coarse, pool.sorted_fine,
 				                                            pool.sh_sorted, static_cast<unsigned>(pool.capacity),
 				                                            status);
+				if ((e = mark(kStShadowSort, 4)) != cudaSuccess)
+					return e;
 			}
 			const int *order_sh = sort_sh ? pool.sh_sorted : nullptr;
 			if (adj)
@@ -738,6 +752,8 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			else
 				k_wf_shadow<false><<<lc.grid_sh, 128, kWfShadowSmem, st>>>(d_jobs, pool, k, oj, order_sh, status);
 		}
+		if ((e = mark(kStShadow, 1)) != cudaSuccess)
+			return e;
 	}
 	if (adj) {
 		k_wf_adj_flush<<<gcam, 256, 0, st>>>(d_jobs, pool, wave);
@@ -745,6 +761,8 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 	}
 	const int gacc = (wave.n_pix + 255) / 256 < 148 * 8 ? (wave.n_pix + 255) / 256 : 148 * 8;
 	k_wf_accumulate<<<gacc, 256, 0, st>>>(d_jobs, pool, wave);
+	if ((e = mark(kStAccumulate, 1)) != cudaSuccess)
+		return e;
 	return cudaGetLastError();
 }
 

@@ -116,10 +116,57 @@ struct WfWave {
 };
 
 // Launch shapes and stage options of a wave.
+// Stage kinds of a frame, for per-stage timing.
+enum WfStage : int {
+	kStCamera = 0,
+	kStRaySort,    // two-level counting sort of a bounce's closest-hit queue
+	kStExtend,     // closest hits
+	kStShade,      // shading, next-event records, continuation
+	kStShadowSort, // counting sort of a bounce's shadow records
+	kStShadow,     // any hits of the shadow records
+	kStAccumulate, // per-pixel sums and the frame's resolve
+	kStCount
+};
+
+// CUDA events recorded after every stage of a frame launched directly (not from
+// the captured graph): consecutive events bracket one stage each. Host-side; the
+// events are created on first use and destroyed with the clock.
+struct WfStageClock {
+	static constexpr int kMax = 4096;
+	cudaEvent_t start = nullptr;
+	cudaEvent_t ev[kMax] = {};
+	int kind[kMax] = {};
+	int n = 0;
+	int launches = 0; // kernels launched in the frame
+	bool overflow = false;
+	cudaError_t mark(int stage, int kernels, cudaStream_t st) {
+		launches += kernels;
+		if (n >= kMax) {
+			overflow = true;
+			return cudaSuccess;
+		}
+		if (!ev[n]) {
+			const cudaError_t e = cudaEventCreate(&ev[n]);
+			if (e != cudaSuccess)
+				return e;
+		}
+		kind[n] = stage;
+		return cudaEventRecord(ev[n++], st);
+	}
+	~WfStageClock() {
+		if (start)
+			cudaEventDestroy(start);
+		for (int i = 0; i < kMax; i++)
+			if (ev[i])
+				cudaEventDestroy(ev[i]);
+	}
+};
+
 struct WfLaunch {
 	int grid_ext, grid_shade, grid_sh, grid_dyn, grid_bin;
 	int dyn;  // traversal stages use persistent warps that replace finished rays per lane
 	int sort; // closest-hit queues after the first bounce are binned by origin and direction
+	WfStageClock *clock = nullptr; // per-stage events (profiled frames only)
 };
 
 cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave &wave, int max_depth, int order,

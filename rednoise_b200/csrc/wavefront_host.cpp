@@ -210,14 +210,21 @@ void WfContext::set_frame_io(float *zero_ptr, size_t zero_bytes, const std::vect
 	resolves_ = resolves;
 }
 
-rn_status WfContext::enqueue(int *status, cudaStream_t st) {
+rn_status WfContext::enqueue(int *status, cudaStream_t st, WfStageClock *clock) {
+	if (clock) {
+		if (!clock->start)
+			RNB_CUDA(cudaEventCreate(&clock->start));
+		RNB_CUDA(cudaEventRecord(clock->start, st));
+	}
 	if (zero_ptr_ && zero_bytes_)
 		RNB_CUDA(cudaMemsetAsync(zero_ptr_, 0, zero_bytes_, st));
-	const WfLaunch lc{grid_ext_, grid_shade_, grid_sh_, grid_dyn_, grid_bin_, dyn_, sort_};
+	const WfLaunch lc{grid_ext_, grid_shade_, grid_sh_, grid_dyn_, grid_bin_, dyn_, sort_, clock};
 	for (const WfWave &w : waves_)
 		RNB_CUDA(wf_launch_wave(d_jobs_.as<WfJob>(), pool_, w, max_depth_, order_, lc, status, st));
 	for (const Resolve &r : resolves_)
 		RNB_CUDA(launch_resolve(r.accum, r.mean, r.n_floats, r.inv_spp, st));
+	if (clock && !resolves_.empty())
+		RNB_CUDA(clock->mark(kStAccumulate, static_cast<int>(resolves_.size()), st));
 	return RN_OK;
 }
 

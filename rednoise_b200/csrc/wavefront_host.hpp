@@ -58,8 +58,9 @@ public:
 		float inv_spp;
 	};
 	void set_frame_io(float *zero_ptr, size_t zero_bytes, const std::vector<Resolve> &resolves);
-	// Enqueue every wave of the frame on st (direct launches).
-	rn_status enqueue(int *status, cudaStream_t st);
+	// Enqueue every wave of the frame on st (direct launches); with a clock, an event
+	// is recorded before the frame and after every stage.
+	rn_status enqueue(int *status, cudaStream_t st, WfStageClock *clock = nullptr);
 	// Capture the frame into a CUDA graph on first use, then launch it.
 	rn_status launch_graph(int *status, cudaStream_t st);
 	int capacity() const { return capacity_; }

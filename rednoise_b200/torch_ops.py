@@ -49,6 +49,10 @@ class _PathTrace(torch.autograd.Function):
             _native.check(lib.rn_pt_render(scene.handle, ctypes.byref(camera), ctypes.byref(settings), flags, stream,
                                            ctypes.c_void_p(img.data_ptr())), "rn_pt_render")
             images.append(img)
+        # The scene holds one set of materials: backward puts this call's back before
+        # replaying the paths, so another forward in between (another parameter set on
+        # the same scene) does not change what this call differentiates.
+        ctx.save_for_backward(albedo, emission)
         ctx.scene = scene
         ctx.adjoint = adjoint
         ctx.device = albedo.device
@@ -67,8 +71,14 @@ class _PathTrace(torch.autograd.Function):
         ptrs = (ctypes.c_void_p * nv)(*[g.data_ptr() for g in gimgs])
         d_alb = torch.empty((n, 3), dtype=torch.float32, device=ctx.device)
         d_em = torch.empty((n, 3), dtype=torch.float32, device=ctx.device)
+        albedo, emission = ctx.saved_tensors
+        stream = _stream_handle()
+        _native.check(lib.rn_pt_scene_set_materials(scene.handle, ctypes.c_void_p(albedo.data_ptr()),
+                                                    ctypes.c_void_p(emission.data_ptr()),
+                                                    _native.RN_PT_DEVICE_POINTERS, stream),
+                      "rn_pt_scene_set_materials")
         _native.check(lib.rn_pt_backward(scene.handle, nv, cams, sets, ptrs, _native.RN_PT_DEVICE_POINTERS,
-                                         _stream_handle(), ctypes.c_void_p(d_alb.data_ptr()),
+                                         stream, ctypes.c_void_p(d_alb.data_ptr()),
                                          ctypes.c_void_p(d_em.data_ptr())), "rn_pt_backward")
         return d_alb, d_em, None, None, None
 

@@ -243,3 +243,43 @@ def test_invalid_settings_rejected(box):
     c = rn.Camera.make((0, 0, 5), (0, 0, 0), width=8, height=8)
     with pytest.raises(rn.RnError):
         s.render_physical(c, rn.Settings.make(spp=1, max_depth=0))
+
+
+def test_profile_wavefront_equals_render_and_times_every_stage():
+    """The profiled frame (kernel by kernel, events between stages) renders the same
+    image as rn_pt_render's captured frame and accounts for every stage."""
+    sc = scenes.icosphere_scene(level=3)
+    s = make_scene(sc)
+    c = cam(64, 48)
+    camera = rn.Camera.make(c["position"], c["target"], c["up"], c["vfov_deg"], 64, 48)
+    for sort in (False, True):
+        st = rn.Settings.make(spp=8, max_depth=6, rr_depth=3, seed=4, integrator=2)
+        want = s.render_physical(camera, st, ray_sort=sort, wavefront_static=True)
+        got, t = s.profile_wavefront(camera, st, ray_sort=sort, wavefront_static=True)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+        assert t["ray_sort"] == int(sort) and t["dynamic_fetch"] == 0
+        for k in ("camera_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms"):
+            assert t[k] > 0, (k, t)
+        parts = sum(t[k] for k in ("camera_ms", "ray_sort_ms", "extend_ms", "shade_ms", "shadow_sort_ms",
+                                   "shadow_ms", "accumulate_ms"))
+        assert abs(parts - t["total_ms"]) <= 1e-3 * t["total_ms"] + 1e-3, (parts, t)
+        per_wave = 2 + 3 * 6 + (4 * 5 + 4 * 6 if sort else 0)
+        assert t["launches"] == t["waves"] * per_wave + 1, t
+
+
+def test_read_probe_measures_bandwidth():
+    import ctypes
+
+    import torch
+
+    from rednoise_b200 import _native
+
+    lib = _native.load()
+    buf = torch.zeros(16 << 20, dtype=torch.uint8, device="cuda")
+    ms = ctypes.c_float(0.0)
+    _native.check(lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr()), buf.numel(), 10, 1, None,
+                                       ctypes.byref(ms)), "rn_pt_probe_read")
+    gbs = buf.numel() * 10 / (ms.value / 1e3) / 1e9
+    assert 100 < gbs < 200000, gbs
+    assert lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr() + 4), 1024, 1, 1, None,
+                                ctypes.byref(ms)) == _native.RN_ERR_INVALID_ARGUMENT
