@@ -38,6 +38,19 @@ def ref_available() -> bool:
     return os.path.isfile(REF_PATH)
 
 
+def reference_dir():
+    """The reference source tree: $RN_REFERENCE_DIR, else the directory oracle/Makefile
+    built _ref/librn_ref.so from (recorded in _ref/source_dir.txt); None when neither
+    names an existing directory (the GPU box has no reference tree)."""
+    d = os.environ.get("RN_REFERENCE_DIR")
+    if not d:
+        rec = os.path.join(HERE, "_ref", "source_dir.txt")
+        if os.path.isfile(rec):
+            with open(rec) as f:
+                d = f.read().strip()
+    return d if d and os.path.isdir(d) else None
+
+
 def ref() -> ctypes.CDLL:
     global _REF
     if _REF is None:

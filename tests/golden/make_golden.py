@@ -94,4 +94,4 @@ def main(refdir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RN_REFERENCE_DIR", "/root/reference"))

@@ -46,16 +46,33 @@ def setup():
     return sc, target, v
 
 
-def test_albedo_gradient_matches_central_differences(setup):
-    sc, target, v = setup
+def test_c4_albedo_gradient_64_parameters_within_2_percent():
+    """The differentiable-render check at its stated size: the 36-triangle box at
+    512x512, 32 spp, depth 6, L2 loss against a render with per-triangle albedo
+    perturbed by N(0, 0.1) clipped to [0.05, 0.95]. Central differences (eps 1e-3,
+    common random numbers: both evaluations and the adjoint replay the same samples)
+    on 64 seeded (triangle, channel) parameters of the 34 non-emitting triangles:
+    every one within 2 % of the adjoint's gradient. Russian roulette is off so the
+    fixed-sample estimator is a polynomial in the albedo (roulette decisions depend on
+    the throughput and would make it piecewise). Parameters that no path reaches (the
+    boxes' bottom faces) have exactly zero gradient and exactly zero difference."""
+    sc = scenes.cornell_box()
+    rng = np.random.default_rng(0x5EED0004)
+    tgt = dict(sc)
+    tgt["albedo"] = np.clip(sc["albedo"] + rng.normal(0, 0.1, sc["albedo"].shape), 0.05, 0.95).astype(np.float32)
+    v = view(512, 512, seed=3, spp=32, depth=6)
+    target = make_scene(tgt).render_physical(v[0], v[1]).astype(np.float64)
     s = make_scene(sc)
     L0, dI = loss_and_grad(s, sc, target, v)
-    ga, ge = s.backward([v], [dI.astype(np.float32)])
-    rng = np.random.default_rng(1)
+    assert L0 > 0
+    ga, _ = s.backward([v], [dI.astype(np.float32)])
+    emitting = sc["emission"].sum(1) > 0
+    cand = [(t, c) for t in np.nonzero(~emitting)[0] for c in range(3)]
+    pick = np.random.default_rng(64).permutation(len(cand))[:64]
     eps = 1e-3
-    errs = []
-    for _ in range(24):
-        tri, ch = int(rng.integers(0, 34)), int(rng.integers(0, 3))
+    errs, zeros = [], 0
+    for i in pick:
+        tri, ch = cand[i]
         alb = sc["albedo"].copy()
         alb[tri, ch] += eps
         s.set_materials(albedo=alb)
@@ -65,10 +82,14 @@ def test_albedo_gradient_matches_central_differences(setup):
         Lm, _ = loss_and_grad(s, sc, target, v)
         s.set_materials(albedo=sc["albedo"])
         fd = (Lp - Lm) / (2 * eps)
-        if abs(fd) > 1e-7:
-            errs.append(abs(fd - ga[tri, ch]) / abs(fd))
-    assert len(errs) >= 8
-    assert np.median(errs) < 0.02 and max(errs) < 0.1, errs
+        if fd == 0.0:
+            assert ga[tri, ch] == 0.0, (tri, ch, ga[tri, ch])
+            zeros += 1
+            continue
+        errs.append((abs(fd - ga[tri, ch]) / abs(fd), int(tri), ch, fd, float(ga[tri, ch])))
+    assert len(errs) + zeros == 64 and len(errs) >= 48
+    worst = max(errs)
+    assert worst[0] < 0.02, sorted(errs)[-4:]
 
 
 def test_emission_gradient_matches_central_differences(setup):
@@ -135,6 +156,45 @@ def test_torch_autograd_function(setup):
     ga, ge = s.backward([v], [dI.astype(np.float32)])
     assert np.allclose(alb.grad.cpu().numpy(), ga, rtol=1e-3, atol=1e-9)
     assert np.allclose(em.grad.cpu().numpy(), ge, rtol=1e-3, atol=1e-9)
+
+
+def test_torch_backward_uses_its_own_forward_materials(setup):
+    """Two forwards on one scene with different albedos, then the FIRST one's
+    backward: the gradient is the first parameter set's (checked against the adjoint
+    at those materials and against central differences there), not the one the
+    second forward left in the scene."""
+    torch = pytest.importorskip("torch")
+    from rednoise_b200 import torch_ops
+
+    sc, target, v = setup
+    s = make_scene(sc)
+    tgt = torch.tensor(target, dtype=torch.float32, device="cuda")
+    alb1 = torch.tensor(sc["albedo"], device="cuda", requires_grad=True)
+    alb2 = torch.tensor(np.clip(sc["albedo"] * 0.6, 0.05, 0.95), device="cuda", requires_grad=True)
+    em = torch.tensor(sc["emission"], device="cuda")
+    (img1,) = torch_ops.render(alb1, em, s, [v])
+    (img2,) = torch_ops.render(alb2, em, s, [v])
+    loss1 = ((img1 - tgt) ** 2).sum()
+    loss1.backward()
+    s.set_materials(albedo=sc["albedo"])
+    _, dI = loss_and_grad(s, sc, target, v)
+    ga, _ = s.backward([v], [dI.astype(np.float32)])
+    got = alb1.grad.cpu().numpy()
+    assert np.abs(ga).max() > 0
+    assert np.allclose(got, ga, rtol=1e-3, atol=1e-9 * np.abs(ga).max())
+    # and against central differences at the first parameters, on its largest entry
+    tri, ch = np.unravel_index(np.argmax(np.abs(ga)), ga.shape)
+    eps = 1e-3
+    alb = sc["albedo"].copy()
+    alb[tri, ch] += eps
+    s.set_materials(albedo=alb)
+    Lp, _ = loss_and_grad(s, sc, target, v)
+    alb[tri, ch] -= 2 * eps
+    s.set_materials(albedo=alb)
+    Lm, _ = loss_and_grad(s, sc, target, v)
+    fd = (Lp - Lm) / (2 * eps)
+    assert abs(got[tri, ch] - fd) <= 0.02 * abs(fd), (got[tri, ch], fd)
+    del img2
 
 
 def test_multi_view_backward_sums_views(setup):

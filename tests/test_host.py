@@ -16,7 +16,7 @@ from rednoise_b200 import _native, scenes
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLD = os.path.join(ROOT, "tests", "golden")
-REF_ASSETS = "/root/reference/assets"
+REF_ASSETS = os.path.join(oracle.reference_dir() or "", "assets")
 
 
 def declared_functions():

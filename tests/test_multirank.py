@@ -99,3 +99,34 @@ def test_single_rank_max_is_identity():
     assert bench.max_over_ranks([3.5, 1.0]) == [3.5, 1.0]
     assert bench.shard_sample_offset(0, 0, 1, 64) == 0
     assert bench.shard_sample_offset(2, 0, 1, 64) == 128
+
+
+def _spawned(out_dir: str):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import bench
+
+    rank, local_rank, world = bench.dist_env()
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    try:
+        t = torch.tensor([rank, local_rank, world, dist.get_rank(), dist.get_world_size()], dtype=torch.int64)
+        every = [torch.zeros_like(t) for _ in range(world)]
+        dist.all_gather(every, t)
+        if rank == 0:
+            np.save(os.path.join(out_dir, "ranks.npy"), torch.stack(every).numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_spawn_ranks_sets_the_launcher_environment(tmp_path):
+    """bench.py --gpus N without torchrun starts N ranks with torchrun's environment
+    (RANK, LOCAL_RANK, WORLD_SIZE, MASTER_ADDR=127.0.0.1, MASTER_PORT)."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    bench.spawn_ranks(2, _spawned, str(tmp_path))
+    got = np.load(tmp_path / "ranks.npy")
+    assert got.tolist() == [[0, 0, 2, 0, 2], [1, 1, 2, 1, 2]]
