@@ -417,23 +417,24 @@ def measured_peaks():
 
 def read_peaks(lib, stream, sptr) -> dict:
     """Read bandwidths measured on this GPU in this run (rn_pt_probe_read, CUDA events):
-    an L2-resident read (16-64 MB buffers, loads that bypass L1; the best size) and an
-    HBM read (a 2 GB buffer)."""
+    an L2-resident read (8-64 MB buffers read repeatedly within each launch, about
+    2 GB per launch, with loads that bypass L1; the best size) and an HBM read (a
+    2 GB buffer, one pass per launch)."""
     import torch
 
     from rednoise_b200 import _native
 
     out = {}
     best = 0.0
-    for mb in (16, 32, 64):
+    for mb in (8, 16, 32, 64):
         buf = torch.empty(mb << 20, dtype=torch.uint8, device="cuda")
         buf.zero_()
         torch.cuda.synchronize()
         ms = ctypes.c_float(0.0)
-        n = 200
-        _native.check(lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr()), buf.numel(), n, 1, sptr,
+        passes, n = (2 << 30) // buf.numel(), 20
+        _native.check(lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr()), buf.numel(), passes, n, 1, sptr,
                                            ctypes.byref(ms)), "rn_pt_probe_read")
-        gbs = buf.numel() * n / (ms.value / 1e3) / 1e9
+        gbs = buf.numel() * passes * n / (ms.value / 1e3) / 1e9
         out[f"l2_read_{mb}MB_gbs"] = gbs
         best = max(best, gbs)
         del buf
@@ -442,8 +443,8 @@ def read_peaks(lib, stream, sptr) -> dict:
     big.zero_()
     torch.cuda.synchronize()
     ms = ctypes.c_float(0.0)
-    _native.check(lib.rn_pt_probe_read(ctypes.c_void_p(big.data_ptr()), big.numel(), 5, 1, sptr, ctypes.byref(ms)),
-                  "rn_pt_probe_read")
+    _native.check(lib.rn_pt_probe_read(ctypes.c_void_p(big.data_ptr()), big.numel(), 1, 5, 1, sptr,
+                                       ctypes.byref(ms)), "rn_pt_probe_read")
     out["hbm_read_gbs"] = big.numel() * 5 / (ms.value / 1e3) / 1e9
     del big
     torch.cuda.empty_cache()

@@ -376,13 +376,15 @@ typedef struct {
 rn_status rn_pt_profile_wavefront(rn_scene *scene, const rn_pt_camera *camera, const rn_pt_settings *settings,
                                   unsigned flags, void *stream, float *rgb, rn_pt_stage_times *out);
 
-/* Read the device buffer buf (bytes, 16-byte aligned) once per launch, `launches`
- * times, with 16-byte loads from a persistent grid, after one untimed launch, and
- * write the device time of the timed launches to *ms (bandwidth = bytes * launches
- * / ms). l2_only: the loads bypass L1, so a buffer well under the L2's size gives
- * the L2 read bandwidth and one far above it the HBM read bandwidth. Synchronises
- * the stream. A roofline probe with no counterpart in the reference. */
-rn_status rn_pt_probe_read(const void *buf, size_t bytes, int launches, int l2_only, void *stream, float *ms);
+/* Read the device buffer buf (bytes, 16-byte aligned) `passes` times per launch,
+ * `launches` times, with 16-byte loads from a persistent grid, after one untimed
+ * launch, and write the device time of the timed launches to *ms (bandwidth =
+ * bytes * passes * launches / ms). l2_only: the loads bypass L1, so a buffer well
+ * under the L2's size gives the L2 read bandwidth and one far above it the HBM
+ * read bandwidth. Synchronises the stream. A roofline probe with no counterpart in
+ * the reference. */
+rn_status rn_pt_probe_read(const void *buf, size_t bytes, int passes, int launches, int l2_only, void *stream,
+                           float *ms);
 
 /* ---- differentiable rendering ---- */
 

@@ -274,7 +274,7 @@ SIGNATURES = {
     "rn_pt_count_traversal": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), vp]),
     "rn_pt_profile_wavefront": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                                vp, vp, ctypes.POINTER(StageTimes)]),
-    "rn_pt_probe_read": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, vp,
+    "rn_pt_probe_read": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
                                         ctypes.POINTER(ctypes.c_float)]),
     "rn_pt_autotune": (ctypes.c_int, [vp, ctypes.POINTER(Camera), ctypes.POINTER(Settings), ctypes.c_uint,
                                       ctypes.POINTER(Tuning)]),

@@ -32,10 +32,6 @@ namespace rnb {
 
 constexpr int kStack = 64; // same bound as the reference's int stack[64]
 
-#ifndef RN_ANY_ORDER
-#define RN_ANY_ORDER 0
-#endif
-
 struct SceneView {
 	const float4 *__restrict__ nodes;  // 4 float4 per internal node (2-wide)
 	const float4 *__restrict__ nodes4; // 8 float4 per node (4-wide collapse), may be null
@@ -734,7 +730,6 @@ __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, 
 				err = 1;
 				return false;
 			}
-#if RN_ANY_ORDER == 0
 			if (b3)
 				st.put(sp++, __float_as_int(rf.w));
 			if (b2)
@@ -749,80 +744,6 @@ __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, 
 				ref = 0x7fffffff;
 				break;
 			}
-#elif RN_ANY_ORDER == 1
-			// Descend into the entry whose box the ray enters first; push the others.
-			const unsigned kMiss = 0xffffffffu;
-			const unsigned k0 = b0 ? __float_as_uint(fmaxf(t0, 0.0f)) : kMiss;
-			const unsigned k1 = b1 ? __float_as_uint(fmaxf(t1, 0.0f)) : kMiss;
-			const unsigned k2 = b2 ? __float_as_uint(fmaxf(t2, 0.0f)) : kMiss;
-			const unsigned k3 = b3 ? __float_as_uint(fmaxf(t3, 0.0f)) : kMiss;
-			int best = 0;
-			unsigned kb = k0;
-			if (k1 < kb) {
-				kb = k1;
-				best = 1;
-			}
-			if (k2 < kb) {
-				kb = k2;
-				best = 2;
-			}
-			if (k3 < kb) {
-				kb = k3;
-				best = 3;
-			}
-			if (b3 && best != 3)
-				st.put(sp++, __float_as_int(rf.w));
-			if (b2 && best != 2)
-				st.put(sp++, __float_as_int(rf.z));
-			if (b1 && best != 1)
-				st.put(sp++, __float_as_int(rf.y));
-			if (b0 && best != 0)
-				st.put(sp++, __float_as_int(rf.x));
-			if (kb != kMiss) {
-				ref = __float_as_int(best == 0 ? rf.x : best == 1 ? rf.y : best == 2 ? rf.z : rf.w);
-			} else if (sp > 0) {
-				ref = st.get(--sp);
-			} else {
-				ref = 0x7fffffff;
-				break;
-			}
-#else
-			// Entries in the order the ray enters their boxes: the nearest is descended
-			// into, the others pushed farthest first.
-			const unsigned long long kMiss = ~0ull;
-			auto key = [](bool b, float t, unsigned slot) {
-				return b ? (static_cast<unsigned long long>(__float_as_uint(fmaxf(t, 0.0f))) << 32) | slot : ~0ull;
-			};
-			unsigned long long e0 = key(b0, t0, 0u), e1 = key(b1, t1, 1u), e2 = key(b2, t2, 2u), e3 = key(b3, t3, 3u);
-			auto cx = [](unsigned long long &a, unsigned long long &b) {
-				const unsigned long long lo = a < b ? a : b, hi = a < b ? b : a;
-				a = lo;
-				b = hi;
-			};
-			cx(e0, e1);
-			cx(e2, e3);
-			cx(e0, e2);
-			cx(e1, e3);
-			cx(e1, e2);
-			auto ref_of = [&](unsigned long long e) {
-				const unsigned slot = static_cast<unsigned>(e) & 3u;
-				return __float_as_int(slot == 0 ? rf.x : slot == 1 ? rf.y : slot == 2 ? rf.z : rf.w);
-			};
-			if (e3 != kMiss)
-				st.put(sp++, ref_of(e3));
-			if (e2 != kMiss)
-				st.put(sp++, ref_of(e2));
-			if (e1 != kMiss)
-				st.put(sp++, ref_of(e1));
-			if (e0 != kMiss) {
-				ref = ref_of(e0);
-			} else if (sp > 0) {
-				ref = st.get(--sp);
-			} else {
-				ref = 0x7fffffff;
-				break;
-			}
-#endif
 		}
 		if (ref == 0x7fffffff)
 			continue;

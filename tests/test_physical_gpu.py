@@ -277,9 +277,11 @@ def test_read_probe_measures_bandwidth():
     lib = _native.load()
     buf = torch.zeros(16 << 20, dtype=torch.uint8, device="cuda")
     ms = ctypes.c_float(0.0)
-    _native.check(lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr()), buf.numel(), 10, 1, None,
+    _native.check(lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr()), buf.numel(), 8, 10, 1, None,
                                        ctypes.byref(ms)), "rn_pt_probe_read")
-    gbs = buf.numel() * 10 / (ms.value / 1e3) / 1e9
+    gbs = buf.numel() * 8 * 10 / (ms.value / 1e3) / 1e9
     assert 100 < gbs < 200000, gbs
-    assert lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr() + 4), 1024, 1, 1, None,
+    assert lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr() + 4), 1024, 1, 1, 1, None,
+                                ctypes.byref(ms)) == _native.RN_ERR_INVALID_ARGUMENT
+    assert lib.rn_pt_probe_read(ctypes.c_void_p(buf.data_ptr()), 1024, 0, 1, 1, None,
                                 ctypes.byref(ms)) == _native.RN_ERR_INVALID_ARGUMENT
