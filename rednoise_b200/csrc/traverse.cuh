@@ -692,6 +692,147 @@ __device__ __forceinline__ HitRec trace_closest4_flat(const SceneView &s, const 
 	return h;
 }
 
+// trace_closest4 with postponed leaves (speculative traversal, Aila & Laine 2009):
+// a lane whose descent reaches a leaf keeps the leaf aside and goes on descending
+// until every active lane of the warp holds a leaf, then the warp tests leaves
+// together, so more lanes run the triangle tests converged. The result is
+// trace_closest4's, bit for bit:
+//   * leaves are tested in the reference's order (the waiting leaf precedes the one
+//     the descent stops at), with the reference's strict `<`;
+//   * interior nodes popped while a leaf waits are pruned against a distance that is
+//     at least the reference's at that point (the waiting leaf's hits are not in it
+//     yet), so every leaf the reference reaches is reached;
+//   * each leaf is tested only if its entry distance is below the best distance
+//     when its turn comes -- the reference's pop-time test with the same best, since
+//     both have tested the same leaves before it. A leaf the reference never reaches
+//     lies under a node the reference pruned, and its entry distance is at least that
+//     node's (a child's box lies inside its parent's and the slab arithmetic rounds
+//     monotonically), so the same test rejects it.
+constexpr int kNoRef = static_cast<int>(0x80000000u); // no leaf ref can take this value
+
+template <class Stack>
+__device__ __forceinline__ HitRec trace_closest4_spec(const SceneView &s, const RayPre &r, int ignore, int &err,
+                                                      Stack &st) {
+	const RayPair r2 = make_pair_ray(r);
+	HitRec h;
+	h.idx = -1;
+	h.rank = 0x7fffffff;
+	h.t = __int_as_float(0x7f800000);
+	h.u = 0.0f;
+	h.v = 0.0f;
+	int sp = 0;
+	int cur = kNoRef, leaf = kNoRef;
+	float cur_te = 0.0f, leaf_te = 0.0f;
+	{
+		float te;
+		if (s.n_tris > 0 &&
+		    slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te)) {
+			cur = s.root4_ref;
+			cur_te = te;
+		}
+	}
+	// next entry of the stack that survives the reference's pop-time test
+	auto pop = [&]() {
+		while (sp > 0) {
+			const unsigned long long e = st.get(--sp);
+			const float te = __int_as_float(static_cast<int>(e >> 32));
+			if (te < h.t) {
+				cur = static_cast<int>(static_cast<unsigned>(e));
+				cur_te = te;
+				return;
+			}
+		}
+		cur = kNoRef;
+	};
+	for (;;) {
+		// Interior nodes. A leaf reached while another waits ends the loop; so does
+		// every active lane holding a leaf.
+		while (cur >= 0) {
+			if (bad_node(s, cur, true)) {
+				err = 1;
+				return h;
+			}
+			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(cur);
+			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
+			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
+			const ulonglong2 z01 = __ldg(nq + 4), z23 = __ldg(nq + 5);
+			const float4 rf = __ldg(nd + 6);
+			const int cnt = __float_as_int(__ldg(nd + 7).x);
+			float t0, t1, t2, t3;
+			const bool b0 = slab2(x01.x, y01.x, z01.x, r2, t0);
+			const bool b1 = slab2(x01.y, y01.y, z01.y, r2, t1);
+			const bool b2 = cnt > 2 && slab2(x23.x, y23.x, z23.x, r2, t2);
+			const bool b3 = cnt > 3 && slab2(x23.y, y23.y, z23.y, r2, t3);
+			if (sp + 3 > kStack) {
+				err = 1;
+				return h;
+			}
+			if (b3)
+				st.put(sp++, pack_entry(__float_as_int(rf.w), t3));
+			if (b2)
+				st.put(sp++, pack_entry(__float_as_int(rf.z), t2));
+			if (b1)
+				st.put(sp++, pack_entry(__float_as_int(rf.y), t1));
+			if (b0 && t0 < h.t) {
+				cur = __float_as_int(rf.x);
+				cur_te = t0;
+			} else {
+				pop();
+			}
+			if (cur < 0 && cur != kNoRef && leaf == kNoRef) { // keep the leaf aside, descend on
+				leaf = cur;
+				leaf_te = cur_te;
+				pop();
+			}
+			if (__all_sync(__activemask(), leaf != kNoRef))
+				break;
+		}
+		// Leaves, in the reference's order: the waiting leaf, then the one the descent
+		// stopped at (if any).
+		if (leaf == kNoRef && cur < 0 && cur != kNoRef) {
+			leaf = cur;
+			leaf_te = cur_te;
+			pop();
+		}
+		while (leaf != kNoRef) {
+			if (leaf_te < h.t) { // the reference's pop-time test, with the current best
+				const int start = leaf_start(leaf);
+				const int count = leaf_count(leaf);
+				if (bad_leaf(s, start, count)) {
+					err = 1;
+					return h;
+				}
+				for (int p = start; p < start + count; p++) {
+					const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
+					const float4 a = __ldg(tp + 0);
+					const int ti = __float_as_int(a.w);
+					if (ti == ignore)
+						continue;
+					const float4 b = __ldg(tp + 1);
+					const float4 c = __ldg(tp + 2);
+					float t, u, v;
+					if (tri_test(a, b, c, r, t, u, v) && t < h.t) {
+						h.idx = ti;
+						h.t = t;
+						h.u = u;
+						h.v = v;
+						h.rank = __float_as_int(b.w);
+					}
+				}
+			}
+			leaf = kNoRef;
+			if (cur < 0 && cur != kNoRef) {
+				leaf = cur;
+				leaf_te = cur_te;
+				pop();
+			}
+		}
+		if (cur == kNoRef)
+			break;
+	}
+	return h;
+}
+
 __device__ __forceinline__ HitRec trace_closest4(const SceneView &s, const RayPre &r, int ignore, int &err) {
 	LocalStack<unsigned long long> st;
 	return trace_closest4(s, r, ignore, err, st);
