@@ -452,19 +452,11 @@ def read_peaks(lib, stream, sptr) -> dict:
 
 
 def kernel_profile():
-    """ncu figures of the traversal kernels (instructions, lanes per instruction, issue
-    activity, DRAM bytes per sample of the frame), committed under profiles/."""
+    """ncu figures of the frame's stage kernels (instructions, lanes per instruction,
+    issue activity, DRAM bytes per sample), committed under profiles/ from a capture of
+    the same scene and wave configuration at 480x270; per-sample traffic is set by the
+    scene, the path pool and the wave, which the autotuner chooses alike at both sizes."""
     path = os.path.join(ROOT, "profiles", "traversal_kernels.json")
-    if not os.path.isfile(path):
-        return None
-    with open(path) as f:
-        return json.load(f)
-
-
-def profiled_traffic():
-    """DRAM bytes per sample of the timed frame (all of its kernels), from the committed ncu
-    capture of a smaller frame of the same scene."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.isfile(path):
         return None
     with open(path) as f:
@@ -685,16 +677,16 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     kernel_ms = float(np.mean(render_ms))
     achieved = bytes_per_sample * samples_per_step / (kernel_ms / 1e3) / 1e9
-    tr = profiled_traffic()
-    traffic = None
-    if tr and tr.get("bytes_per_sample"):
-        traffic = tr["bytes_per_sample"] * samples_per_step
+    kp = kernel_profile() or {}
+    # DRAM bytes of the frame's three stage kernels (about 93 % of its device time),
+    # per sample from the committed ncu capture of the same scene at 480x270
+    stage_bps = sum(kp[k]["dram_bytes_per_sample"] for k in ("k_wf_extend", "k_wf_shadow", "k_wf_shade") if k in kp)
+    traffic = stage_bps * samples_per_step if stage_bps else None
     # Traversal kernels against the level that holds their working set (the 4-wide tree
     # and the triangles, ~150 MB, mostly L1/L2-resident): algorithmic bytes of the
     # reference traversal per stage over the stage's device time.
     ext_bps = (24.0 * counts["closest_boxes"] + 36.0 * counts["closest_tris"]) / counts["samples"]
     sh_bps = (24.0 * counts["any_boxes"] + 36.0 * counts["any_tris"]) / counts["samples"]
-    kp = kernel_profile() or {}
     per_kernel = {}
     for name, bps, ms_key in (("k_wf_extend", ext_bps, "extend_ms"), ("k_wf_shadow", sh_bps, "shadow_ms")):
         ms = stages[ms_key]
@@ -704,7 +696,7 @@ def run_ours(args):
                "frac_of_l2_read": gbs / peaks["l2_read_gbs"] if gbs else None,
                "frac_of_hbm": gbs / peak if gbs else None}
         if name in kp:
-            ent["ncu"] = kp[name]
+            ent["ncu"] = {k: v for k, v in kp[name].items() if k != "per_launch"}
         per_kernel[name] = ent
     top = per_kernel["k_wf_extend"]
     top_traffic = None
@@ -730,11 +722,17 @@ def run_ours(args):
                      "kernel_ms_per_launch": top["ms_per_frame"] / args.depth,
                      "hbm": {"peak": peak, "peak_kind": peak_kind, "frac": top["frac_of_hbm"],
                              "read_probe_gbs": peaks["hbm_read_gbs"]},
+                     "issue": ({"bound_by": "instruction issue (see profiles/traversal_kernels_*.md)",
+                                "issue_active_pct": kp["k_wf_extend"]["issue_active_pct"],
+                                "issue_active_pct_bounces_0_2": float(np.mean(
+                                    [l["issue_pct"] for l in kp["k_wf_extend"]["per_launch"][:3]])),
+                                "threads_per_instruction": kp["k_wf_extend"]["threads_per_instruction"]}
+                               if "k_wf_extend" in kp else None),
                      "per_kernel": per_kernel,
                      "stages_ms": stages,
                      "frame": {"achieved": achieved, "bytes_per_sample": bytes_per_sample, "kernel_ms": kernel_ms,
                                "frac_of_l2_read": achieved / peaks["l2_read_gbs"], "frac_of_hbm": achieved / peak,
-                               "dram_traffic": traffic},
+                               "dram_traffic_stage_kernels": traffic},
                      "probes": peaks},
         "time_to_rmse": t_rmse,
         "clocks": clk,

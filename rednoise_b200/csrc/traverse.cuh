@@ -909,6 +909,91 @@ __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, 
 	return false;
 }
 
+// trace_any4 with postponed leaves (the closest-hit version's scheme): occlusion
+// does not depend on the order in which a fixed tree's reachable leaves are tested,
+// so the result is trace_any4's.
+template <class Stack>
+__device__ __forceinline__ bool trace_any4_spec(const SceneView &s, const RayPre &r, float tmax, int ignore,
+                                                int &err, Stack &st) {
+	const RayPair r2 = make_pair_ray(r);
+	int sp = 0;
+	int cur = kNoRef, leaf = kNoRef;
+	float te;
+	if (s.n_tris > 0 && slab(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r, te) &&
+	    te < tmax)
+		cur = s.root4_ref;
+	auto pop = [&]() { cur = sp > 0 ? st.get(--sp) : kNoRef; };
+	for (;;) {
+		while (cur >= 0) {
+			if (bad_node(s, cur, true)) {
+				err = 1;
+				return false;
+			}
+			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(cur);
+			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
+			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
+			const ulonglong2 z01 = __ldg(nq + 4), z23 = __ldg(nq + 5);
+			const float4 rf = __ldg(nd + 6);
+			const int cnt = __float_as_int(__ldg(nd + 7).x);
+			float t0, t1, t2, t3;
+			const bool b0 = slab2(x01.x, y01.x, z01.x, r2, t0) && t0 < tmax;
+			const bool b1 = slab2(x01.y, y01.y, z01.y, r2, t1) && t1 < tmax;
+			const bool b2 = cnt > 2 && slab2(x23.x, y23.x, z23.x, r2, t2) && t2 < tmax;
+			const bool b3 = cnt > 3 && slab2(x23.y, y23.y, z23.y, r2, t3) && t3 < tmax;
+			if (sp + 3 > kStack) {
+				err = 1;
+				return false;
+			}
+			if (b3)
+				st.put(sp++, __float_as_int(rf.w));
+			if (b2)
+				st.put(sp++, __float_as_int(rf.z));
+			if (b1)
+				st.put(sp++, __float_as_int(rf.y));
+			if (b0)
+				cur = __float_as_int(rf.x);
+			else
+				pop();
+			if (cur < 0 && cur != kNoRef && leaf == kNoRef) {
+				leaf = cur;
+				pop();
+			}
+			if (__all_sync(__activemask(), leaf != kNoRef))
+				break;
+		}
+		if (leaf == kNoRef && cur < 0 && cur != kNoRef) {
+			leaf = cur;
+			pop();
+		}
+		while (leaf != kNoRef) {
+			const int start = leaf_start(leaf);
+			const int count = leaf_count(leaf);
+			if (bad_leaf(s, start, count)) {
+				err = 1;
+				return false;
+			}
+			for (int p = start; p < start + count; p++) {
+				const float4 *tp = s.tris + 3 * static_cast<size_t>(p);
+				const float4 a = __ldg(tp + 0);
+				if (__float_as_int(a.w) == ignore)
+					continue;
+				const float4 b = __ldg(tp + 1);
+				const float4 c = __ldg(tp + 2);
+				float t, u, v;
+				if (tri_test(a, b, c, r, t, u, v) && t < tmax)
+					return true;
+			}
+			leaf = kNoRef;
+			if (cur < 0 && cur != kNoRef) {
+				leaf = cur;
+				pop();
+			}
+		}
+		if (cur == kNoRef)
+			return false;
+	}
+}
+
 __device__ __forceinline__ bool trace_any4(const SceneView &s, const RayPre &r, float tmax, int ignore, int &err) {
 	LocalStack<int> st;
 	return trace_any4(s, r, tmax, ignore, err, st);

@@ -67,6 +67,9 @@ constexpr int kWfShortStack = 8;
 #ifndef RN_SPEC_EXTEND
 #define RN_SPEC_EXTEND 0
 #endif
+#ifndef RN_SPEC_SHADOW
+#define RN_SPEC_SHADOW 0
+#endif
 constexpr size_t kWfExtendSmem = static_cast<size_t>(kWfShortStack) * 128 * sizeof(unsigned long long);
 constexpr size_t kWfShadowSmem = static_cast<size_t>(kWfShortStack) * 128 * sizeof(int);
 
@@ -330,7 +333,13 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 			if constexpr (kWfShortStack > 0) {
 				extern __shared__ int wf_sh_stack[];
 				SharedShortStack<int, kWfShortStack> st(wf_sh_stack + threadIdx.x, blockDim.x);
-				occluded = trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err, st);
+#if RN_SPEC_SHADOW
+				const SceneView &sv = jobs[j].sc.sv;
+				if (sv.nodes4 && finite_inverse(r))
+					occluded = trace_any4_spec(sv, r, so.w, __float_as_int(sd.w), err, st);
+				else
+#endif
+					occluded = trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err, st);
 			} else {
 				occluded = trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err);
 			}
