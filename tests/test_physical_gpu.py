@@ -1,10 +1,12 @@
-"""GPU parity of the physical-mode megakernel against the CPU oracle.
+"""GPU parity of the physical-mode integrators against the CPU oracle.
 
-The GPU and the oracle draw the same counter-based uniforms for every path, so
-their renders are compared with common random numbers: per-pixel means agree to
-float rounding except where rounding moves a single path (tolerances below).
-Statistical checks (independent seeds, Russian roulette) use per-pixel
-confidence intervals.
+The GPU and the oracle draw the same counter-based uniforms for every path and
+compute each sample's radiance with the same IEEE float operations in the same
+order (no multiply-add contraction on either side), so with common random numbers
+a frame equals the oracle's per-sample radiance summed in float in sample order and
+scaled by 1 / spp, bit for bit. Statistical checks (independent seeds, Russian
+roulette, the FP64 estimator) use per-pixel confidence intervals or relative
+tolerances.
 """
 import numpy as np
 import pytest
@@ -45,6 +47,26 @@ def crn_agree(gpu_mean, orc_mean, rel_l1=2e-3, pix_frac=0.01):
     return l1, frac
 
 
+def oracle_frame(sc, c, spp, depth, rr, seed=1, offset=0):
+    """The oracle's FP32 frame as the GPU forms it: each sample's radiance (a one-sample
+    sum in double holds the float exactly), summed in float32 in sample order, times
+    the float 1 / spp."""
+    orc = oracle.OrcPhysScene(sc)
+    acc = np.zeros((c["width"] * c["height"], 3), np.float32)
+    for k in range(spp):
+        one = orc.render_sums(c, 1, depth, rr, seed=seed, offset=offset + k)
+        assert np.array_equal(one.astype(np.float32).astype(np.float64), one)
+        acc = (acc + one.astype(np.float32)).astype(np.float32)
+    return (acc * (np.float32(1.0) / np.float32(spp))).astype(np.float32)
+
+
+def bit_equal(gpu, want):
+    g = np.ascontiguousarray(gpu, np.float32).reshape(-1, 3)
+    w = np.ascontiguousarray(want, np.float32).reshape(-1, 3)
+    bad = np.any(g.view(np.uint32) != w.view(np.uint32), axis=1)
+    assert not bad.any(), (int(bad.sum()), np.nonzero(bad)[0][:8], g[bad][:3], w[bad][:3])
+
+
 @pytest.fixture(scope="module")
 def box():
     return scenes.cornell_box()
@@ -55,9 +77,8 @@ def test_cornell_box_matches_oracle_crn(box):
     c = cam(64, 48)
     spp, depth = 32, 5
     g = gpu_render(s, c, spp, depth)
-    o = oracle.OrcPhysScene(box).render_sums(c, spp, depth, depth, seed=1) / spp
     assert g.mean() > 0
-    crn_agree(g, o)
+    bit_equal(g, oracle_frame(box, c, spp, depth, depth))
 
 
 def test_fp64_oracle_agrees(box):
@@ -69,13 +90,14 @@ def test_fp64_oracle_agrees(box):
     crn_agree(g, o, rel_l1=5e-3, pix_frac=0.03)
 
 
-def test_mixed_materials_match_oracle_crn():
+@pytest.mark.parametrize("integrator", [1, 2])
+def test_mixed_materials_match_oracle_crn(integrator):
+    """Lambert, GGX and dielectric triangles, roulette from vertex 3: bit for bit."""
     sc = scenes.icosphere_scene(level=3)
     s = make_scene(sc)
     c = cam(64, 48)
-    g = gpu_render(s, c, 16, 8, rr=3)
-    o = oracle.OrcPhysScene(sc).render_sums(c, 16, 8, 3, seed=1) / 16
-    crn_agree(g, o, rel_l1=1e-2, pix_frac=0.05)
+    g = gpu_render(s, c, 16, 8, rr=3, integrator=integrator)
+    bit_equal(g, oracle_frame(sc, c, 16, 8, 3))
 
 
 def test_reference_order_equals_nearest_order_renders(box):
@@ -131,11 +153,11 @@ def test_wavefront_equals_megakernel(nearest):
     c = cam(64, 48)
     a = gpu_render(s, c, 12, 8, rr=3, nearest=nearest, integrator=1)
     b = gpu_render(s, c, 12, 8, rr=3, nearest=nearest, integrator=2)
-    crn_agree(b, a, rel_l1=1e-5, pix_frac=1e-3)
+    bit_equal(b, a)
     # a second wavefront frame replays the captured graph with new sample indices
     b2 = gpu_render(s, c, 12, 8, rr=3, nearest=nearest, integrator=2, offset=12)
     a2 = gpu_render(s, c, 12, 8, rr=3, nearest=nearest, integrator=1, offset=12)
-    crn_agree(b2, a2, rel_l1=1e-5, pix_frac=1e-3)
+    bit_equal(b2, a2)
     assert not np.array_equal(a, a2)
 
 
@@ -149,8 +171,8 @@ def test_wavefront_static_and_refetch_agree():
     a = s.render_physical(camera, st)
     b = s.render_physical(camera, st, wavefront_static=True)
     m = s.render_physical(camera, rn.Settings.make(spp=8, max_depth=8, rr_depth=3, seed=4, integrator=1))
-    crn_agree(a, b, rel_l1=1e-5, pix_frac=1e-3)
-    crn_agree(a, m, rel_l1=1e-5, pix_frac=1e-3)
+    bit_equal(a, b)
+    bit_equal(a, m)
 
 
 @pytest.mark.parametrize("static,level,w,h,spp", [(False, 3, 64, 48, 8), (True, 3, 64, 48, 8),
@@ -169,7 +191,7 @@ def test_ray_binning_changes_no_path(static, level, w, h, spp):
     binned = s.render_physical(camera, st, wavefront_static=static, ray_sort=True)
     assert np.array_equal(plain.view(np.uint32), binned.view(np.uint32))
     m = s.render_physical(camera, rn.Settings.make(spp=spp, max_depth=8, rr_depth=3, seed=6, integrator=1))
-    crn_agree(binned, m, rel_l1=1e-5, pix_frac=1e-3)
+    bit_equal(binned, m)
     # a second binned frame replays the captured graph
     binned2 = s.render_physical(camera, st, wavefront_static=static, ray_sort=True)
     assert np.array_equal(binned.view(np.uint32), binned2.view(np.uint32))
@@ -184,15 +206,14 @@ def test_autotune_reports_ray_binning():
     assert t["ray_sort"] in (0, 1) and t["integrator"] in (1, 2)
     a = s.render_physical(camera, rn.Settings.make(spp=8, max_depth=6, seed=1))
     b = s.render_physical(camera, rn.Settings.make(spp=8, max_depth=6, seed=1, integrator=1))
-    crn_agree(a, b, rel_l1=1e-5, pix_frac=1e-3)
+    bit_equal(a, b)
 
 
 def test_wavefront_matches_oracle_crn(box):
     s = make_scene(box)
     c = cam(48, 36)
     g = gpu_render(s, c, 16, 5, integrator=2)
-    o = oracle.OrcPhysScene(box).render_sums(c, 16, 5, 5, seed=1) / 16
-    crn_agree(g, o)
+    bit_equal(g, oracle_frame(box, c, 16, 5, 5))
 
 
 def test_batched_wavefront_equals_per_job_megakernel():
@@ -215,7 +236,7 @@ def test_batched_wavefront_equals_per_job_megakernel():
         assert b.integrator in (1, 2)
         outs = b.render()
         for o, r in zip(outs, refs):
-            crn_agree(o, r, rel_l1=1e-5, pix_frac=1e-3)
+            bit_equal(o, r)
         outs2 = b.render(sample_offset=1000)
         assert not np.array_equal(outs2[1], outs[1])
         b.close()
