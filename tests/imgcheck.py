@@ -38,3 +38,23 @@ def light_records(lights):
         r[19:22] = L.v_axis[:]
         out.append(r)
     return np.stack(out)
+
+
+def oracle_float_frame(orc, cam, spp, depth, rr, seed=1, offset=0):
+    """The oracle's FP32 physical-mode frame formed the way the GPU forms it: each
+    sample's radiance (a one-sample sum in double holds the float exactly), summed in
+    float32 in sample order, times the float 1 / spp; (pixels, 3) float32."""
+    acc = np.zeros((cam["width"] * cam["height"], 3), np.float32)
+    for k in range(spp):
+        one = orc.render_sums(cam, 1, depth, rr, seed=seed, offset=offset + k)
+        assert np.array_equal(one.astype(np.float32).astype(np.float64), one)
+        acc = (acc + one.astype(np.float32)).astype(np.float32)
+    return (acc * (np.float32(1.0) / np.float32(spp))).astype(np.float32)
+
+
+def assert_bit_equal(got, want):
+    """Two float images with the same bits in every channel."""
+    g = np.ascontiguousarray(got, np.float32).reshape(-1, 3)
+    w = np.ascontiguousarray(want, np.float32).reshape(-1, 3)
+    bad = np.any(g.view(np.uint32) != w.view(np.uint32), axis=1)
+    assert not bad.any(), (int(bad.sum()), np.nonzero(bad)[0][:8], g[bad][:3], w[bad][:3])

@@ -13,6 +13,7 @@ import pytest
 
 import oracle
 import rednoise_b200 as rn
+from imgcheck import assert_bit_equal, oracle_float_frame
 from rednoise_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -48,23 +49,10 @@ def crn_agree(gpu_mean, orc_mean, rel_l1=2e-3, pix_frac=0.01):
 
 
 def oracle_frame(sc, c, spp, depth, rr, seed=1, offset=0):
-    """The oracle's FP32 frame as the GPU forms it: each sample's radiance (a one-sample
-    sum in double holds the float exactly), summed in float32 in sample order, times
-    the float 1 / spp."""
-    orc = oracle.OrcPhysScene(sc)
-    acc = np.zeros((c["width"] * c["height"], 3), np.float32)
-    for k in range(spp):
-        one = orc.render_sums(c, 1, depth, rr, seed=seed, offset=offset + k)
-        assert np.array_equal(one.astype(np.float32).astype(np.float64), one)
-        acc = (acc + one.astype(np.float32)).astype(np.float32)
-    return (acc * (np.float32(1.0) / np.float32(spp))).astype(np.float32)
+    return oracle_float_frame(oracle.OrcPhysScene(sc), c, spp, depth, rr, seed=seed, offset=offset)
 
 
-def bit_equal(gpu, want):
-    g = np.ascontiguousarray(gpu, np.float32).reshape(-1, 3)
-    w = np.ascontiguousarray(want, np.float32).reshape(-1, 3)
-    bad = np.any(g.view(np.uint32) != w.view(np.uint32), axis=1)
-    assert not bad.any(), (int(bad.sum()), np.nonzero(bad)[0][:8], g[bad][:3], w[bad][:3])
+bit_equal = assert_bit_equal
 
 
 @pytest.fixture(scope="module")
