@@ -64,12 +64,6 @@ __global__ void __launch_bounds__(256) k_wf_camera(const WfJob *__restrict__ job
 // the 1.31M-triangle frame 8 and 16 entries measure the same frame rate as the
 // all-local stack: the L1-cached local stack is not what bounds these stages.
 constexpr int kWfShortStack = 8;
-#ifndef RN_SPEC_EXTEND
-#define RN_SPEC_EXTEND 0
-#endif
-#ifndef RN_SPEC_SHADOW
-#define RN_SPEC_SHADOW 0
-#endif
 constexpr size_t kWfExtendSmem = static_cast<size_t>(kWfShortStack) * 128 * sizeof(unsigned long long);
 constexpr size_t kWfShadowSmem = static_cast<size_t>(kWfShortStack) * 128 * sizeof(int);
 
@@ -97,13 +91,7 @@ __global__ void __launch_bounds__(128) k_wf_extend(const WfJob *__restrict__ job
 			if constexpr (kWfShortStack > 0) {
 				extern __shared__ unsigned long long wf_ext_stack[];
 				SharedShortStack<unsigned long long, kWfShortStack> st(wf_ext_stack + threadIdx.x, blockDim.x);
-#if RN_SPEC_EXTEND
-				const SceneView &sv = jobs[j].sc.sv;
-				if (kOrder == kOrderReference && sv.nodes4 && finite_inverse(r))
-					h = trace_closest4_spec(sv, r, __float_as_int(o.w), err, st);
-				else
-#endif
-					h = trace_closest_best<kOrder>(jobs[j].sc.sv, r, __float_as_int(o.w), err, st);
+				h = trace_closest_best<kOrder>(jobs[j].sc.sv, r, __float_as_int(o.w), err, st);
 			} else {
 				h = trace_closest_best<kOrder>(jobs[j].sc.sv, r, __float_as_int(o.w), err);
 			}
@@ -333,13 +321,7 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const WfJob *__restrict__ job
 			if constexpr (kWfShortStack > 0) {
 				extern __shared__ int wf_sh_stack[];
 				SharedShortStack<int, kWfShortStack> st(wf_sh_stack + threadIdx.x, blockDim.x);
-#if RN_SPEC_SHADOW
-				const SceneView &sv = jobs[j].sc.sv;
-				if (sv.nodes4 && finite_inverse(r))
-					occluded = trace_any4_spec(sv, r, so.w, __float_as_int(sd.w), err, st);
-				else
-#endif
-					occluded = trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err, st);
+				occluded = trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err, st);
 			} else {
 				occluded = trace_any_best(jobs[j].sc.sv, r, so.w, __float_as_int(sd.w), err);
 			}
