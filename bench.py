@@ -63,8 +63,6 @@ def parse():
                    help="bidirectional / metropolis / dropin: the small case used for profiles (160x120 at 16 spp, "
                         "400 000 mutations, 480x270 at 1 spp)")
     p.add_argument("--inverse-steps", type=int, default=200)
-    p.add_argument("--inverse-lr-final", type=float, default=None,
-                   help="inverse: cosine-decay Adam's step from 0.02 to this value (default: constant 0.02)")
     return p.parse_args()
 
 
@@ -870,7 +868,7 @@ def observed_pixels(scene, views) -> np.ndarray:
     return counts
 
 
-def measure_inverse(steps: int, lr_final=None) -> dict:
+def measure_inverse(steps: int) -> dict:
     """Multi-view albedo recovery: 16 views of the 36-triangle box at 384x384, 16 spp
     primal + 16 spp adjoint, depth 5, Adam (lr 0.02) from the unperturbed albedo
     towards targets rendered with albedo perturbed by N(0, 0.1) clipped to [0.05, 0.95].
@@ -899,8 +897,7 @@ def measure_inverse(steps: int, lr_final=None) -> dict:
                                  material=sc["material"], material_param=sc["material_param"])
     seen = observed_pixels(scene, views) > 0
     refl = sc["emission"].sum(1) == 0
-    fit = AlbedoFit(scene, views, targets, sc["albedo"], spp=16, max_depth=5, lr=0.02, lr_final=lr_final,
-                    total_steps=steps)
+    fit = AlbedoFit(scene, views, targets, sc["albedo"], spp=16, max_depth=5, lr=0.02)
     rmse0 = float(np.sqrt(((sc["albedo"][refl] - truth[refl]) ** 2).mean()))
     fit.step()  # warm-up: graph capture
     torch.cuda.synchronize()
@@ -932,8 +929,6 @@ def measure_inverse(steps: int, lr_final=None) -> dict:
     return {"metric": "ms per inverse-rendering step", "value": ms_step, "unit": "ms",
             "config": {"workload": "16 views x 384x384 of the 36-triangle box, 16 spp primal + 16 spp adjoint, "
                                    "depth 5, Adam lr 0.02 on per-triangle albedo", "adam_steps": steps,
-                       "lr_schedule": "constant 0.02" if lr_final is None else
-                                      f"cosine from 0.02 to {lr_final} over the steps",
                        "batch_integrator": {1: "megakernel", 2: "wavefront"}.get(batch_integrator, "?")},
             "albedo_rmse": {"all_reflecting": {"triangles": int(refl.sum()), "initial": rmse0,
                                                "final": rmse(alb, refl)},
@@ -947,7 +942,7 @@ def measure_inverse(steps: int, lr_final=None) -> dict:
 
 
 def run_inverse(args):
-    r = measure_inverse(args.inverse_steps, args.inverse_lr_final)
+    r = measure_inverse(args.inverse_steps)
     line = dict(r)
     line.update({"n_gpus": 1, "steps": args.inverse_steps, "warmup": 1, "higher_is_better": False, "dtype": "f32",
                  "data": "synthetic"})

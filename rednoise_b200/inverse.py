@@ -11,7 +11,6 @@ gradient estimate is unbiased for the expected loss.
 from __future__ import annotations
 
 import ctypes
-import math
 from typing import Callable, List, Optional, Sequence
 
 import numpy as np
@@ -31,8 +30,7 @@ class AlbedoFit:
     against ``targets`` (one (h, w, 3) image per view, host or CUDA)."""
 
     def __init__(self, scene, views: Sequence, targets: Sequence, albedo0, spp: int = 16, max_depth: int = 5,
-                 lr: float = 0.02, seed: int = 1, bounds=(0.01, 0.99), lr_final: Optional[float] = None,
-                 total_steps: int = 200):
+                 lr: float = 0.02, seed: int = 1, bounds=(0.01, 0.99)):
         import torch
 
         from . import Batch
@@ -51,10 +49,6 @@ class AlbedoFit:
         self.albedo = torch.as_tensor(np.asarray(albedo0, np.float32), device=dev).reshape(-1, 3).clone()
         self.albedo.requires_grad_(True)
         self.opt = torch.optim.Adam([self.albedo], lr=lr)
-        # optional cosine decay of the step size from lr to lr_final over total_steps:
-        # Adam's normalised steps keep a noisy gradient's parameters moving by about
-        # the step size, so a shrinking step lets them settle
-        self.lr, self.lr_final, self.total_steps = float(lr), lr_final, max(1, int(total_steps))
         self.images = [torch.empty(c.height * c.width * 3, device=dev) for c in self.cams]
         self.d_images = [torch.empty_like(i) for i in self.images]
         self.g_alb = torch.empty(self.albedo.numel(), device=dev)
@@ -107,10 +101,6 @@ class AlbedoFit:
             loss = loss / self.n_values
             self.adjoint(sample_offset=(2 * k + 1) * self.spp)
             self.albedo.grad = self.g_alb.view_as(self.albedo)
-            if self.lr_final is not None:
-                f = min(k, self.total_steps - 1) / max(self.total_steps - 1, 1)
-                for grp in self.opt.param_groups:
-                    grp["lr"] = self.lr_final + 0.5 * (self.lr - self.lr_final) * (1.0 + math.cos(math.pi * f))
             self.opt.step()
             with torch.no_grad():
                 self.albedo.clamp_(*self.bounds)
