@@ -722,7 +722,8 @@ def run_ours(args):
                      "kernel_ms_per_launch": top["ms_per_frame"] / args.depth,
                      "hbm": {"peak": peak, "peak_kind": peak_kind, "frac": top["frac_of_hbm"],
                              "read_probe_gbs": peaks["hbm_read_gbs"]},
-                     "issue": ({"bound_by": "instruction issue (see profiles/traversal_kernels_*.md)",
+                     "issue": ({"bound_by": "L1 throughput and instruction issue (profiles/traversal_kernels_*.md, "
+                                            "profiles/k_wf_extend_*.md)",
                                 "issue_active_pct": kp["k_wf_extend"]["issue_active_pct"],
                                 "issue_active_pct_bounces_0_2": float(np.mean(
                                     [l["issue_pct"] for l in kp["k_wf_extend"]["per_launch"][:3]])),
