@@ -32,10 +32,6 @@ namespace rnb {
 
 constexpr int kStack = 64; // same bound as the reference's int stack[64]
 
-#ifndef RN_LD256
-#define RN_LD256 0
-#endif
-
 struct SceneView {
 	const float4 *__restrict__ nodes;  // 4 float4 per internal node (2-wide)
 	const float4 *__restrict__ nodes4; // 8 float4 per node (4-wide collapse), may be null
@@ -410,13 +406,6 @@ __device__ __forceinline__ float min3(float a, float b, float c) {
 	return r;
 }
 
-#if RN_LD256
-// One 32-byte read-only load (sm_100's 256-bit global load): four 64-bit words.
-__device__ __forceinline__ void ld_nc_256(const void *p, unsigned long long &a, unsigned long long &b,
-                                          unsigned long long &c, unsigned long long &d) {
-	asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
-}
-#endif
 
 // The ray's origin and inverse direction duplicated into pairs.
 struct RayPair {
@@ -765,25 +754,11 @@ __device__ __forceinline__ HitRec trace_closest4_spec(const SceneView &s, const 
 				return h;
 			}
 			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(cur);
-#if RN_LD256
-			ulonglong2 x01, x23, y01, y23, z01, z23;
-			ld_nc_256(nd + 0, x01.x, x01.y, x23.x, x23.y);
-			ld_nc_256(nd + 2, y01.x, y01.y, y23.x, y23.y);
-			ld_nc_256(nd + 4, z01.x, z01.y, z23.x, z23.y);
-			unsigned long long r01, r23, c01, c23;
-			ld_nc_256(nd + 6, r01, r23, c01, c23);
-			float4 rf;
-			unpair2(r01, rf.x, rf.y);
-			unpair2(r23, rf.z, rf.w);
-			const int cnt = static_cast<int>(static_cast<unsigned>(c01));
-			(void)c23;
-#else
 			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
 			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
 			const ulonglong2 z01 = __ldg(nq + 4), z23 = __ldg(nq + 5);
 			const float4 rf = __ldg(nd + 6);
 			const int cnt = __float_as_int(__ldg(nd + 7).x);
-#endif
 			float t0, t1, t2, t3;
 			const bool b0 = slab2(x01.x, y01.x, z01.x, r2, t0);
 			const bool b1 = slab2(x01.y, y01.y, z01.y, r2, t1);
@@ -956,25 +931,11 @@ __device__ __forceinline__ bool trace_any4_spec(const SceneView &s, const RayPre
 				return false;
 			}
 			const float4 *nd = s.nodes4 + 8 * static_cast<size_t>(cur);
-#if RN_LD256
-			ulonglong2 x01, x23, y01, y23, z01, z23;
-			ld_nc_256(nd + 0, x01.x, x01.y, x23.x, x23.y);
-			ld_nc_256(nd + 2, y01.x, y01.y, y23.x, y23.y);
-			ld_nc_256(nd + 4, z01.x, z01.y, z23.x, z23.y);
-			unsigned long long r01, r23, c01, c23;
-			ld_nc_256(nd + 6, r01, r23, c01, c23);
-			float4 rf;
-			unpair2(r01, rf.x, rf.y);
-			unpair2(r23, rf.z, rf.w);
-			const int cnt = static_cast<int>(static_cast<unsigned>(c01));
-			(void)c23;
-#else
 			const ulonglong2 *nq = reinterpret_cast<const ulonglong2 *>(nd);
 			const ulonglong2 x01 = __ldg(nq + 0), x23 = __ldg(nq + 1), y01 = __ldg(nq + 2), y23 = __ldg(nq + 3);
 			const ulonglong2 z01 = __ldg(nq + 4), z23 = __ldg(nq + 5);
 			const float4 rf = __ldg(nd + 6);
 			const int cnt = __float_as_int(__ldg(nd + 7).x);
-#endif
 			float t0, t1, t2, t3;
 			const bool b0 = slab2(x01.x, y01.x, z01.x, r2, t0) && t0 < tmax;
 			const bool b1 = slab2(x01.y, y01.y, z01.y, r2, t1) && t1 < tmax;
