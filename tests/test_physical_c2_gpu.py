@@ -22,6 +22,7 @@ import numpy as np
 import pytest
 
 import oracle
+import raysets
 import rednoise_b200 as rn
 from rednoise_b200 import _native, scenes
 
@@ -117,3 +118,103 @@ def test_c2_within_confidence_of_fp64(c2):
     # the subset's mean level: within 4 standard errors of the FP64 level
     se = np.sqrt((var + c2["fp64_var"]).sum()) / mean.size
     assert abs(mean.mean() - c2["fp64_mean"].mean()) < 4 * se, (mean.mean(), c2["fp64_mean"].mean(), se)
+
+
+def test_c2_hits_match_the_reference_bvh(c2):
+    """The reference's own BVH (src/BVH.cpp built from its sources, oracle/_ref) over the
+    1.31M-triangle scene against the GPU's speculative 4-wide traversal: 60 000 seeded
+    rays -- aimed at random points of random triangles (15 % at edges and vertices)
+    from inside the room, and secondary rays from their hit points in random
+    directions ignoring the hit triangle -- closest-hit index, t, u, v bit for bit,
+    and occlusion of shadow rays towards the emitter identical."""
+    if not oracle.ref_available():
+        pytest.skip("reference build absent")
+    sc = c2["sc"]
+    v9 = sc["vertices"]
+    ref = oracle.RefModel.from_arrays(v9, sc["ref_rgb"], sc["ref_material"], sc["ref_roughness"])
+    o1, d1 = raysets.towards_rays(30000, 31, v9, (-2.5, -2.5, -2.5), (2.5, 2.5, 2.5))
+    s = c2["s"]
+    idx, t, u, v = s.trace_closest(o1, d1)
+    ri, rt, ru, rv = ref.intersect(o1, d1)
+    assert np.array_equal(idx, ri), np.nonzero(idx != ri)[0][:8]
+    assert np.array_equal(t.view(np.uint32), rt.view(np.uint32))
+    assert np.array_equal(u.view(np.uint32), ru.view(np.uint32))
+    assert np.array_equal(v.view(np.uint32), rv.view(np.uint32))
+    hit = idx >= 0
+    assert hit.mean() > 0.9
+    rng = np.random.default_rng(32)
+    p = (o1[hit] + d1[hit] * t[hit, None]).astype(np.float32)
+    d2 = rng.normal(size=p.shape).astype(np.float32)
+    d2 = scenes.glm_normalize(d2)
+    ig = idx[hit].astype(np.int32)
+    idx2, t2, _, _ = s.trace_closest(p, d2, ignore=ig)
+    ri2, rt2, _, _ = ref.intersect(p, d2, ignore=ig)
+    assert np.array_equal(idx2, ri2) and np.array_equal(t2.view(np.uint32), rt2.view(np.uint32))
+    # shadow rays to random points of the emitter
+    em = np.nonzero(sc["emission"].sum(1) > 0)[0]
+    e = v9[rng.choice(em, size=p.shape[0])].reshape(-1, 3, 3).astype(np.float64)
+    w = rng.random((p.shape[0], 3))
+    w /= w.sum(1, keepdims=True)
+    q = (e * w[:, :, None]).sum(1)
+    dd = q - p
+    dist = np.linalg.norm(dd, axis=1)
+    d3 = scenes.glm_normalize(dd.astype(np.float32))
+    tmax = (dist * 0.999).astype(np.float32)
+    occ = s.trace_any(p, d3, tmax, ignore=ig)
+    rocc = ref.occluded(p, d3, tmax, ignore=ig)
+    assert np.array_equal(np.asarray(occ).astype(bool), np.asarray(rocc).astype(bool))
+    assert 0.05 < np.mean(occ) < 0.95
+
+
+def test_c2_albedo_gradient_matches_central_differences(c2):
+    """The gradient the bench times -- d loss / d albedo over all 1,310,756 x 3 albedos
+    of the 1.31M-triangle scene at 512x512, 32 spp, depth 6 -- against central
+    differences (eps 1e-3, common random numbers, roulette off so the fixed-sample
+    estimator is a polynomial in the albedo) on 16 seeded parameters of the room's
+    wall and box triangles, each within 2 %. The sphere's triangles cover a tenth of
+    a pixel each at this size, so their differences drown in the float rounding of
+    the 786 432-value loss; they are checked against the FP64 oracle's gradient in
+    tests/test_adjoint_gpu.py instead."""
+    sc = c2["sc"]
+    s = c2["s"]
+    cam = scenes.camera(512, 512)
+    camera = rn.Camera.make(cam["position"], cam["target"], cam["up"], cam["vfov_deg"], 512, 512)
+    st = rn.Settings.make(spp=32, max_depth=6, rr_depth=6, seed=3, integrator=_native.RN_PT_MEGAKERNEL)
+    room = np.nonzero(sc["emission"][:36].sum(1) == 0)[0]
+    rng = np.random.default_rng(0x5EED0004)
+    alb_t = sc["albedo"].copy()
+    alb_t[room] = np.clip(alb_t[room] + rng.normal(0, 0.1, (room.size, 3)), 0.05, 0.95)
+    s.set_materials(albedo=alb_t)
+    target = s.render_physical(camera, st).astype(np.float64)
+    s.set_materials(albedo=sc["albedo"])
+
+    def loss():
+        img = s.render_physical(camera, st).astype(np.float64)
+        return ((img - target) ** 2).sum(), 2 * (img - target)
+
+    try:
+        L0, dI = loss()
+        ga, _ = s.backward([(camera, st)], [dI.astype(np.float32)])
+        assert ga.shape == (sc["vertices"].shape[0], 3)
+        cand = [(int(t), c) for t in room for c in range(3)]
+        pick = np.random.default_rng(16).permutation(len(cand))[:16]
+        eps = 1e-3
+        errs = []
+        for i in pick:
+            tri, ch = cand[i]
+            alb = sc["albedo"].copy()
+            alb[tri, ch] += eps
+            s.set_materials(albedo=alb)
+            Lp, _ = loss()
+            alb[tri, ch] -= 2 * eps
+            s.set_materials(albedo=alb)
+            Lm, _ = loss()
+            fd = (Lp - Lm) / (2 * eps)
+            if fd == 0.0:
+                assert ga[tri, ch] == 0.0
+                continue
+            errs.append((abs(fd - ga[tri, ch]) / abs(fd), tri, ch, fd, float(ga[tri, ch])))
+        assert len(errs) >= 12
+        assert max(errs)[0] < 0.02, sorted(errs)[-3:]
+    finally:
+        s.set_materials(albedo=sc["albedo"])
