@@ -202,7 +202,10 @@ __device__ __forceinline__ F3 adj_weight(const WfJob &job, uint32_t pixel) {
 // the bench frame with the same image; tighter caps spilled and changed how ptxas
 // fused multiply-adds.
 template <bool kAdj>
-__global__ void __launch_bounds__(128, 5) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
+#ifndef RN_SHADE_MINB
+#define RN_SHADE_MINB 5
+#endif
+__global__ void __launch_bounds__(128, RN_SHADE_MINB) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
                                                   const int *__restrict__ q, int write_keys, int *status) {
 	const unsigned n = pool.counters[kCntRays + k];
 	int *__restrict__ qn = pool.queue[(k + 1) & 1];
