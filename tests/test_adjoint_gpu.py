@@ -210,9 +210,34 @@ def test_multi_view_backward_sums_views(setup):
     assert np.allclose(e12, e1 + e2, rtol=1e-4, atol=1e-7)
 
 
+def _seen_triangles(scene, views):
+    """Triangles that some view's pixel-centre primary ray hits first."""
+    counts = np.zeros(scene.triangle_count, np.int64)
+    for v in views:
+        w, h = v["width"], v["height"]
+        pos = np.asarray(v["position"], np.float64)
+        f = np.asarray(v["target"], np.float64) - pos
+        f /= np.linalg.norm(f)
+        r = np.cross(f, np.asarray(v["up"], np.float64))
+        r /= np.linalg.norm(r)
+        u = np.cross(r, f)
+        th = np.tan(np.radians(v["vfov_deg"]) / 2)
+        ys, xs = np.mgrid[0:h, 0:w]
+        sx = ((xs + 0.5) / w) * 2 - 1
+        sy = 1 - ((ys + 0.5) / h) * 2
+        d = f + r * (sx * th * (w / h))[..., None] + u * (sy * th)[..., None]
+        d /= np.linalg.norm(d, axis=-1, keepdims=True)
+        idx, _, _, _ = scene.trace_closest(np.broadcast_to(pos, d.shape).reshape(-1, 3), d.reshape(-1, 3))
+        counts += np.bincount(idx[idx >= 0], minlength=counts.size)
+    return counts > 0
+
+
 def test_inverse_rendering_recovers_albedo():
-    """A few dozen Adam steps over 4 views move the box's albedo towards the
-    perturbed albedo the targets were rendered with."""
+    """60 Adam steps over 4 views bring the albedo of every triangle a view sees
+    directly to the perturbed albedo the targets were rendered with (mean error down
+    to under 35 % of its start; the CPU oracle running the same fit reaches 17 %),
+    while the triangles no view sees (the boxes' bottoms, backs and wall-facing
+    sides) reach the images only through interreflection and barely move."""
     from rednoise_b200.inverse import AlbedoFit
 
     sc = scenes.cornell_box(light_scale=4.0)
@@ -227,15 +252,15 @@ def test_inverse_rendering_recovers_albedo():
         targets.append(tgt_scene.render_physical(cam, rn.Settings.make(spp=512, max_depth=4, seed=9)))
     scene = rn.Scene.from_arrays(sc["vertices"], albedo=sc["albedo"], emission=sc["emission"],
                                  material=sc["material"], material_param=sc["material_param"])
+    seen = _seen_triangles(scene, views) & (sc["emission"].sum(1) == 0)
+    assert seen.sum() >= 12
     fit = AlbedoFit(scene, views, targets, sc["albedo"], spp=32, max_depth=4, lr=0.02)
     losses = fit.run(60)
     alb = fit.albedo.detach().cpu().numpy()
     fit.close()
-    moved = np.abs(alb - sc["albedo"]).sum(1) > 1e-4
-    assert moved.sum() >= 8
-    err0 = np.abs(sc["albedo"][moved] - truth[moved]).mean()
-    err1 = np.abs(alb[moved] - truth[moved]).mean()
-    assert err1 < 0.8 * err0, (err0, err1)
+    err0 = np.abs(sc["albedo"][seen] - truth[seen]).mean()
+    err1 = np.abs(alb[seen] - truth[seen]).mean()
+    assert err1 < 0.35 * err0, (err0, err1)
     assert np.mean(losses[-10:]) < np.mean(losses[:5])
 
 
