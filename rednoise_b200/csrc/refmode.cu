@@ -371,8 +371,27 @@ __global__ void __launch_bounds__(128) k_ref_shadow(SceneView sv, const RefParam
 		const float4 r0 = dv.rec[3 * ri], r1 = dv.rec[3 * ri + 1];
 		const V3 point = mk(r0.x, r0.y, r0.z);
 		const VisTaps T = vis_taps(p.lights[l], point);
+		// At a diffuse level, directLight multiplies this light's visibility by its
+		// cone and incidence terms (direct_light_recorded, the same expressions): where
+		// either is zero the light adds vis * 0 whatever the visibility, so its taps
+		// need no ray. On the 1.31M-triangle 1080p x 2 spp frame this took the frame
+		// from 35.2 to 31.1 ms with a bit-identical canvas (points on the lower half
+		// of the sphere face away from the default light).
+		bool needed = true;
+		const int kind = __float_as_int(r0.w);
+		if (kind == kLvDiffuse || kind == kLvDiffuseEnd) {
+			const RefLight &L = p.lights[l];
+			V3 ld;
+			float atten;
+			light_dir(L, point, ld, atten);
+			float cone = 1.0f;
+			if (L.type == kLightSpot)
+				cone = (dot(-ld, normalize(l3(L.direction))) > L.cone_cos) ? 1.0f : 0.0f;
+			const float incidence = smax(0.0f, dot(mk(r1.x, r1.y, r1.z), ld));
+			needed = cone != 0.0f && incidence != 0.0f;
+		}
 		uint8_t occ = 0;
-		if (!T.all_visible) {
+		if (!T.all_visible && needed) {
 			V3 dir;
 			float dist;
 			vis_tap(T, point, k, dir, dist);
