@@ -406,6 +406,55 @@ void flatten_bvh4(const Bvh2 &bvh, DeviceLayout4 &out) {
 		out.root_ref = leaf_ref(root);
 		return;
 	}
+	// Which reference levels become 4-wide nodes. Every node spans two reference
+	// levels at most, and any such frontier gives the same traversal result, so the
+	// choice only moves cost: each 4-wide node costs one fetch per ray that reaches
+	// it, about in proportion to its box's surface area. Bottom-up over the tree,
+	// F(n) = area(n) + sum over n's children c of G(c) is the cost below n when n
+	// roots a 4-wide node, and G(c) = min(F(c), F of c's internal children) picks,
+	// per internal child, between keeping it as an entry and splicing its two
+	// children in. On a complete tree of odd height this puts the 4-wide nodes at
+	// even heights above the leaves (all nodes full, about half as many) where a
+	// top-down collapse leaves the bottom level half empty.
+	const size_t nn = bvh.nodes.size();
+	std::vector<double> cost_root(nn, 0.0), cost_best(nn, 0.0);
+	std::vector<char> splice(nn, 0);
+	{
+		auto area = [](const BvhNode &nd) {
+			const double x = std::max(0.0, static_cast<double>(nd.bmax.x) - nd.bmin.x);
+			const double y = std::max(0.0, static_cast<double>(nd.bmax.y) - nd.bmin.y);
+			const double z = std::max(0.0, static_cast<double>(nd.bmax.z) - nd.bmin.z);
+			return x * y + y * z + z * x;
+		};
+		std::vector<int> pre; // pre-order; walked backwards, children come before parents
+		std::vector<int> st{bvh.root};
+		while (!st.empty()) {
+			const int i = st.back();
+			st.pop_back();
+			pre.push_back(i);
+			const BvhNode &nd = bvh.nodes[static_cast<size_t>(i)];
+			if (nd.count == 0) {
+				st.push_back(nd.left);
+				st.push_back(nd.right);
+			}
+		}
+		auto internal_root_cost = [&](int c) {
+			return bvh.nodes[static_cast<size_t>(c)].count > 0 ? 0.0 : cost_root[static_cast<size_t>(c)];
+		};
+		for (size_t k = pre.size(); k-- > 0;) {
+			const int i = pre[k];
+			const BvhNode &nd = bvh.nodes[static_cast<size_t>(i)];
+			if (nd.count > 0)
+				continue;
+			const size_t l = static_cast<size_t>(nd.left), r = static_cast<size_t>(nd.right);
+			const bool leaf_l = bvh.nodes[l].count > 0, leaf_r = bvh.nodes[r].count > 0;
+			cost_root[static_cast<size_t>(i)] =
+			    area(nd) + (leaf_l ? 0.0 : cost_best[l]) + (leaf_r ? 0.0 : cost_best[r]);
+			const double spliced = internal_root_cost(nd.left) + internal_root_cost(nd.right);
+			splice[static_cast<size_t>(i)] = spliced < cost_root[static_cast<size_t>(i)];
+			cost_best[static_cast<size_t>(i)] = std::min(cost_root[static_cast<size_t>(i)], spliced);
+		}
+	}
 	// Iterative build: each work item fills node `slot` from reference node `src`.
 	std::vector<std::pair<int, int>> work; // (slot, src)
 	out.nodes.resize(8);
@@ -419,7 +468,7 @@ void flatten_bvh4(const Bvh2 &bvh, DeviceLayout4 &out) {
 		int cnt = 0;
 		for (int c : {n.right, n.left}) {
 			const BvhNode &cn = bvh.nodes[static_cast<size_t>(c)];
-			if (cn.count > 0) {
+			if (cn.count > 0 || !splice[static_cast<size_t>(c)]) {
 				ent[cnt++] = c;
 			} else {
 				ent[cnt++] = cn.right;

@@ -3,6 +3,7 @@
 // loader on well-formed and malformed files, the reference-identical BVH build
 // (including its threaded top levels) on random, degenerate and coincident
 // triangles, and both device-layout flattenings, with the tree invariants checked.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -110,6 +111,63 @@ static void check_layouts(const std::vector<float> &v, const Bvh2 &b) {
 		for (int k = 0; k < cnt && k < 4; k++)
 			CHECK(ref_ok(rr[k], n4));
 	}
+	// With every box passing, the 4-wide layout pops the reference's leaves in the
+	// reference's own order (right child first), each exactly once.
+	std::vector<int> want, got;
+	std::vector<int> st{b.root};
+	while (!st.empty()) {
+		const BvhNode &nd = b.nodes[static_cast<size_t>(st.back())];
+		st.pop_back();
+		if (nd.count > 0) {
+			want.push_back(~((nd.start << 3) | nd.count));
+		} else {
+			st.push_back(nd.left);
+			st.push_back(nd.right);
+		}
+	}
+	st.assign(1, l4.root_ref);
+	size_t guard = 0;
+	while (!st.empty() && guard++ < 8 * want.size() + 8) {
+		const int r = st.back();
+		st.pop_back();
+		if (r < 0) {
+			got.push_back(r);
+			continue;
+		}
+		CHECK(r < n4);
+		if (r >= n4)
+			break;
+		const F4 *o = &l4.nodes[8 * static_cast<size_t>(r)];
+		const int cnt = as_int(o[7].x);
+		const int rr[4] = {as_int(o[6].x), as_int(o[6].y), as_int(o[6].z), as_int(o[6].w)};
+		for (int k = std::min(cnt, 4); k-- > 0;)
+			st.push_back(rr[k]);
+	}
+	CHECK(got == want);
+}
+
+// A complete tree of odd height collapses into full 4-wide nodes only, apart from
+// the root: 512 triangles in a row give 2^7 leaves of 4 under a tree of height 7,
+// and 1 + 2 + 8 + 32 = 43 nodes (a top-down collapse gives 1 + 4 + 16 + 64 = 85,
+// the last 64 with two entries).
+static void complete_tree_case() {
+	std::vector<float> v;
+	for (int i = 0; i < 512; i++) {
+		const float x = static_cast<float>(i);
+		const float t[9] = {x, 0.0f, 0.0f, x + 0.5f, 1.0f, 0.0f, x + 0.25f, 0.0f, 1.0f};
+		v.insert(v.end(), t, t + 9);
+	}
+	Bvh2 b;
+	build_reference_bvh(v.data(), 512, b);
+	DeviceLayout4 l4;
+	flatten_bvh4(b, l4);
+	const int n4 = static_cast<int>(l4.nodes.size() / 8);
+	int full = 0;
+	for (int i = 0; i < n4; i++)
+		full += as_int(l4.nodes[8 * static_cast<size_t>(i) + 7].x) == 4;
+	CHECK(b.depth == 8);
+	CHECK(n4 == 43);
+	CHECK(full == 42);
 }
 
 static void tree_case(const std::vector<float> &v) {
@@ -186,6 +244,7 @@ int main(int argc, char **argv) {
 	std::vector<float> same(9 * 50, 0.5f); // every centroid equal, zero-area triangles
 	tree_case(same);
 	tree_case(soup(300000, 5u, 1.0f)); // large enough for the threaded top levels
+	complete_tree_case();
 	std::printf(g_fail ? "FAILED\n" : "host checks passed\n");
 	return g_fail;
 }
