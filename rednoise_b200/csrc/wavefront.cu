@@ -446,11 +446,18 @@ __global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ 
 }
 
 // Binning sorts of the closest-hit and shadow queues of bounce k (counting sorts on
-// the keys the shade stage wrote): histogram, exclusive scan, scatter. Blocks of 1024
-// threads with a kBins-word histogram in dynamic shared memory; keys are masked
-// to kBins so every shared-memory index is in range.
-// A counting sort of `*count` items by 15-bit key: out[position] = items[i], or i
-// when items is null; with fine set, fine_out[position] = fine[i] as well.
+// the keys the shade stage wrote). A counting sort of `*count` items by 15-bit key:
+// out[position] = items[i], or i when items is null; with fine set, fine_out[position]
+// = fine[i] as well. Each of `grid` blocks (1024 threads, a kBins-word histogram in
+// dynamic shared memory) owns one contiguous chunk of the items:
+//   count:   the chunk's histogram, written as row `block` of hist (block-major);
+//   colscan: per bin, the exclusive prefix of its row entries over the blocks (in
+//            place) and the bin's total, into bins;
+//   scan:    bins -> exclusive bin starts;
+//   scatter: block b places its items from bins[key] + hist[b][key] on, with
+//            shared-memory atomics only.
+// No global atomics: a block's share of every bin is known before it writes. Keys
+// are masked to kBins so every shared-memory index is in range.
 struct BinSrc {
 	const uint16_t *keys;
 	const unsigned *count;
@@ -460,18 +467,53 @@ struct BinSrc {
 	uint8_t *fine_out;
 };
 
-__global__ void __launch_bounds__(1024) k_wf_bin_count(BinSrc src, unsigned *bins) {
-	extern __shared__ unsigned h[];
+// The items [c0, c1) of block `blk` of `nblk` (the same split in count and scatter).
+__device__ __forceinline__ void bin_chunk(unsigned n, unsigned blk, unsigned nblk, unsigned &c0, unsigned &c1) {
+	const unsigned per = (n + nblk - 1) / nblk;
+	c0 = min(n, blk * per);
+	c1 = min(n, c0 + per);
+}
+
+__global__ void __launch_bounds__(1024) k_wf_bin_count(BinSrc src, unsigned *hist) {
+	extern __shared__ __align__(16) unsigned h[];
 	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
 		h[b] = 0;
 	__syncthreads();
-	const unsigned n = *src.count;
-	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	unsigned c0, c1;
+	bin_chunk(*src.count, blockIdx.x, gridDim.x, c0, c1);
+	for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x)
 		atomicAdd(&h[src.keys[i] & (kBins - 1)], 1u);
 	__syncthreads();
-	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
-		if (h[b])
-			atomicAdd(&bins[b], h[b]);
+	uint4 *row = reinterpret_cast<uint4 *>(hist + static_cast<size_t>(blockIdx.x) * kBins);
+	const uint4 *hv = reinterpret_cast<const uint4 *>(h);
+	for (int b = threadIdx.x; b < kBins / 4; b += blockDim.x)
+		row[b] = hv[b];
+}
+
+// One thread per bin, walking the blocks' rows eight at a time.
+constexpr int kColScanThreads = 256;
+static_assert(kBins % kColScanThreads == 0, "k_wf_bin_colscan covers the bins exactly");
+__global__ void __launch_bounds__(kColScanThreads) k_wf_bin_colscan(unsigned *hist, int blocks, unsigned *bins) {
+	const int b = blockIdx.x * blockDim.x + threadIdx.x;
+	unsigned run = 0;
+	int k = 0;
+	for (; k + 8 <= blocks; k += 8) {
+		unsigned c[8];
+#pragma unroll
+		for (int j = 0; j < 8; j++)
+			c[j] = hist[static_cast<size_t>(k + j) * kBins + b];
+#pragma unroll
+		for (int j = 0; j < 8; j++) {
+			hist[static_cast<size_t>(k + j) * kBins + b] = run;
+			run += c[j];
+		}
+	}
+	for (; k < blocks; k++) {
+		const unsigned c = hist[static_cast<size_t>(k) * kBins + b];
+		hist[static_cast<size_t>(k) * kBins + b] = run;
+		run += c;
+	}
+	bins[b] = run;
 }
 
 // One block of 1024 threads, kBins / 1024 consecutive bins each: counts -> exclusive offsets.
@@ -513,25 +555,23 @@ __global__ void __launch_bounds__(kScanThreads) k_wf_bin_scan(unsigned *bins) {
 	}
 }
 
-// Each block takes a contiguous chunk of the items, reserves its share of every
-// bin with one atomic per non-empty bin, then places its items.
-__global__ void __launch_bounds__(1024) k_wf_bin_scatter(BinSrc src, unsigned *bins, int *status) {
-	extern __shared__ unsigned h[];
-	for (int b = threadIdx.x; b < kBins; b += blockDim.x)
-		h[b] = 0;
-	__syncthreads();
-	const unsigned n = *src.count;
-	const unsigned per = (n + gridDim.x - 1) / gridDim.x;
-	const unsigned c0 = min(n, blockIdx.x * per);
-	const unsigned c1 = min(n, c0 + per);
-	for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x)
-		atomicAdd(&h[src.keys[i] & (kBins - 1)], 1u);
-	__syncthreads();
-	for (int b = threadIdx.x; b < kBins; b += blockDim.x) {
-		const unsigned c = h[b];
-		h[b] = c ? atomicAdd(&bins[b], c) : 0u;
+// Block b's share of bin k starts at bins[k] + hist[b][k] (bins: exclusive bin starts).
+__global__ void __launch_bounds__(1024) k_wf_bin_scatter(BinSrc src, const unsigned *bins, const unsigned *hist,
+                                                         int *status) {
+	extern __shared__ __align__(16) unsigned h[];
+	{
+		const uint4 *row = reinterpret_cast<const uint4 *>(hist + static_cast<size_t>(blockIdx.x) * kBins);
+		const uint4 *bv = reinterpret_cast<const uint4 *>(bins);
+		uint4 *hv = reinterpret_cast<uint4 *>(h);
+		for (int b = threadIdx.x; b < kBins / 4; b += blockDim.x) {
+			const uint4 r = row[b], o = bv[b];
+			hv[b] = make_uint4(o.x + r.x, o.y + r.y, o.z + r.z, o.w + r.w);
+		}
 	}
 	__syncthreads();
+	const unsigned n = *src.count;
+	unsigned c0, c1;
+	bin_chunk(n, blockIdx.x, gridDim.x, c0, c1);
 	for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
 		const unsigned pos = atomicAdd(&h[src.keys[i] & (kBins - 1)], 1u);
 		if (kBoundsCheck && pos >= n) {
@@ -545,17 +585,18 @@ __global__ void __launch_bounds__(1024) k_wf_bin_scatter(BinSrc src, unsigned *b
 }
 
 // Second level of the ray sort: block b takes origin cell b's entries of the first
-// level's output (after the scatter bins[b] holds the end of cell b, so the cell
-// spans [bins[b-1], bins[b])) and places them by their 8-bit direction cell with a
-// shared-memory counting sort. The queue ends up ordered by (origin cell,
+// level's output (bins holds the exclusive cell starts, so the cell spans
+// [bins[b], bins[b+1]), the last one up to the item count) and places them by their
+// 8-bit direction cell with a shared-memory counting sort. The queue ends up ordered by (origin cell,
 // direction cell); entries of one bin keep no particular order.
 constexpr int kFineBins = 256;
-__global__ void __launch_bounds__(kFineBins) k_wf_bin_refine(const unsigned *bins, const int *in, const uint8_t *fine,
-                                                             int *out, unsigned n_max, int *status) {
+__global__ void __launch_bounds__(kFineBins) k_wf_bin_refine(const unsigned *bins, const unsigned *count,
+                                                             const int *in, const uint8_t *fine, int *out,
+                                                             unsigned n_max, int *status) {
 	__shared__ unsigned h[kFineBins];
 	__shared__ unsigned wsum[kFineBins / 32];
-	const unsigned s = blockIdx.x ? bins[blockIdx.x - 1] : 0u;
-	const unsigned e = bins[blockIdx.x];
+	const unsigned s = bins[blockIdx.x];
+	const unsigned e = blockIdx.x + 1 < kBins ? bins[blockIdx.x + 1] : *count;
 	if (e <= s) // the same for every thread of the block
 		return;
 	if (kBoundsCheck && e > n_max) {
@@ -604,13 +645,12 @@ __global__ void __launch_bounds__(kFineBins) k_wf_bin_refine(const unsigned *bin
 	}
 }
 
-cudaError_t bin_sort(const BinSrc &src, unsigned *bins, int grid, int *status, cudaStream_t st) {
-	cudaError_t e = cudaMemsetAsync(bins, 0, kBins * sizeof(unsigned), st);
-	if (e != cudaSuccess)
-		return e;
-	k_wf_bin_count<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, bins);
+// Four launches; `grid` <= kBinBlocksMax (the rows of hist).
+cudaError_t bin_sort(const BinSrc &src, unsigned *bins, unsigned *hist, int grid, int *status, cudaStream_t st) {
+	k_wf_bin_count<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, hist);
+	k_wf_bin_colscan<<<kBins / kColScanThreads, kColScanThreads, 0, st>>>(hist, grid, bins);
 	k_wf_bin_scan<<<1, kScanThreads, 0, st>>>(bins);
-	k_wf_bin_scatter<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, bins, status);
+	k_wf_bin_scatter<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, bins, hist, status);
 	return cudaGetLastError();
 }
 
@@ -695,19 +735,20 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 		return e;
 	const bool use_dyn = lc.dyn && order == kOrderReference && !adj;
 	const bool sort = lc.sort && pool.keys && pool.fine && pool.sorted_coarse && pool.sorted_fine && pool.sorted &&
-	                  pool.bins;
+	                  pool.bins && pool.bin_hist && lc.grid_bin >= 1 && lc.grid_bin <= kBinBlocksMax;
 	for (int k = 0; k < max_depth; k++) {
 		const int *q = pool.queue[k & 1];
 		if (sort && k > 0) {
 			e = bin_sort(BinSrc{pool.keys, pool.counters + kCntRays + k, q, pool.sorted_coarse, pool.fine,
 			                    pool.sorted_fine},
-			             pool.bins, lc.grid_bin, status, st);
+			             pool.bins, pool.bin_hist, lc.grid_bin, status, st);
 			if (e != cudaSuccess)
 				return e;
-			k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.sorted_coarse, pool.sorted_fine, pool.sorted,
+			k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.counters + kCntRays + k, pool.sorted_coarse,
+			                                            pool.sorted_fine, pool.sorted,
 			                                            static_cast<unsigned>(pool.capacity), status);
 			q = pool.sorted;
-			if ((e = mark(kStRaySort, 4)) != cudaSuccess)
+			if ((e = mark(kStRaySort, 5)) != cudaSuccess)
 				return e;
 		}
 		const int oj = wave.only_job;
@@ -739,13 +780,13 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			if (sort_sh) {
 				e = bin_sort(BinSrc{pool.sh_keys, pool.counters + kCntShadow + k, nullptr, pool.sorted_coarse,
 				                    pool.sh_fine, pool.sorted_fine},
-				             pool.bins, lc.grid_bin, status, st);
+				             pool.bins, pool.bin_hist, lc.grid_bin, status, st);
 				if (e != cudaSuccess)
 					return e;
-				k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.sorted_coarse, pool.sorted_fine,
-				                                            pool.sh_sorted, static_cast<unsigned>(pool.capacity),
-				                                            status);
-				if ((e = mark(kStShadowSort, 4)) != cudaSuccess)
+				k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.counters + kCntShadow + k,
+				                                            pool.sorted_coarse, pool.sorted_fine, pool.sh_sorted,
+				                                            static_cast<unsigned>(pool.capacity), status);
+				if ((e = mark(kStShadowSort, 5)) != cudaSuccess)
 					return e;
 			}
 			const int *order_sh = sort_sh ? pool.sh_sorted : nullptr;
@@ -784,7 +825,7 @@ void wf_grid_sizes(int &grid_ext, int &grid_shade, int &grid_sh, int &grid_dyn, 
 	grid_sh = sms * (c > 0 ? c : 1);
 	const int d = d0 < d1 ? d0 : d1;
 	grid_dyn = sms * (d > 0 ? d : 1);
-	grid_bin = sms; // one 1024-thread block per SM keeps the bin atomics few
+	grid_bin = sms < kBinBlocksMax ? sms : kBinBlocksMax; // one 1024-thread block per SM
 	constexpr int kHist = kBins * static_cast<int>(sizeof(unsigned));
 	if (kHist > 48 * 1024) {
 		cudaFuncSetAttribute(k_wf_bin_count, cudaFuncAttributeMaxDynamicSharedMemorySize, kHist);

@@ -63,7 +63,8 @@ struct WfPool {
 	int *sorted_coarse;
 	uint8_t *sorted_fine;
 	int *sorted;
-	unsigned *bins; // kBins counters, then offsets
+	unsigned *bins;     // kBins bin totals, then exclusive bin starts
+	unsigned *bin_hist; // kBinBlocksMax rows of kBins: per-block counts, then per-block offsets
 	// With binning on, each shadow record's key in two parts (the 15-bit Morton cell
 	// of its origin, the shading point, and the 6-bit Morton sub-cell of the origin
 	// inside it) and the shadow stage's order sorted by them (the same two counting
@@ -92,6 +93,7 @@ struct WfPool {
 
 constexpr int kBinBits = 15;
 constexpr int kBins = 1 << kBinBits;
+constexpr int kBinBlocksMax = 256; // blocks of the counting sorts
 
 constexpr int kCntRays = 0;
 constexpr int kCntShadow = kWfMaxDepth + 1;

@@ -46,6 +46,7 @@ rn_status WfContext::ensure_pool(int capacity) {
 	RNB_CUDA(sorted_fine_.ensure(n));
 	RNB_CUDA(sorted_.ensure(n * 4));
 	RNB_CUDA(bins_.ensure(kBins * sizeof(unsigned)));
+	RNB_CUDA(bin_hist_.ensure(static_cast<size_t>(kBinBlocksMax) * kBins * sizeof(unsigned)));
 	RNB_CUDA(sh_keys_.ensure(n * sizeof(uint16_t)));
 	RNB_CUDA(sh_fine_.ensure(n));
 	RNB_CUDA(sh_sorted_.ensure(n * 4));
@@ -70,6 +71,7 @@ rn_status WfContext::ensure_pool(int capacity) {
 	pool_.sorted_fine = sorted_fine_.as<uint8_t>();
 	pool_.sorted = sorted_.as<int>();
 	pool_.bins = bins_.as<unsigned>();
+	pool_.bin_hist = bin_hist_.as<unsigned>();
 	pool_.sh_keys = sh_keys_.as<uint16_t>();
 	pool_.sh_fine = sh_fine_.as<uint8_t>();
 	pool_.sh_sorted = sh_sorted_.as<int>();

@@ -94,7 +94,7 @@ private:
 	void release_graph();
 
 	DevBuf o_, d_, beta_, L_, pixel_, sample_, hit_idx_, hit_t_, q0_, q1_, sh_o_, sh_d_, sh_c_, counters_;
-	DevBuf keys_, fine_, sorted_coarse_, sorted_fine_, sorted_, bins_, sh_keys_, sh_fine_, sh_sorted_;
+	DevBuf keys_, fine_, sorted_coarse_, sorted_fine_, sorted_, bins_, bin_hist_, sh_keys_, sh_fine_, sh_sorted_;
 	DevBuf adj_pt_, adj_dlog_, adj_n_, sh_gdlog_, sh_gle_;
 	DevBuf d_jobs_, d_wave_tab_;
 	WfPool pool_{};
