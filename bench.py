@@ -545,9 +545,9 @@ def run_ours(args):
         waves = (spp + spw - 1) // spw
         per_wave = 2 + 3 * args.depth  # camera, 3 stages per bounce, accumulate
         if tuned["ray_sort"] and not tuned["dynamic_fetch"]:
-            # two-level counting sorts (count, column scan, bin scan, scatter, refine) of the
-            # ray queue before bounces 1.. and of the shadow queue at every bounce
-            per_wave += 5 * (args.depth - 1) + 5 * args.depth
+            # two-level counting sorts (count, column scan, scatter, refine) of the ray queue
+            # before bounces 1.. and of the shadow queue at every bounce
+            per_wave += 4 * (args.depth - 1) + 4 * args.depth
         launches_per_step = waves * per_wave + 1  # + resolve
 
     with torch.cuda.stream(stream):

@@ -452,10 +452,10 @@ __global__ void __launch_bounds__(128) k_wf_trace_dyn(const WfJob *__restrict__ 
 // dynamic shared memory) owns one contiguous chunk of the items:
 //   count:   the chunk's histogram, written as row `block` of hist (block-major);
 //   colscan: per bin, the exclusive prefix of its row entries over the blocks (in
-//            place) and the bin's total, into bins;
-//   scan:    bins -> exclusive bin starts;
-//   scatter: block b places its items from bins[key] + hist[b][key] on, with
-//            shared-memory atomics only.
+//            place) and the bin's total, into bins[0, kBins);
+//   scatter: every block scans the bin totals into exclusive bin starts on its own
+//            (block 0 also stores them in bins[kBins, 2 kBins)), then places its
+//            items from start[key] + hist[b][key] on, with shared-memory atomics only.
 // No global atomics: a block's share of every bin is known before it writes. Keys
 // are masked to kBins so every shared-memory index is in range.
 struct BinSrc {
@@ -516,17 +516,22 @@ __global__ void __launch_bounds__(kColScanThreads) k_wf_bin_colscan(unsigned *hi
 	bins[b] = run;
 }
 
-// One block of 1024 threads, kBins / 1024 consecutive bins each: counts -> exclusive offsets.
+
+// Exclusive scan of the kBins bin totals into shared memory, by one block of 1024
+// threads (32 consecutive bins each); every scatter block runs it on its own copy.
 constexpr int kScanThreads = 1024;
 constexpr int kBinsPerThread = kBins / kScanThreads;
-static_assert(kBins % kScanThreads == 0, "k_wf_bin_scan splits the bins evenly");
-__global__ void __launch_bounds__(kScanThreads) k_wf_bin_scan(unsigned *bins) {
-	__shared__ unsigned warp_sum[kScanThreads / 32];
+static_assert(kBins == kScanThreads * 32, "block_scan_bins gives each thread 8 uint4 of bins");
+__device__ __forceinline__ void block_scan_bins(const unsigned *totals, unsigned *h, unsigned *warp_sum) {
 	const int t = threadIdx.x;
-	unsigned *mine = bins + t * kBinsPerThread;
+	const uint4 *tv = reinterpret_cast<const uint4 *>(totals) + t * (kBinsPerThread / 4);
+	uint4 v[kBinsPerThread / 4];
 	unsigned own = 0;
-	for (int i = 0; i < kBinsPerThread; i++)
-		own += mine[i];
+#pragma unroll
+	for (int j = 0; j < kBinsPerThread / 4; j++) {
+		v[j] = tv[j];
+		own += v[j].x + v[j].y + v[j].z + v[j].w;
+	}
 	unsigned x = own;
 	for (int o = 1; o < 32; o <<= 1) {
 		const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
@@ -548,23 +553,36 @@ __global__ void __launch_bounds__(kScanThreads) k_wf_bin_scan(unsigned *bins) {
 	}
 	__syncthreads();
 	unsigned run = warp_sum[t >> 5] + x - own;
-	for (int i = 0; i < kBinsPerThread; i++) {
-		const unsigned c = mine[i];
-		mine[i] = run;
-		run += c;
+	uint4 *hv = reinterpret_cast<uint4 *>(h) + t * (kBinsPerThread / 4);
+#pragma unroll
+	for (int j = 0; j < kBinsPerThread / 4; j++) {
+		uint4 o;
+		o.x = run;
+		o.y = o.x + v[j].x;
+		o.z = o.y + v[j].y;
+		o.w = o.z + v[j].z;
+		run = o.w + v[j].w;
+		hv[j] = o;
 	}
 }
 
-// Block b's share of bin k starts at bins[k] + hist[b][k] (bins: exclusive bin starts).
-__global__ void __launch_bounds__(1024) k_wf_bin_scatter(BinSrc src, const unsigned *bins, const unsigned *hist,
+// Block b's share of bin k starts at start[k] + hist[b][k], start being the exclusive
+// scan of the bin totals (bins[0, kBins)), which every block computes for itself;
+// block 0 also stores it in bins[kBins, 2 kBins) for the second-level sort.
+__global__ void __launch_bounds__(1024) k_wf_bin_scatter(BinSrc src, unsigned *bins, const unsigned *hist,
                                                          int *status) {
 	extern __shared__ __align__(16) unsigned h[];
+	__shared__ unsigned warp_sum[kScanThreads / 32];
+	block_scan_bins(bins, h, warp_sum);
+	__syncthreads();
 	{
 		const uint4 *row = reinterpret_cast<const uint4 *>(hist + static_cast<size_t>(blockIdx.x) * kBins);
-		const uint4 *bv = reinterpret_cast<const uint4 *>(bins);
 		uint4 *hv = reinterpret_cast<uint4 *>(h);
+		uint4 *starts = reinterpret_cast<uint4 *>(bins + kBins);
 		for (int b = threadIdx.x; b < kBins / 4; b += blockDim.x) {
-			const uint4 r = row[b], o = bv[b];
+			const uint4 r = row[b], o = hv[b];
+			if (blockIdx.x == 0)
+				starts[b] = o;
 			hv[b] = make_uint4(o.x + r.x, o.y + r.y, o.z + r.z, o.w + r.w);
 		}
 	}
@@ -585,18 +603,18 @@ __global__ void __launch_bounds__(1024) k_wf_bin_scatter(BinSrc src, const unsig
 }
 
 // Second level of the ray sort: block b takes origin cell b's entries of the first
-// level's output (bins holds the exclusive cell starts, so the cell spans
+// level's output (starts holds the exclusive cell starts, so the cell spans
 // [bins[b], bins[b+1]), the last one up to the item count) and places them by their
 // 8-bit direction cell with a shared-memory counting sort. The queue ends up ordered by (origin cell,
 // direction cell); entries of one bin keep no particular order.
 constexpr int kFineBins = 256;
-__global__ void __launch_bounds__(kFineBins) k_wf_bin_refine(const unsigned *bins, const unsigned *count,
+__global__ void __launch_bounds__(kFineBins) k_wf_bin_refine(const unsigned *starts, const unsigned *count,
                                                              const int *in, const uint8_t *fine, int *out,
                                                              unsigned n_max, int *status) {
 	__shared__ unsigned h[kFineBins];
 	__shared__ unsigned wsum[kFineBins / 32];
-	const unsigned s = bins[blockIdx.x];
-	const unsigned e = blockIdx.x + 1 < kBins ? bins[blockIdx.x + 1] : *count;
+	const unsigned s = starts[blockIdx.x];
+	const unsigned e = blockIdx.x + 1 < kBins ? starts[blockIdx.x + 1] : *count;
 	if (e <= s) // the same for every thread of the block
 		return;
 	if (kBoundsCheck && e > n_max) {
@@ -645,11 +663,10 @@ __global__ void __launch_bounds__(kFineBins) k_wf_bin_refine(const unsigned *bin
 	}
 }
 
-// Four launches; `grid` <= kBinBlocksMax (the rows of hist).
+// Three launches; `grid` <= kBinBlocksMax (the rows of hist). bins holds 2 kBins words.
 cudaError_t bin_sort(const BinSrc &src, unsigned *bins, unsigned *hist, int grid, int *status, cudaStream_t st) {
 	k_wf_bin_count<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, hist);
 	k_wf_bin_colscan<<<kBins / kColScanThreads, kColScanThreads, 0, st>>>(hist, grid, bins);
-	k_wf_bin_scan<<<1, kScanThreads, 0, st>>>(bins);
 	k_wf_bin_scatter<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, bins, hist, status);
 	return cudaGetLastError();
 }
@@ -744,11 +761,11 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 			             pool.bins, pool.bin_hist, lc.grid_bin, status, st);
 			if (e != cudaSuccess)
 				return e;
-			k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.counters + kCntRays + k, pool.sorted_coarse,
+			k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins + kBins, pool.counters + kCntRays + k, pool.sorted_coarse,
 			                                            pool.sorted_fine, pool.sorted,
 			                                            static_cast<unsigned>(pool.capacity), status);
 			q = pool.sorted;
-			if ((e = mark(kStRaySort, 5)) != cudaSuccess)
+			if ((e = mark(kStRaySort, 4)) != cudaSuccess)
 				return e;
 		}
 		const int oj = wave.only_job;
@@ -783,10 +800,10 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 				             pool.bins, pool.bin_hist, lc.grid_bin, status, st);
 				if (e != cudaSuccess)
 					return e;
-				k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins, pool.counters + kCntShadow + k,
+				k_wf_bin_refine<<<kBins, kFineBins, 0, st>>>(pool.bins + kBins, pool.counters + kCntShadow + k,
 				                                            pool.sorted_coarse, pool.sorted_fine, pool.sh_sorted,
 				                                            static_cast<unsigned>(pool.capacity), status);
-				if ((e = mark(kStShadowSort, 5)) != cudaSuccess)
+				if ((e = mark(kStShadowSort, 4)) != cudaSuccess)
 					return e;
 			}
 			const int *order_sh = sort_sh ? pool.sh_sorted : nullptr;

@@ -63,7 +63,7 @@ struct WfPool {
 	int *sorted_coarse;
 	uint8_t *sorted_fine;
 	int *sorted;
-	unsigned *bins;     // kBins bin totals, then exclusive bin starts
+	unsigned *bins;     // kBins bin totals, then kBins exclusive bin starts
 	unsigned *bin_hist; // kBinBlocksMax rows of kBins: per-block counts, then per-block offsets
 	// With binning on, each shadow record's key in two parts (the 15-bit Morton cell
 	// of its origin, the shading point, and the 6-bit Morton sub-cell of the origin

@@ -45,7 +45,7 @@ rn_status WfContext::ensure_pool(int capacity) {
 	RNB_CUDA(sorted_coarse_.ensure(n * 4));
 	RNB_CUDA(sorted_fine_.ensure(n));
 	RNB_CUDA(sorted_.ensure(n * 4));
-	RNB_CUDA(bins_.ensure(kBins * sizeof(unsigned)));
+	RNB_CUDA(bins_.ensure(2 * kBins * sizeof(unsigned)));
 	RNB_CUDA(bin_hist_.ensure(static_cast<size_t>(kBinBlocksMax) * kBins * sizeof(unsigned)));
 	RNB_CUDA(sh_keys_.ensure(n * sizeof(uint16_t)));
 	RNB_CUDA(sh_fine_.ensure(n));

@@ -272,9 +272,9 @@ def test_profile_wavefront_equals_render_and_times_every_stage():
         parts = sum(t[k] for k in ("camera_ms", "ray_sort_ms", "extend_ms", "shade_ms", "shadow_sort_ms",
                                    "shadow_ms", "accumulate_ms"))
         assert abs(parts - t["total_ms"]) <= 1e-3 * t["total_ms"] + 1e-3, (parts, t)
-        # camera + accumulate, 3 stages per bounce, and 5 kernels per sort (count, column
-        # scan, bin scan, scatter, refine): 5 ray sorts and 6 shadow sorts at depth 6
-        per_wave = 2 + 3 * 6 + (5 * 5 + 5 * 6 if sort else 0)
+        # camera + accumulate, 3 stages per bounce, and 4 kernels per sort (count, column
+        # scan, scatter, refine): 5 ray sorts and 6 shadow sorts at depth 6
+        per_wave = 2 + 3 * 6 + (4 * 5 + 4 * 6 if sort else 0)
         assert t["launches"] == t["waves"] * per_wave + 1, t
 
 
