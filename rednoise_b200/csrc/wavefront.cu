@@ -490,14 +490,36 @@ __global__ void __launch_bounds__(1024) k_wf_bin_count(BinSrc src, unsigned *his
 		row[b] = hv[b];
 }
 
-// One thread per bin, walking the blocks' rows eight at a time.
+// kColSplit consecutive lanes per bin, each walking one stretch of the blocks' rows
+// (eight loads in flight), joined by a shuffle scan across the stretches.
 constexpr int kColScanThreads = 256;
-static_assert(kBins % kColScanThreads == 0, "k_wf_bin_colscan covers the bins exactly");
+constexpr int kColSplit = 4;
+static_assert(kBins * kColSplit % kColScanThreads == 0, "k_wf_bin_colscan covers the bins exactly");
+static_assert(32 % kColSplit == 0, "a bin's lanes share a warp");
 __global__ void __launch_bounds__(kColScanThreads) k_wf_bin_colscan(unsigned *hist, int blocks, unsigned *bins) {
-	const int b = blockIdx.x * blockDim.x + threadIdx.x;
-	unsigned run = 0;
-	int k = 0;
-	for (; k + 8 <= blocks; k += 8) {
+	const int g = blockIdx.x * blockDim.x + threadIdx.x;
+	const int b = g / kColSplit, part = g % kColSplit;
+	const int per = (blocks + kColSplit - 1) / kColSplit;
+	const int k0 = min(blocks, part * per), k1 = min(blocks, k0 + per);
+	unsigned sum = 0;
+	int k = k0;
+	for (; k + 8 <= k1; k += 8) {
+#pragma unroll
+		for (int j = 0; j < 8; j++)
+			sum += hist[static_cast<size_t>(k + j) * kBins + b];
+	}
+	for (; k < k1; k++)
+		sum += hist[static_cast<size_t>(k) * kBins + b];
+	unsigned x = sum;
+	for (int o = 1; o < kColSplit; o <<= 1) {
+		const unsigned y = __shfl_up_sync(0xffffffffu, x, o, kColSplit);
+		if (part >= o)
+			x += y;
+	}
+	const unsigned total = __shfl_sync(0xffffffffu, x, kColSplit - 1, kColSplit);
+	unsigned run = x - sum;
+	k = k0;
+	for (; k + 8 <= k1; k += 8) {
 		unsigned c[8];
 #pragma unroll
 		for (int j = 0; j < 8; j++)
@@ -508,14 +530,14 @@ __global__ void __launch_bounds__(kColScanThreads) k_wf_bin_colscan(unsigned *hi
 			run += c[j];
 		}
 	}
-	for (; k < blocks; k++) {
+	for (; k < k1; k++) {
 		const unsigned c = hist[static_cast<size_t>(k) * kBins + b];
 		hist[static_cast<size_t>(k) * kBins + b] = run;
 		run += c;
 	}
-	bins[b] = run;
+	if (part == 0)
+		bins[b] = total;
 }
-
 
 // Exclusive scan of the kBins bin totals into shared memory, by one block of 1024
 // threads (32 consecutive bins each); every scatter block runs it on its own copy.
@@ -666,7 +688,7 @@ __global__ void __launch_bounds__(kFineBins) k_wf_bin_refine(const unsigned *sta
 // Three launches; `grid` <= kBinBlocksMax (the rows of hist). bins holds 2 kBins words.
 cudaError_t bin_sort(const BinSrc &src, unsigned *bins, unsigned *hist, int grid, int *status, cudaStream_t st) {
 	k_wf_bin_count<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, hist);
-	k_wf_bin_colscan<<<kBins / kColScanThreads, kColScanThreads, 0, st>>>(hist, grid, bins);
+	k_wf_bin_colscan<<<kBins * kColSplit / kColScanThreads, kColScanThreads, 0, st>>>(hist, grid, bins);
 	k_wf_bin_scatter<<<grid, 1024, kBins * sizeof(unsigned), st>>>(src, bins, hist, status);
 	return cudaGetLastError();
 }
