@@ -104,9 +104,11 @@ struct DeviceLayout {
 void flatten_bvh(const TriangleSet &ts, const Bvh2 &bvh, DeviceLayout &out);
 
 // Four-wide collapse of the same tree for the fast traversal. A node holds the
-// children of one reference node, with every internal child replaced by its own
-// two children (so up to four entries), in the order the reference pops them;
-// refs are int bits (>= 0 node, < 0 leaf as in the 2-wide layout).
+// children of one reference node, with an internal child either kept as an entry
+// or replaced by its own two children (so two to four entries), in the order the
+// reference pops them; which children are replaced is chosen bottom-up by an
+// area-weighted fetch cost. refs are int bits (>= 0 node, < 0 leaf as in the
+// 2-wide layout).
 // Boxes are the reference's own node boxes. Because float subtraction and
 // multiplication round monotonically, a grandchild's slab interval lies inside
 // its parent's, so skipping the parent's test never admits a node the
