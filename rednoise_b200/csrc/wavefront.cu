@@ -37,6 +37,20 @@ __device__ __forceinline__ int find_base(const int *bases, int n, int x) {
 	return lo;
 }
 
+// Position of pixel p (row-major, w x h) in the first closest-hit queue: 8 x 4 pixel
+// tiles in row-major tile order (one warp per tile), then the pixels the full tiles
+// leave over (the right strip row by row, then the bottom strip), a bijection on
+// [0, w h). Camera rays of one warp then start from a compact patch of the image.
+__device__ __forceinline__ uint32_t tile_order(uint32_t p, uint32_t w, uint32_t h) {
+	const uint32_t x = p % w, y = p / w;
+	const uint32_t w8 = w - w % 8, h4 = h - h % 4;
+	if (x < w8 && y < h4)
+		return ((y / 4) * (w8 / 8) + x / 8) * 32 + (y % 4) * 8 + x % 8;
+	if (y < h4)
+		return w8 * h4 + y * (w - w8) + (x - w8);
+	return w8 * h4 + h4 * (w - w8) + (y - h4) * w + x;
+}
+
 __global__ void __launch_bounds__(256) k_wf_camera(const WfJob *__restrict__ jobs, WfPool pool, WfWave wave) {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < wave.n_slots; i += gridDim.x * blockDim.x) {
 		const int a = find_base(wave.bases, wave.n_jobs, i);
@@ -53,7 +67,11 @@ __global__ void __launch_bounds__(256) k_wf_camera(const WfJob *__restrict__ job
 		pool.L[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(j));
 		pool.pixel[i] = pixel;
 		pool.sample[i] = sample;
-		pool.queue[0][i] = i;
+		const bool tiled = job.cam.width > 0 && job.cam.height > 0 &&
+		                   static_cast<long long>(job.cam.width) * job.cam.height == job.n_pix;
+		const int in_block = tiled ? static_cast<int>(tile_order(pixel, job.cam.width, job.cam.height))
+		                           : static_cast<int>(pixel);
+		pool.queue[0][i - static_cast<int>(pixel) + in_block] = i;
 	}
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		pool.counters[kCntRays] = static_cast<unsigned>(wave.n_slots);
@@ -209,7 +227,7 @@ __global__ void __launch_bounds__(128, kAdj ? 5 : 8) k_wf_shade(const WfJob *__r
 	const unsigned n = pool.counters[kCntRays + k];
 	int *__restrict__ qn = pool.queue[(k + 1) & 1];
 	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-		const int slot = q[i];
+		const int slot = q ? q[i] : static_cast<int>(i); // null q: every slot, in slot order
 		const float4 o = pool.o[slot], d = pool.d[slot], b = pool.beta[slot], L = pool.L[slot];
 		const int j = __float_as_int(L.w);
 		const WfJob &job = jobs[j];
@@ -802,12 +820,14 @@ cudaError_t wf_launch_wave(const WfJob *d_jobs, const WfPool &pool, const WfWave
 		// Shading takes the queue in its append order, not the binned order: the previous
 		// bounce appended each warp's surviving slots in increasing order, so the path
 		// state reads and writes of neighbouring lanes fall on neighbouring slots. The
-		// results do not depend on the order in which paths are shaded.
+		// first bounce shades every slot in slot order (its queue is in pixel-tile order
+		// for the closest-hit stage). The results do not depend on the order in which
+		// paths are shaded.
+		const int *qs = k == 0 ? nullptr : pool.queue[k & 1];
 		if (adj)
-			k_wf_shade<true><<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, pool.queue[k & 1], sort ? 1 : 0, status);
+			k_wf_shade<true><<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, qs, sort ? 1 : 0, status);
 		else
-			k_wf_shade<false><<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, pool.queue[k & 1], sort ? 1 : 0,
-			                                                 status);
+			k_wf_shade<false><<<lc.grid_shade, 128, 0, st>>>(d_jobs, pool, k, qs, sort ? 1 : 0, status);
 		if ((e = mark(kStShade, 1)) != cudaSuccess)
 			return e;
 		if (use_dyn)
