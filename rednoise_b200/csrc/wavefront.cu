@@ -1,5 +1,6 @@
 // Wavefront integrator kernels (see wavefront.cuh).
 #include "wavefront.cuh"
+#include "pixel_tiles.cuh"
 
 namespace rnb {
 
@@ -35,20 +36,6 @@ __device__ __forceinline__ int find_base(const int *bases, int n, int x) {
 			hi = mid - 1;
 	}
 	return lo;
-}
-
-// Position of pixel p (row-major, w x h) in the first closest-hit queue: 8 x 4 pixel
-// tiles in row-major tile order (one warp per tile), then the pixels the full tiles
-// leave over (the right strip row by row, then the bottom strip), a bijection on
-// [0, w h). Camera rays of one warp then start from a compact patch of the image.
-__device__ __forceinline__ uint32_t tile_order(uint32_t p, uint32_t w, uint32_t h) {
-	const uint32_t x = p % w, y = p / w;
-	const uint32_t w8 = w - w % 8, h4 = h - h % 4;
-	if (x < w8 && y < h4)
-		return ((y / 4) * (w8 / 8) + x / 8) * 32 + (y % 4) * 8 + x % 8;
-	if (y < h4)
-		return w8 * h4 + y * (w - w8) + (x - w8);
-	return w8 * h4 + h4 * (w - w8) + (y - h4) * w + x;
 }
 
 __global__ void __launch_bounds__(256) k_wf_camera(const WfJob *__restrict__ jobs, WfPool pool, WfWave wave) {
