@@ -164,12 +164,15 @@ def test_wavefront_static_and_refetch_agree():
 
 
 @pytest.mark.parametrize("static,level,w,h,spp", [(False, 3, 64, 48, 8), (True, 3, 64, 48, 8),
-                                                  (False, 6, 320, 240, 32)])
+                                                  (False, 6, 320, 240, 32), (False, 3, 37, 23, 8),
+                                                  (False, 2, 5, 3, 8)])
 def test_ray_binning_changes_no_path(static, level, w, h, spp):
     """Binning each bounce's rays only reorders the queue: the image is bit-identical
     to the unbinned wavefront's and agrees with the megakernel's. The 320x240x32 case
     (2.46 M paths, 82k triangles) fills origin cells with thousands of rays each, so the
-    second sort level places large cells by direction cell."""
+    second sort level places large cells by direction cell. The 37x23 and 5x3 frames
+    are not whole 8 x 4 pixel tiles: the first queue's tile order then covers a ragged
+    right and bottom strip, or the strips alone."""
     sc = scenes.icosphere_scene(level=level)
     s = make_scene(sc)
     c = cam(w, h)
