@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(256) k_wf_camera(const WfJob *__restrict__ job
 		const PathState ps = camera_path(job.cam, job.st, pixel, sample);
 		pool.o[i] = make_float4(ps.o.x, ps.o.y, ps.o.z, __int_as_float(-1));
 		pool.d[i] = make_float4(ps.d.x, ps.d.y, ps.d.z, 0.0f);
-		pool.beta[i] = make_float4(1.0f, 1.0f, 1.0f, __int_as_float(0));
+		// beta is not written: the first shading stage takes throughput 1 at bounce 0
 		pool.L[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(j));
 		pool.pixel[i] = pixel;
 		pool.sample[i] = sample;
@@ -215,7 +215,9 @@ __global__ void __launch_bounds__(128, kAdj ? 5 : 8) k_wf_shade(const WfJob *__r
 	int *__restrict__ qn = pool.queue[(k + 1) & 1];
 	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
 		const int slot = q ? q[i] : static_cast<int>(i); // null q: every slot, in slot order
-		const float4 o = pool.o[slot], d = pool.d[slot], b = pool.beta[slot], L = pool.L[slot];
+		const float4 o = pool.o[slot], d = pool.d[slot], L = pool.L[slot];
+		// a camera path enters its first shading stage with throughput 1 at bounce 0
+		const float4 b = k == 0 ? make_float4(1.0f, 1.0f, 1.0f, __int_as_float(0)) : pool.beta[slot];
 		const int j = __float_as_int(L.w);
 		const WfJob &job = jobs[j];
 		PathState ps;
