@@ -595,6 +595,11 @@ __device__ __forceinline__ void block_scan_bins(const unsigned *totals, unsigned
 	}
 }
 
+// Measured on the 1.31M-triangle 1080p frame (sorts per frame): one pass 9.43 ms,
+// two 8.46 ms, four 10.65 ms, eight 15.1 ms (every pass walks the whole chunk).
+constexpr int kScatterPasses = 2;
+static_assert(kBins % kScatterPasses == 0, "each scatter pass takes a whole range of bins");
+
 // Block b's share of bin k starts at start[k] + hist[b][k], start being the exclusive
 // scan of the bin totals (bins[0, kBins)), which every block computes for itself;
 // block 0 also stores it in bins[kBins, 2 kBins) for the second-level sort.
@@ -619,15 +624,23 @@ __global__ void __launch_bounds__(1024) k_wf_bin_scatter(BinSrc src, unsigned *b
 	const unsigned n = *src.count;
 	unsigned c0, c1;
 	bin_chunk(n, blockIdx.x, gridDim.x, c0, c1);
-	for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-		const unsigned pos = atomicAdd(&h[src.keys[i] & (kBins - 1)], 1u);
-		if (kBoundsCheck && pos >= n) {
-			atomicOr(status, 1);
-			continue;
+	// kScatterPasses passes over the chunk, each placing the items of one range of
+	// bins: fewer partly written output sectors are open at a time when the keys
+	// arrive in random order (a later pass only re-reads the keys).
+	for (int pass = 0; pass < kScatterPasses; pass++) {
+		for (unsigned i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+			const unsigned key = src.keys[i] & (kBins - 1);
+			if (static_cast<int>(key / (kBins / kScatterPasses)) != pass)
+				continue;
+			const unsigned pos = atomicAdd(&h[key], 1u);
+			if (kBoundsCheck && pos >= n) {
+				atomicOr(status, 1);
+				continue;
+			}
+			src.out[pos] = src.items ? src.items[i] : static_cast<int>(i);
+			if (src.fine)
+				src.fine_out[pos] = src.fine[i];
 		}
-		src.out[pos] = src.items ? src.items[i] : static_cast<int>(i);
-		if (src.fine)
-			src.fine_out[pos] = src.fine[i];
 	}
 }
 
