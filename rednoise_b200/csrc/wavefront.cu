@@ -202,14 +202,15 @@ __device__ __forceinline__ F3 adj_weight(const WfJob &job, uint32_t pixel) {
 // radiance is complete when this stage starts (its next-event term was added by the
 // shadow stage), emission terms go to d_em here, next-event terms are handed to the
 // shadow stage with the record, and a continuing vertex joins the slot's list.
-// Eight resident blocks per SM for the primal stage: it waits on scattered loads of
+// Seven resident blocks per SM for the primal stage: it waits on scattered loads of
 // path state, and more warps in flight measured 18.3 ms (five blocks) -> 17.3 (six)
-// -> 17.0 ms (eight) on the bench frame, same image (the translation unit is
-// compiled without multiply-add contraction, so the register budget cannot change
-// the arithmetic). The adjoint instantiation keeps five: it carries the gradient
-// terms as well.
+// -> 17.0 ms (eight) on the bench frame; after the first bounce's shading moved to
+// slot order, seven gave 17.25 ms against eight's 17.6, nine 18.5 and ten 23.2
+// (spills). Same image throughout (the translation unit is compiled without
+// multiply-add contraction, so the register budget cannot change the arithmetic).
+// The adjoint instantiation keeps five: it carries the gradient terms as well.
 template <bool kAdj>
-__global__ void __launch_bounds__(128, kAdj ? 5 : 8) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
+__global__ void __launch_bounds__(128, kAdj ? 5 : 7) k_wf_shade(const WfJob *__restrict__ jobs, WfPool pool, int k,
                                                   const int *__restrict__ q, int write_keys, int *status) {
 	const unsigned n = pool.counters[kCntRays + k];
 	int *__restrict__ qn = pool.queue[(k + 1) & 1];
