@@ -8,10 +8,16 @@
 
 #include <stdint.h>
 
+#ifdef __CUDACC__
+#define RNB_TILE_FN __host__ __device__ __forceinline__
+#else
+#define RNB_TILE_FN inline // host-only builds (the host tests)
+#endif
+
 namespace rnb {
 
 // Position of row-major pixel p of a w x h image in tile order (a bijection on [0, w h)).
-__device__ __forceinline__ uint32_t tile_order(uint32_t p, uint32_t w, uint32_t h) {
+RNB_TILE_FN uint32_t tile_order(uint32_t p, uint32_t w, uint32_t h) {
 	const uint32_t x = p % w, y = p / w;
 	const uint32_t w8 = w - w % 8, h4 = h - h % 4;
 	if (x < w8 && y < h4)

@@ -2,7 +2,8 @@
 // under ThreadSanitizer (tests/test_host_sanitize.py builds it): the OBJ/MTL
 // loader on well-formed and malformed files, the reference-identical BVH build
 // (including its threaded top levels) on random, degenerate and coincident
-// triangles, and both device-layout flattenings, with the tree invariants checked.
+// triangles, and both device-layout flattenings, with the tree invariants checked;
+// also the wavefront's first-queue pixel order (a permutation for every frame size).
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -13,6 +14,7 @@
 #include <vector>
 
 #include "host_scene.hpp"
+#include "pixel_tiles.cuh"
 
 using namespace rnb;
 
@@ -170,6 +172,34 @@ static void complete_tree_case() {
 	CHECK(full == 42);
 }
 
+// The first closest-hit queue's pixel order is a permutation of the frame's pixels
+// for every frame size, whole 8 x 4 tiles or not.
+static void tile_order_cases() {
+	for (uint32_t w = 1; w <= 41; w++)
+		for (uint32_t h = 1; h <= 13; h++) {
+			std::vector<int> seen(static_cast<size_t>(w) * h, 0);
+			for (uint32_t p = 0; p < w * h; p++) {
+				const uint32_t t = tile_order(p, w, h);
+				CHECK(t < w * h);
+				if (t < w * h)
+					seen[t]++;
+			}
+			for (int c : seen)
+				CHECK(c == 1);
+		}
+	const uint32_t w = 1920, h = 1080;
+	std::vector<uint8_t> seen(static_cast<size_t>(w) * h, 0);
+	bool ok = true;
+	for (uint32_t p = 0; p < w * h; p++) {
+		const uint32_t t = tile_order(p, w, h);
+		ok = ok && t < w * h && !seen[t];
+		if (t < w * h)
+			seen[t] = 1;
+	}
+	CHECK(ok);
+	CHECK(tile_order(0, w, h) == 0 && tile_order(1, w, h) == 1 && tile_order(w, w, h) == 8);
+}
+
 static void tree_case(const std::vector<float> &v) {
 	Bvh2 b;
 	build_reference_bvh(v.data(), static_cast<int>(v.size() / 9), b);
@@ -245,6 +275,7 @@ int main(int argc, char **argv) {
 	tree_case(same);
 	tree_case(soup(300000, 5u, 1.0f)); // large enough for the threaded top levels
 	complete_tree_case();
+	tile_order_cases();
 	std::printf(g_fail ? "FAILED\n" : "host checks passed\n");
 	return g_fail;
 }
